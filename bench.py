@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""EDGE steps/s at 256x128x128 on B200 (four-vortex collision, EDGE variant).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one substep of the EDGE driver loop (run_edge.py:588-712): CFL dt,
+map reinitialisation every 12 steps, semi-Lagrangian midpoint advection,
+MGPCG projection, EDGE flow-map march, forward-map march, BFECC pullback of
+velocity and dye with clamps, second projection.  Workload: 256x128x128 MAC
+grid (dx = 1/128), four vortex rings of init_four_vorts rotated to travel
+along x, CFL 0.5, epsilon 0.025 dx, 6-level MGPCG (base_level 2) to the
+reference tolerance (r.r < 1e-12 or 1e-12 z0.r0), BFECC clamp on.  Synthetic
+seeded input (no dataset); the step's working set (~1.7 GB) exceeds L2, so L2
+is not warm between timed steps.
+
+Multi-GPU: the solver does not shard (one grid per GPU); N ranks run N
+independent replicas, value = N x K / max-over-ranks time ("scaling": "weak").
+
+--impl reference times the reference's CPU restatement (the oracle, OpenMP on
+all host cores) on the same workload, rank 0 only, a bounded number of steps.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "edge-flow-maps_b200")
+for _p in (PKG, ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+RES = (256, 128, 128)
+DX = 1.0 / 128
+CFL = 0.5
+REINIT = 12
+BASE_LEVEL = 2
+EPS_FRAC = 0.025
+METRIC = "EDGE steps/s at 256x128x128"
+UNIT = "steps/s"
+
+# algorithmic work per unit (cells Nc, faces Nf; float32)
+NC = RES[0] * RES[1] * RES[2]
+NF = (RES[0] + 1) * RES[1] * RES[2] + RES[0] * (RES[1] + 1) * RES[2] + RES[0] * RES[1] * (RES[2] + 1)
+# MGPCG: per CG iteration 117 B per fine cell; set-up 100 B per cell plus
+# divergence / gradient update 36 B per face
+MG_ITER_BYTES = 117 * NC
+MG_SETUP_BYTES = 100 * NC + 36 * NF
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_sim(variant="edge"):
+    from edgeb200.sim import EdgeSim, four_vortex_init
+    sim = EdgeSim(RES, DX, variant=variant, cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * DX,
+                  base_level=BASE_LEVEL, bfecc_clamp=True, visualize_dt=0.1)
+    u, smoke = four_vortex_init(RES, DX)
+    sim.set_velocity(*u)
+    sim.set_smoke(smoke)
+    sim.proj.poisson(*sim.u)  # run_edge.py:557 projection of the initial field
+    return sim
+
+
+class EventTimers:
+    """CUDA-event phase timers with the reference SimpleTimer's names."""
+
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.open = {}
+        self.done = []
+
+    def start(self, k):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.open[k] = e
+
+    def stop(self, k, skip=0):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.done.append((k, self.open.pop(k), e))
+
+    def totals(self):
+        self.torch.cuda.synchronize()
+        out = {}
+        for k, a, b in self.done:
+            out[k] = out.get(k, 0.0) + a.elapsed_time(b)
+        return out
+
+
+def instrumented_step(sim):
+    """One step with CUDA events around every kernel family (outside the timed
+    region).  Returns {stage: ms} and the two solves' iteration counts."""
+    import torch
+
+    from edgeb200 import ops
+    evs = []
+
+    def mark(name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        evs.append((name, e))
+
+    dx = sim.dx
+    sim.i += 1
+    j = sim.i % sim.reinit_every
+    dt = sim.next_dt()
+    if j == 0:
+        ops.reset_faces(sim.res, dx, sim.phi, sim.F)
+        for a, b in zip(sim.init_u, sim.u):
+            ops.copy(b, a)
+        ops.copy(sim.smoke, sim.init_smoke)
+    mark("start")
+    ops.advect_u_sl(sim.u, dx, 0.5 * dt, sim.tmp_u)
+    sim.u, sim.tmp_u = sim.tmp_u, sim.u
+    mark("advect_u_semi_lagrangian")
+    sim.proj.poisson(*sim.u)
+    mark("mgpcg_solve_1")
+    it1 = sim.proj.result()[0]
+    mark("_sync1")
+    sim._march(dt, j == 0)
+    mark("march_edge")
+    ops.advance_map(sim.u, dx, dt, sim.phi, sim.F)
+    mark("advance_map")
+    m = sim.map
+    ops.face_map(sim.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), sim.fpsi, sim.fcol)
+    mark("face_map")
+    ops.pullback_u(sim.init_u, dx, sim.fpsi, sim.fcol, sim.u)
+    ops.pullback_u(sim.u, dx, sim.phi, sim.F, sim.err_u, init=sim.init_u, scale=0.5)
+    ops.pullback_u(sim.err_u, dx, sim.fpsi, sim.fcol, sim.tmp_u, sub=sim.u)
+    mark("pullback_u")
+    ops.pullback_dye(sim.init_smoke, dx, sim.fpsi, sim.smoke)
+    ops.pullback_dye(sim.smoke, dx, sim.phi, sim.err_smoke, init=sim.init_smoke, scale=0.5)
+    ops.pullback_dye(sim.err_smoke, dx, sim.fpsi, sim.smoke, sub=sim.smoke, clampsrc=sim.init_smoke)
+    mark("pullback_dye")
+    ops.clamp_u(sim.tmp_u, sim.u, sim.tmp_u)
+    sim.u, sim.tmp_u = sim.tmp_u, sim.u
+    mark("clamp_u")
+    sim.proj.poisson(*sim.u)
+    mark("mgpcg_solve_2")
+    torch.cuda.synchronize()
+    it2 = sim.proj.result()[0]
+    out = {}
+    for (a, ea), (b, eb) in zip(evs[:-1], evs[1:]):
+        if b.startswith("_") or a.startswith("_") and b != "march_edge":
+            continue
+        name = b
+        if a == "_sync1":
+            name = "march_edge"
+        out[name] = out.get(name, 0.0) + ea.elapsed_time(eb)
+    return out, (it1, it2)
+
+
+def cpu_reference_steps(k, warm):
+    """The oracle substep on the host cores; returns (seconds per step, cores,
+    steps timed)."""
+    import numpy as np
+
+    from oracle import edge_oracle as O
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    u_c = np.zeros(RES + (3,), np.float32)
+    smoke = np.zeros(RES + (4,), np.float32)
+    tmp = np.zeros(RES + (4,), np.float32)
+    # init_four_vorts geometry with the long axis along x (see edgeb200.sim.four_vortex_init)
+    c45 = math.cos(math.pi / 4)
+    mid = RES[0] * DX / 2
+    perm = lambda v: [v[2], v[1], v[0]]  # noqa: E731
+    rings = [(2.e-2, (0.34, 0.34, mid), (-c45, c45, 0.), (1, 0, 0)), (-2.e-2, (0.66, 0.34, mid), (c45, c45, 0.), (0, 1, 0)),
+             (2.e-2, (0.34, 0.66, mid), (c45, c45, 0.), (0, 0, 1)), (-2.e-2, (0.66, 0.66, mid), (-c45, c45, 0.), (0, 0, 0))]
+    for q, (w, c, ex, col) in enumerate(rings):
+        n = math.sqrt(sum(v * v for v in ex))
+        ex = [v / n for v in ex]
+        tgt = smoke if q == 0 else tmp
+        if q:
+            tmp[...] = 0
+        O.add_vortex_ring(RES, DX, w, 0.15, 0.024, perm(c), perm(ex), perm((0., 0., 1.)), u_c, tgt, col, 500)
+        if q:
+            smoke += tmp
+    u = O.split_central_vector(u_c)
+    O.poisson(u, BASE_LEVEL)
+    st = O.EdgeState(RES, DX, u, smoke)
+    for _ in range(warm):
+        O.edge_substep(st, cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * DX, base_level=BASE_LEVEL)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        O.edge_substep(st, cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * DX, base_level=BASE_LEVEL)
+    return (time.perf_counter() - t0) / k, int(os.environ.get("OMP_NUM_THREADS", cores)), k
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    k = max(1, min(args.steps, args.ref_max_steps))
+    warm = min(args.warmup, 1)
+    sec, cores, k = cpu_reference_steps(k, warm)
+    v = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
+        "warmup": warm, "ms_per_step": 1000 * sec, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded four-vortex rings)",
+        "config": {"workload": "four-vortex collision 256x128x128, EDGE, CFL 0.5, reinit 12, 6-level MGPCG",
+                   "res": list(RES)},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{k} full substep(s) of the same workload after {warm} warm-up, "
+                                   f"C/OpenMP restatement of the reference kernels (Taichi is not installable)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    from edgeb200 import ops
+    sim = make_sim(args.variant)
+    for _ in range(args.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    # per-stage breakdown (outside the timed region)
+    stages, iters = instrumented_step(sim)
+    # timed region
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            sim.step()
+        e1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t[0])
+    value = world * args.steps * 1000.0 / ms_max
+    # end to end through the public API with host buffers: every step copies
+    # the velocity and dye in from pinned host memory and reads them back
+    e2e = None
+    if args.e2e_steps > 0:
+        host_u = [torch.empty(t_.shape, dtype=torch.float32, pin_memory=True) for t_ in sim.u]
+        host_s = torch.empty(sim.smoke.shape, dtype=torch.float32, pin_memory=True)
+        for h, d in zip(host_u, sim.u):
+            h.copy_(d)
+        host_s.copy_(sim.smoke)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record()
+        for _ in range(args.e2e_steps):
+            sim.set_velocity(*[h.cuda(non_blocking=True) for h in host_u])
+            sim.set_smoke(host_s.cuda(non_blocking=True))
+            sim.step()
+            for h, d in zip(host_u, sim.u):
+                h.copy_(d, non_blocking=True)
+            host_s.copy_(sim.smoke, non_blocking=True)
+        e3.record()
+        torch.cuda.synchronize()
+        t2 = torch.tensor([e2.elapsed_time(e3)], device="cuda")
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        nbytes = sum(h.numel() * 4 for h in host_u) + host_s.numel() * 4
+        e2e = {"value": world * args.e2e_steps * 1000.0 / float(t2[0]), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, cores, k = cpu_reference_steps(1, 0)
+        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "1 full substep of the same workload (first step after reinit), C/OpenMP restatement "
+                         "of the reference kernels"}
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        hbm, src = peaks()
+        # dominant HBM-bound stage: one MGPCG solve (graph of the CG loop)
+        solve_ms = stages.get("mgpcg_solve_2", 0.0)
+        it2 = max(iters[1], 0) + 1
+        mg_bytes = MG_SETUP_BYTES + it2 * MG_ITER_BYTES
+        achieved = mg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded four-vortex rings, init_four_vorts geometry)",
+            "config": {"workload": "four-vortex collision 256x128x128, EDGE, CFL 0.5, reinit 12, 6-level MGPCG, "
+                                   "BFECC clamp", "res": list(RES), "variant": args.variant,
+                       "parallelism": f"replicas x{world}", "l2": "step working set ~1.7 GB > L2 (no flush needed)"},
+            "roofline": {"kernel": "mgpcg_solve (CG loop graph, second projection of the step)", "bound": "hbm",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "algorithmic_bytes": mg_bytes, "iterations": it2, "peak_source": src},
+            "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+            "mgpcg_iters": list(iters),
+            "clocks": clk.summary(),
+            "gpu_launches": None,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="edge", choices=["edge", "ed4", "ed8"])
+    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-max-steps", type=int, default=2)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,989 @@
+// MGPCG pressure projection (sim/mgpcg.py, sim/mgpcg_solid.py) for sm_100a.
+//
+// One solve is a CUDA graph: set-up kernels, then a conditional WHILE node
+// whose body is one CG iteration, then the pressure-gradient update.  The CG
+// scalars (alpha, beta, r.r, z.r, the recentering mean) live in device memory
+// and are produced by "last block" reductions (per-block float64 partials
+// summed in block order, so results are run-to-run deterministic); the body's
+// last kernel sets the loop condition, so a solve makes no host round trip.
+//
+// Arrays: level l holds r[l], z[l] (float32, n>>l per axis); the fine level
+// also holds x, two p buffers (ping-pong, so update_p fuses into the Ap
+// stencil) and Ap.  The all-Neumann recentering (mgpcg.py:169-175) is kept as
+// a pending scalar `mean` that every reader of r[0] subtracts, and that the
+// r update folds into the stored residual.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "edge_common.cuh"
+
+using namespace edge;
+
+namespace {
+
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_NOCONV = 2, ST_NAN = 3 };
+
+struct SolveState {
+    double zTr, pAp, rTr, rsum, tol, abs_tol, rel_tol, div_sum;
+    float alpha, beta, mean, pad0;
+    int it, max_iters, status, setup;
+    int pcur, all_neumann, n_fluid, pad1;
+    unsigned int counter[8];
+};
+
+constexpr int TX = 4, TY = 8, TZ = 32;  // smoothing tile (cells), 256 threads
+
+struct Lvl {
+    int n0, n1, n2;
+    float* r;
+    float* z;
+    const int* bm;  // solid mask (level 0: the caller's; NULL: plain solver)
+};
+
+struct Ctx {  // everything a kernel needs, passed by value
+    Lvl lv[16];
+    int L;
+    int bt[6];
+    float* x;
+    float* p[2];
+    float* Ap;
+    float* div;
+    double* partials;
+    SolveState* st;
+    cudaGraphConditionalHandle cond;
+};
+
+EDGE_D bool is_fluid(const int* bm, int e) { return bm == nullptr || __ldg(bm + e) <= 0; }
+
+// mgpcg.py:100-110 num_fluid_neighbors (+ mgpcg_solid.py:113-130 solid faces)
+EDGE_D float n_fluid(const Ctx& c, const Lvl& L, int i, int j, int k) {
+    float num = 6.0f;
+    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (I[a] <= 0 && c.bt[2 * a] == 2) num -= 1.0f;
+        else if (L.bm && I[a] > 0) {
+            int e = idx3(i - (a == 0), j - (a == 1), k - (a == 2), L.n1, L.n2);
+            if (__ldg(L.bm + e) > 0) num -= 1.0f;
+        }
+        if (I[a] >= D[a] - 1 && c.bt[2 * a + 1] == 2) num -= 1.0f;
+        else if (L.bm && I[a] < D[a] - 1) {
+            int e = idx3(i + (a == 0), j + (a == 1), k + (a == 2), L.n1, L.n2);
+            if (__ldg(L.bm + e) > 0) num -= 1.0f;
+        }
+    }
+    return num;
+}
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+template <int N>
+EDGE_D void block_sum(double (&v)[N]) {
+    __shared__ double sm[N][32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < N; q++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < N; q++) sm[q][wid] = v[q];
+    __syncthreads();
+    int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < N; q++) {
+        double t = (wid == 0 && lane < nw) ? sm[q][lane] : 0.0;
+        if (wid == 0)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        v[q] = t;  // valid in thread 0
+    }
+}
+
+// Publish this block's partials; returns true in every thread of the block
+// that arrives last, after which partials[q*nblk + b] hold all blocks' sums.
+template <int N>
+EDGE_D bool last_block(const Ctx& c, int slot, double (&v)[N]) {
+    __shared__ bool am_last;
+    block_sum<N>(v);
+    int nblk = gridDim.x * gridDim.y * gridDim.z;
+    int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < N; q++) c.partials[q * nblk + b] = v[q];
+        __threadfence();
+        unsigned t = atomicAdd(&c.st->counter[slot], 1u);
+        am_last = (t == (unsigned)nblk - 1);
+    }
+    __syncthreads();
+    return am_last;
+}
+
+// Sum the published partials (fixed order: deterministic) in the last block.
+template <int N>
+EDGE_D void final_sum(const Ctx& c, int slot, double (&out)[N]) {
+    __threadfence();
+    int nblk = gridDim.x * gridDim.y * gridDim.z;
+    double v[N];
+#pragma unroll
+    for (int q = 0; q < N; q++) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(c.partials + q * nblk + b);
+        v[q] = s;
+    }
+    block_sum<N>(v);
+#pragma unroll
+    for (int q = 0; q < N; q++) out[q] = v[q];
+    if (threadIdx.x == 0) c.st->counter[slot] = 0;
+}
+
+EDGE_D bool running(const Ctx& c) { return *((volatile int*)&c.st->status) == ST_RUNNING; }
+
+// ---------------------------------------------------------------------------
+// set-up: apply_bc, divergence, solid correction, recentering mean
+// ---------------------------------------------------------------------------
+struct Faces {
+    float* u[3];
+    float* f[3];
+};
+
+// mgpcg.py:374-392 apply_bc (walls)
+__global__ void k_apply_walls(Ctx c, int nx, int ny, int nz, Faces U) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_faces(nx, ny, nz)) return;
+    FaceIdx f = face_decompose(t, nx, ny, nz);
+    int I[3] = {f.i, f.j, f.k};
+    int D[3] = {nx, ny, nz};
+    int a = f.axis;
+    if ((I[a] == 0 && c.bt[2 * a] == 2) || (I[a] == D[a] && c.bt[2 * a + 1] == 2)) U.u[a][f.e] = 0.0f;
+}
+
+// mgpcg_solid.py:344-356: solid-cell velocities on their six faces
+__global__ void k_apply_solid(int nx, int ny, int nz, const int* bm, const float* bvel, Faces U) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nx * ny * nz || bm[e] <= 0) return;
+    int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
+    float vx = bvel[3 * e], vy = bvel[3 * e + 1], vz = bvel[3 * e + 2];
+    U.u[0][idx3(i, j, k, ny, nz)] = vx;
+    U.u[0][idx3(i + 1, j, k, ny, nz)] = vx;
+    U.u[1][idx3(i, j, k, ny + 1, nz)] = vy;
+    U.u[1][idx3(i, j + 1, k, ny + 1, nz)] = vy;
+    U.u[2][idx3(i, j, k, ny, nz + 1)] = vz;
+    U.u[2][idx3(i, j, k + 1, ny, nz + 1)] = vz;
+}
+
+// mgpcg.py:394-404 divergence + init(u_div, -1) (mgpcg.py:67-75); solid:
+// mgpcg_solid.py:359-372 (fluid-only divergence, its sum and count).  With
+// rhs != NULL the right-hand side is taken from rhs instead (edge_mgpcg_solve).
+__global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, double rel_tol, int max_iters) {
+    const Lvl& L = c.lv[0];
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[3] = {0.0, 0.0, 0.0};  // sum div (fluid), fluid count, sum r
+    if (e < n) {
+        int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+        float d;
+        bool fl = is_fluid(L.bm, e);
+        if (rhs) {
+            d = -rhs[e];
+        } else if (fl) {
+            const int nx = L.n0, ny = L.n1, nz = L.n2;
+            float vl = U.u[0][idx3(i, j, k, ny, nz)], vr = U.u[0][idx3(i + 1, j, k, ny, nz)];
+            float vb = U.u[1][idx3(i, j, k, ny + 1, nz)], vt = U.u[1][idx3(i, j + 1, k, ny + 1, nz)];
+            float va = U.u[2][idx3(i, j, k, ny, nz + 1)], vc = U.u[2][idx3(i, j, k + 1, ny, nz + 1)];
+            d = vr - vl + vt - vb + vc - va;
+            (void)nx;
+        } else {
+            d = 0.0f;
+        }
+        c.div[e] = d;
+        float r = d * -1.0f;
+        L.r[e] = r;
+        c.x[e] = 0.0f;
+        c.p[0][e] = 0.0f;
+        c.p[1][e] = 0.0f;
+        if (fl) {
+            v[0] = d;
+            v[1] = 1.0;
+        }
+        v[2] = r;
+    }
+    if (last_block<3>(c, 0, v)) {
+        double s[3];
+        final_sum<3>(c, 0, s);
+        if (threadIdx.x == 0) {
+            SolveState* st = c.st;
+            st->div_sum = (double)(float)s[0];
+            st->n_fluid = (int)s[1];
+            st->rsum = s[2];
+            st->abs_tol = abs_tol;
+            st->rel_tol = rel_tol;
+            st->max_iters = max_iters;
+            st->it = 0;
+            st->status = ST_RUNNING;
+            st->setup = 1;
+            st->beta = 0.0f;
+            st->alpha = 0.0f;
+            st->pcur = 0;
+            st->mean = st->all_neumann ? (float)(s[2] / (double)n) : 0.0f;
+        }
+    }
+}
+
+// mgpcg_solid.py:374-383, 422-424: if the fluid divergence sums to > 0,
+// subtract its mean from every fluid cell; then the recentering mean.
+__global__ void k_solid_fix(Ctx c) {
+    const Lvl& L = c.lv[0];
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    SolveState* st = c.st;
+    float dsum = (float)st->div_sum;
+    bool fix = dsum > 0.0f && st->n_fluid > 0;
+    float avg = fix ? dsum / (float)st->n_fluid : 0.0f;
+    double v[1] = {0.0};
+    if (e < n) {
+        float r = L.r[e];
+        if (fix && is_fluid(L.bm, e)) {
+            float d = c.div[e] - avg;
+            c.div[e] = d;
+            r = d * -1.0f;
+            L.r[e] = r;
+        }
+        v[0] = r;
+    }
+    if (last_block<1>(c, 1, v)) {
+        double s[1];
+        final_sum<1>(c, 1, s);
+        if (threadIdx.x == 0) st->mean = st->all_neumann ? (float)(s[0] / (double)n) : 0.0f;
+    }
+}
+
+// mgpcg_solid.py:87-97 downsample_bm: coarse solid iff all 8 children solid
+__global__ void k_downsample_bm(const int* fine, int* coarse, int c0, int c1, int c2, int f1, int f2) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= c0 * c1 * c2) return;
+    int K = e % c2, J = (e / c2) % c1, I = e / (c1 * c2);
+    int all = 1;
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int q = 0; q < 2; q++)
+                if (fine[idx3(2 * I + a, 2 * J + b, 2 * K + q, f1, f2)] <= 0) all = 0;
+    coarse[e] = all;
+}
+
+// ---------------------------------------------------------------------------
+// CG vector kernels
+// ---------------------------------------------------------------------------
+// update_p (mgpcg.py:143-145) fused into compute_Ap (mgpcg.py:112-117):
+// p_new = z + beta p_old on the fly (also at the stencil neighbours), Ap,
+// and the p.Ap partials; the last block forms alpha (mgpcg.py:237-240).
+__global__ void __launch_bounds__(256) k_cg_ap(Ctx c) {
+    // The loop stops unless the iteration's last kernel completes its
+    // reduction and asks to continue: a lost reduction can never spin.
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        cudaGraphSetConditional(c.cond, 0);
+        if (c.st->it > c.st->max_iters + 8) c.st->status = ST_NOCONV;  // hard cap
+    }
+    if (!running(c)) return;
+    const Lvl& L = c.lv[0];
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    SolveState* st = c.st;
+    int pc = st->pcur;
+    const float* __restrict__ po = c.p[pc];
+    float* __restrict__ pn = c.p[pc ^ 1];
+    const float* __restrict__ z = L.z;
+    float beta = st->beta;
+    double v[1] = {0.0};
+    if (e < n) {
+        float pe = 0.0f, ape = 0.0f;
+        if (is_fluid(L.bm, e)) {
+            int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+            pe = __ldg(z + e) + beta * __ldg(po + e);
+            float nsum = 0.0f;
+            int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+            int stride[3] = {L.n1 * L.n2, L.n2, 1};
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                if (I[a] < D[a] - 1) {
+                    int q = e + stride[a];
+                    if (is_fluid(L.bm, q)) nsum += __ldg(z + q) + beta * __ldg(po + q);
+                }
+                if (I[a] > 0) {
+                    int q = e - stride[a];
+                    if (is_fluid(L.bm, q)) nsum += __ldg(z + q) + beta * __ldg(po + q);
+                }
+            }
+            ape = n_fluid(c, L, i, j, k) * pe - nsum;
+            v[0] = (double)pe * (double)ape;
+        }
+        pn[e] = pe;
+        c.Ap[e] = ape;
+    }
+    if (last_block<1>(c, 2, v)) {
+        double s[1];
+        final_sum<1>(c, 2, s);
+        if (threadIdx.x == 0) {
+            double pAp = (double)(float)s[0];
+            st->pAp = pAp;
+            st->alpha = (float)(st->zTr / (pAp + 1e-12));
+            st->pcur = pc ^ 1;
+        }
+    }
+}
+
+// update_x / update_r (mgpcg.py:133-141), r.r (mgpcg.py:247-249), the
+// convergence test (mgpcg.py:254) and the recentering sum (mgpcg.py:169-175).
+// Solid cells only take the recentering (mgpcg_solid.py:197-202).
+__global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
+    if (!running(c)) return;
+    const Lvl& L = c.lv[0];
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    SolveState* st = c.st;
+    float alpha = st->alpha, mean = st->mean;
+    const float* __restrict__ p = c.p[st->pcur];
+    double v[2] = {0.0, 0.0};
+    if (e < n) {
+        float r = L.r[e] - mean;
+        if (is_fluid(L.bm, e)) {
+            c.x[e] += alpha * __ldg(p + e);
+            r -= alpha * __ldg(c.Ap + e);
+            v[0] = (double)r * (double)r;
+        }
+        L.r[e] = r;
+        v[1] = r;
+    }
+    if (last_block<2>(c, 3, v)) {
+        double s[2];
+        final_sum<2>(c, 3, s);
+        if (threadIdx.x == 0) {
+            double rTr = (double)(float)s[0];
+            st->rTr = rTr;
+            st->rsum = s[1];
+            st->mean = st->all_neumann ? (float)(s[1] / (double)n) : 0.0f;
+            if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
+            else if (rTr < st->tol) st->status = ST_CONVERGED;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle (mgpcg.py:177-195)
+// ---------------------------------------------------------------------------
+// One red-black Gauss-Seidel sweep (mgpcg.py:160-167) of level l on a
+// TX x TY x TZ tile, in shared memory with a 2-cell halo: the first colour
+// is updated on the tile plus a 1-cell rim, the second on the tile.
+//   FIRST : z starts at zero (first sweep after fill(0)); z is not read
+//   PROLONG: z += z[l+1][I/2] on load (mgpcg.py:155-158)
+//   ZR    : also accumulate z.(r-mean) over fluid cells (level 0) and run the
+//           end-of-iteration logic (beta, iteration count, loop condition)
+template <bool FIRST, bool PROLONG, bool ZR>
+__global__ void __launch_bounds__(256) k_sweep(Ctx c, int l, int phase0) {
+    constexpr int RX = TX + 4, RY = TY + 4, RZ = TZ + 4;
+    __shared__ float zs[RX * RY * RZ];
+    __shared__ float rs[RX * RY * RZ];
+    __shared__ unsigned char fs[RX * RY * RZ];  // 1 = fluid cell inside the grid
+    if (!running(c)) {
+        if (ZR && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0)
+            cudaGraphSetConditional(c.cond, 0);
+        return;
+    }
+    const Lvl& L = c.lv[l];
+    const float mean = l == 0 ? c.st->mean : 0.0f;
+    const int i0 = blockIdx.z * TX - 2, j0 = blockIdx.y * TY - 2, k0 = blockIdx.x * TZ - 2;
+    // load region
+    for (int s = threadIdx.x; s < RX * RY * RZ; s += blockDim.x) {
+        int kk = s % RZ, jj = (s / RZ) % RY, ii = s / (RZ * RY);
+        int i = i0 + ii, j = j0 + jj, k = k0 + kk;
+        float zv = 0.0f, rv = 0.0f;
+        unsigned char fl = 0;
+        if (i >= 0 && i < L.n0 && j >= 0 && j < L.n1 && k >= 0 && k < L.n2) {
+            int e = idx3(i, j, k, L.n1, L.n2);
+            fl = is_fluid(L.bm, e) ? 1 : 0;
+            rv = __ldg(L.r + e) - mean;
+            if (!FIRST) zv = L.z[e];
+            if (PROLONG) {
+                const Lvl& C = c.lv[l + 1];
+                zv += __ldg(C.z + idx3(i >> 1, j >> 1, k >> 1, C.n1, C.n2));
+            }
+        }
+        zs[s] = zv;
+        rs[s] = rv;
+        fs[s] = fl;
+    }
+    __syncthreads();
+    // two half sweeps: colour phase0 on [1, R-2], colour phase0^1 on [2, R-3]
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        int lo = h == 0 ? 1 : 2;
+        int ex = RX - 2 * lo, ey = RY - 2 * lo, ez = RZ - 2 * lo;
+        int color = phase0 ^ h;
+        for (int s = threadIdx.x; s < ex * ey * ez; s += blockDim.x) {
+            int kk = s % ez + lo, jj = (s / ez) % ey + lo, ii = s / (ez * ey) + lo;
+            int i = i0 + ii, j = j0 + jj, k = k0 + kk;
+            if (((i + j + k) & 1) != color) continue;
+            int q = (ii * RY + jj) * RZ + kk;
+            if (!fs[q]) continue;
+            if (i < 0 || i >= L.n0 || j < 0 || j >= L.n1 || k < 0 || k >= L.n2) continue;
+            float ns = 0.0f;
+            // neighbours inside the grid that are fluid (fs is 0 outside)
+            ns += fs[q + RY * RZ] ? zs[q + RY * RZ] : 0.0f;
+            ns += fs[q - RY * RZ] ? zs[q - RY * RZ] : 0.0f;
+            ns += fs[q + RZ] ? zs[q + RZ] : 0.0f;
+            ns += fs[q - RZ] ? zs[q - RZ] : 0.0f;
+            ns += fs[q + 1] ? zs[q + 1] : 0.0f;
+            ns += fs[q - 1] ? zs[q - 1] : 0.0f;
+            zs[q] = (rs[q] + ns) / n_fluid(c, L, i, j, k);
+        }
+        __syncthreads();
+    }
+    // write the tile
+    double v[1] = {0.0};
+    for (int s = threadIdx.x; s < TX * TY * TZ; s += blockDim.x) {
+        int kk = s % TZ + 2, jj = (s / TZ) % TY + 2, ii = s / (TZ * TY) + 2;
+        int i = i0 + ii, j = j0 + jj, k = k0 + kk;
+        if (i >= L.n0 || j >= L.n1 || k >= L.n2) continue;
+        int q = (ii * RY + jj) * RZ + kk;
+        L.z[idx3(i, j, k, L.n1, L.n2)] = zs[q];
+        if (ZR && fs[q]) v[0] += (double)zs[q] * (double)rs[q];
+    }
+    if (ZR) {
+        // mgpcg.py:263-275: z.r, beta, update bookkeeping, loop condition
+        if (last_block<1>(c, 4, v)) {
+            double s[1];
+            final_sum<1>(c, 4, s);
+            if (threadIdx.x == 0) {
+                SolveState* st = c.st;
+                double zTr = (double)(float)s[0];
+                if (st->setup) {
+                    st->setup = 0;
+                    st->zTr = zTr;
+                    st->beta = 0.0f;
+                    st->tol = fmax(st->abs_tol, zTr * st->rel_tol);
+                    if (st->max_iters <= 0) st->status = ST_NOCONV;
+                } else {
+                    st->beta = (float)(zTr / (st->zTr + 1e-12));
+                    st->zTr = zTr;
+                    st->it += 1;
+                    if (st->it >= st->max_iters) st->status = ST_NOCONV;
+                }
+                cudaGraphSetConditional(c.cond, st->status == ST_RUNNING ? 1u : 0u);
+            }
+        }
+    }
+}
+
+// restrict (mgpcg.py:147-153): r[l+1] = sum over the 8 children of
+// (r - A z) / (dim - 1), solid children skipped (mgpcg_solid.py:168-174)
+__global__ void __launch_bounds__(256) k_restrict(Ctx c, int l) {
+    if (!running(c)) return;
+    const Lvl& L = c.lv[l];
+    const Lvl& C = c.lv[l + 1];
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= C.n0 * C.n1 * C.n2) return;
+    const float mean = l == 0 ? c.st->mean : 0.0f;
+    int K = e % C.n2, J = (e / C.n2) % C.n1, I = e / (C.n1 * C.n2);
+    const float* __restrict__ z = L.z;
+    float acc = 0.0f;
+    int stride[3] = {L.n1 * L.n2, L.n2, 1};
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int q = 0; q < 2; q++) {
+                int i = 2 * I + a, j = 2 * J + b, k = 2 * K + q;
+                int f = idx3(i, j, k, L.n1, L.n2);
+                if (!is_fluid(L.bm, f)) continue;
+                int Ix[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+                float ns = 0.0f;
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    if (Ix[d] < D[d] - 1 && is_fluid(L.bm, f + stride[d])) ns += __ldg(z + f + stride[d]);
+                    if (Ix[d] > 0 && is_fluid(L.bm, f - stride[d])) ns += __ldg(z + f - stride[d]);
+                }
+                float res = (__ldg(L.r + f) - mean) - (n_fluid(c, L, i, j, k) * __ldg(z + f) - ns);
+                acc += res * 0.5f;
+            }
+    C.r[e] = acc;
+}
+
+// bottom smoothing (mgpcg.py:186-189): 20 red-black sweeps from z = 0 on the
+// coarsest level, one thread block, shared memory
+__global__ void __launch_bounds__(1024) k_bottom(Ctx c, int l, int iters) {
+    extern __shared__ float sh[];
+    if (!running(c)) return;
+    const Lvl& L = c.lv[l];
+    int n = L.n0 * L.n1 * L.n2;
+    float* zs = sh;
+    float* rs = sh + n;
+    const float mean = l == 0 ? c.st->mean : 0.0f;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        zs[e] = 0.0f;
+        rs[e] = __ldg(L.r + e) - mean;
+    }
+    __syncthreads();
+    int stride[3] = {L.n1 * L.n2, L.n2, 1};
+    for (int it = 0; it < iters; it++) {
+        for (int color = 0; color < 2; color++) {
+            for (int e = threadIdx.x; e < n; e += blockDim.x) {
+                int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+                if (((i + j + k) & 1) != color || !is_fluid(L.bm, e)) continue;
+                int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+                float ns = 0.0f;
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    if (I[d] < D[d] - 1 && is_fluid(L.bm, e + stride[d])) ns += zs[e + stride[d]];
+                    if (I[d] > 0 && is_fluid(L.bm, e - stride[d])) ns += zs[e - stride[d]];
+                }
+                zs[e] = (rs[e] + ns) / n_fluid(c, L, i, j, k);
+            }
+            __syncthreads();
+        }
+    }
+    for (int e = threadIdx.x; e < n; e += blockDim.x) L.z[e] = zs[e];
+}
+
+// end of the set-up V-cycle when it ran on a single level (L == 1): z.r and
+// the same bookkeeping as k_sweep<ZR>
+__global__ void k_zr_single(Ctx c) {
+    const Lvl& L = c.lv[0];
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!running(c)) {
+        if (e == 0) cudaGraphSetConditional(c.cond, 0);
+        return;
+    }
+    double v[1] = {0.0};
+    float mean = c.st->mean;
+    if (e < n && is_fluid(L.bm, e)) v[0] = (double)L.z[e] * (double)(L.r[e] - mean);
+    if (last_block<1>(c, 4, v)) {
+        double s[1];
+        final_sum<1>(c, 4, s);
+        if (threadIdx.x == 0) {
+            SolveState* st = c.st;
+            double zTr = (double)(float)s[0];
+            if (st->setup) {
+                st->setup = 0;
+                st->zTr = zTr;
+                st->beta = 0.0f;
+                st->tol = fmax(st->abs_tol, zTr * st->rel_tol);
+                if (st->max_iters <= 0) st->status = ST_NOCONV;
+            } else {
+                st->beta = (float)(zTr / (st->zTr + 1e-12));
+                st->zTr = zTr;
+                st->it += 1;
+                if (st->it >= st->max_iters) st->status = ST_NOCONV;
+            }
+            cudaGraphSetConditional(c.cond, st->status == ST_RUNNING ? 1u : 0u);
+        }
+    }
+}
+
+// mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
+// wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479)
+__global__ void k_grad_p(Ctx c, int nx, int ny, int nz, Faces U) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_faces(nx, ny, nz)) return;
+    FaceIdx f = face_decompose(t, nx, ny, nz);
+    int a = f.axis;
+    int I[3] = {f.i, f.j, f.k}, D[3] = {nx, ny, nz};
+    int hi[3] = {min(f.i, nx - 1), min(f.j, ny - 1), min(f.k, nz - 1)};
+    int lo[3] = {hi[0], hi[1], hi[2]};
+    lo[a] = max(I[a] - 1, 0);
+    float pr = c.x[idx3(hi[0], hi[1], hi[2], ny, nz)];
+    float pl = c.x[idx3(lo[0], lo[1], lo[2], ny, nz)];
+    if (I[a] - 1 < 0) pl = 0.0f;
+    if (I[a] >= D[a]) pr = 0.0f;
+    float g = pr - pl;
+    float u = U.u[a][f.e] - g;
+    if ((I[a] == 0 && c.bt[2 * a] == 2) || (I[a] == D[a] && c.bt[2 * a + 1] == 2)) u = 0.0f;
+    U.u[a][f.e] = u;
+    if (U.f[a]) U.f[a][f.e] = -g;
+}
+
+__global__ void k_copy(const float* a, float* b, int n) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) b[e] = a[e];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+inline int grid_for(long long n, int b = 256) { return (int)((n + b - 1) / b); }
+
+inline int cu(cudaError_t e) { return e == cudaSuccess ? EDGE_OK : (int)e; }
+#define CK(x)                        \
+    do {                             \
+        int _r = cu(x);              \
+        if (_r != EDGE_OK) return _r; \
+    } while (0)
+
+struct GraphKey {
+    const void* a[7];
+    double abs_tol, rel_tol;
+    int max_iters;
+    bool operator<(const GraphKey& o) const {
+        return std::tie(a[0], a[1], a[2], a[3], a[4], a[5], a[6], abs_tol, rel_tol, max_iters) <
+               std::tie(o.a[0], o.a[1], o.a[2], o.a[3], o.a[4], o.a[5], o.a[6], o.abs_tol, o.rel_tol, o.max_iters);
+    }
+};
+
+struct Solver {
+    Ctx ctx;
+    int nx, ny, nz;
+    bool solid;
+    const float* bvel;
+    int precision;
+    std::vector<void*> allocs;
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+    std::vector<cudaGraph_t> graph_defs;
+    SolveState* st_host;  // pinned
+    int max_blocks;
+};
+
+int alloc(Solver* s, void** p, size_t bytes) {
+    CK(cudaMalloc(p, bytes));
+    s->allocs.push_back(*p);
+    return EDGE_OK;
+}
+
+// The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
+void enqueue_iteration(Solver* s, cudaStream_t stream);
+
+void enqueue_vcycle(Solver* s, cudaStream_t stream, bool final_zr) {
+    Ctx& c = s->ctx;
+    int Lb = c.L - 1;
+    for (int l = 0; l < Lb; l++) {
+        const Lvl& L = c.lv[l];
+        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
+        k_sweep<true, false, false><<<g, 256, 0, stream>>>(c, l, 0);
+        k_sweep<false, false, false><<<g, 256, 0, stream>>>(c, l, 0);
+        const Lvl& C = c.lv[l + 1];
+        k_restrict<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c, l);
+    }
+    {
+        const Lvl& B = c.lv[Lb];
+        int n = B.n0 * B.n1 * B.n2;
+        k_bottom<<<1, 1024, 2 * n * sizeof(float), stream>>>(c, Lb, 20);
+    }
+    for (int l = Lb - 1; l >= 0; l--) {
+        const Lvl& L = c.lv[l];
+        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
+        k_sweep<false, true, false><<<g, 256, 0, stream>>>(c, l, 1);
+        if (l == 0 && final_zr)
+            k_sweep<false, false, true><<<g, 256, 0, stream>>>(c, l, 1);
+        else
+            k_sweep<false, false, false><<<g, 256, 0, stream>>>(c, l, 1);
+    }
+    if (Lb == 0 && final_zr) {
+        const Lvl& L = c.lv[0];
+        k_zr_single<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, stream>>>(c);
+    }
+}
+
+void enqueue_iteration(Solver* s, cudaStream_t stream) {
+    Ctx& c = s->ctx;
+    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
+    k_cg_ap<<<grid_for(n), 256, 0, stream>>>(c);
+    k_cg_xr<<<grid_for(n), 256, 0, stream>>>(c);
+    enqueue_vcycle(s, stream, true);
+}
+
+// set-up kernels of Poisson / solve, then the conditional while node, then
+// the gradient update; captured into a graph
+int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
+                cudaGraphExec_t* exec) {
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph;
+    CK(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle;
+    CK(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
+    s->ctx.cond = handle;
+    Ctx& c = s->ctx;
+    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
+    int nx = s->nx, ny = s->ny, nz = s->nz;
+    // 1) set-up
+    CK(cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    if (!rhs) {
+        k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(nx, ny, nz, c.lv[0].bm, s->bvel, U);
+    }
+    if (s->solid) {
+        for (int l = 1; l < c.L; l++) {
+            const Lvl& F = c.lv[l - 1];
+            const Lvl& C = c.lv[l];
+            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(F.bm, (int*)C.bm, C.n0, C.n1,
+                                                                                    C.n2, F.n1, F.n2);
+        }
+    }
+    CK(cudaMemsetAsync(c.st->counter, 0, sizeof(c.st->counter), cs));  // fresh reduction counters
+    k_setup_rhs<<<grid_for(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
+    if (s->solid && !rhs) k_solid_fix<<<grid_for(n), 256, 0, cs>>>(c);
+    enqueue_vcycle(s, cs, true);  // first preconditioner application + z.r + tol
+    cudaGraph_t g2;
+    CK(cudaStreamEndCapture(cs, &g2));
+    // leaf of the set-up chain
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(graph, nodes.data(), &nn));
+    cudaGraphNode_t leaf = nullptr;
+    for (auto nd : nodes) {
+        size_t nout = 0;
+        CK(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+        if (nout == 0) leaf = nd;
+    }
+    // 2) while (condition) { one CG iteration }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, graph, &leaf, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration(s, cs);
+    cudaGraph_t b2;
+    CK(cudaStreamEndCapture(cs, &b2));
+    // 3) finish
+    CK(cudaStreamBeginCaptureToGraph(cs, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
+    if (!rhs) {
+        k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(nx, ny, nz, c.lv[0].bm, s->bvel, U);
+    } else {
+        k_copy<<<grid_for(n), 256, 0, cs>>>(c.x, xout, n);
+    }
+    CK(cudaStreamEndCapture(cs, &g2));
+    int r = cu(cudaGraphInstantiate(exec, graph, 0));
+    s->graph_defs.push_back(graph);
+    cudaStreamDestroy(cs);
+    return r;
+}
+
+int run_solve(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
+              cudaStream_t stream) {
+    GraphKey key;
+    memset(&key, 0, sizeof(key));
+    key.a[0] = U.u[0]; key.a[1] = U.u[1]; key.a[2] = U.u[2];
+    key.a[3] = U.f[0]; key.a[4] = U.f[1]; key.a[5] = U.f[2];
+    key.a[6] = rhs ? (const void*)rhs : (const void*)xout;
+    key.abs_tol = abs_tol; key.rel_tol = rel_tol; key.max_iters = max_iters;
+    auto it = s->graphs.find(key);
+    cudaGraphExec_t exec;
+    if (it == s->graphs.end()) {
+        int r = build_graph(s, U, rhs, xout, abs_tol, rel_tol, max_iters, &exec);
+        if (r != EDGE_OK) return r;
+        s->graphs[key] = exec;
+    } else {
+        exec = it->second;
+    }
+    return cu(cudaGraphLaunch(exec, stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, const int* bt, const int* mask,
+                      const float* bvel, int precision) {
+    if (!handle || !bt || nx < 2 || ny < 2 || nz < 2) return EDGE_EINVAL;
+    if ((mask == nullptr) != (bvel == nullptr)) return EDGE_EINVAL;
+    if (precision != 0) return EDGE_EINVAL;
+    long long n = (long long)nx * ny * nz;
+    if (n * 3 >= (1LL << 31)) return EDGE_EINVAL;
+    int mn = std::min(nx, std::min(ny, nz));
+    int lg = 0;
+    while ((1 << (lg + 1)) <= mn) lg++;
+    int L = lg - base_level + 1;  // mgpcg.py:34
+    if (L < 1 || L > 16) return EDGE_EINVAL;
+    for (int l = 1; l < L; l++) {
+        int f = 1 << l;
+        // restrict writes r[l+1][I//2]: every level must halve exactly
+        if (nx % f || ny % f || nz % f) return EDGE_EINVAL;
+    }
+    Solver* s = new Solver();
+    s->nx = nx; s->ny = ny; s->nz = nz;
+    s->solid = mask != nullptr;
+    s->bvel = bvel;
+    s->precision = precision;
+    Ctx& c = s->ctx;
+    memset(&c, 0, sizeof(c));
+    c.L = L;
+    for (int q = 0; q < 6; q++) c.bt[q] = bt[q];
+    int r = EDGE_OK;
+    for (int l = 0; l < L && r == EDGE_OK; l++) {
+        Lvl& V = c.lv[l];
+        V.n0 = nx >> l; V.n1 = ny >> l; V.n2 = nz >> l;
+        size_t m = (size_t)V.n0 * V.n1 * V.n2;
+        r = alloc(s, (void**)&V.r, m * sizeof(float));
+        if (r == EDGE_OK) r = alloc(s, (void**)&V.z, m * sizeof(float));
+        if (r == EDGE_OK) r = cu(cudaMemset(V.z, 0, m * sizeof(float)));
+        if (s->solid) {
+            if (l == 0) V.bm = mask;
+            else if (r == EDGE_OK) r = alloc(s, (void**)&V.bm, m * sizeof(int));
+        }
+    }
+    const Lvl& B = c.lv[L - 1];
+    if ((size_t)B.n0 * B.n1 * B.n2 * 2 * sizeof(float) > 200 * 1024) r = EDGE_EINVAL;  // bottom must fit in smem
+    if (r == EDGE_OK && (size_t)B.n0 * B.n1 * B.n2 * 2 * sizeof(float) > 48 * 1024)
+        r = cu(cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.x, n * sizeof(float));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.p[0], n * sizeof(float));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.p[1], n * sizeof(float));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.Ap, n * sizeof(float));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.div, n * sizeof(float));
+    long long maxblk = std::max<long long>(grid_for(n), grid_for(n_faces(nx, ny, nz))) + 1024;
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.partials, 3 * maxblk * sizeof(double));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.st, sizeof(SolveState));
+    if (r == EDGE_OK) {
+        SolveState st;
+        memset(&st, 0, sizeof(st));
+        st.all_neumann = (bt[0] + bt[1] + bt[2] + bt[3] + bt[4] + bt[5]) == 12;
+        r = cu(cudaMemcpy(c.st, &st, sizeof(st), cudaMemcpyHostToDevice));
+    }
+    if (r == EDGE_OK) r = cu(cudaMallocHost((void**)&s->st_host, sizeof(SolveState)));
+    if (r != EDGE_OK) {
+        for (void* p : s->allocs) cudaFree(p);
+        delete s;
+        return r;
+    }
+    *handle = s;
+    return EDGE_OK;
+}
+
+int edge_mgpcg_destroy(void* handle) {
+    if (!handle) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    cudaDeviceSynchronize();
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto g : s->graph_defs) cudaGraphDestroy(g);
+    for (void* p : s->allocs) cudaFree(p);
+    cudaFreeHost(s->st_host);
+    delete s;
+    return EDGE_OK;
+}
+
+int edge_mgpcg_levels(void* handle) { return handle ? ((Solver*)handle)->ctx.L : EDGE_EINVAL; }
+
+int edge_mgpcg_poisson(void* handle, float* ux, float* uy, float* uz, float* fx, float* fy, float* fz,
+                       double abs_tol, double rel_tol, int max_iters, void* stream) {
+    if (!handle || !ux || !uy || !uz) return EDGE_EINVAL;
+    if ((fx == nullptr) != (fy == nullptr) || (fx == nullptr) != (fz == nullptr)) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    if (max_iters < 0) max_iters = s->solid ? 100 : 400;
+    Faces U = {{ux, uy, uz}, {fx, fy, fz}};
+    return run_solve(s, U, nullptr, nullptr, abs_tol, rel_tol, max_iters, (cudaStream_t)stream);
+}
+
+int edge_mgpcg_solve(void* handle, const float* b, float* x, double abs_tol, double rel_tol, int max_iters,
+                     void* stream) {
+    if (!handle || !b || !x) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    if (max_iters < 0) max_iters = s->solid ? 100 : 400;
+    Faces U = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    return run_solve(s, U, b, x, abs_tol, rel_tol, max_iters, (cudaStream_t)stream);
+}
+
+int edge_mgpcg_result(void* handle, int* iters, double* rTr, int* status, void* stream) {
+    if (!handle) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    CK(cudaMemcpyAsync(s->st_host, s->ctx.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    const SolveState& st = *s->st_host;
+    if (iters) *iters = st.it;
+    if (rTr) *rTr = st.rTr;
+    if (status)
+        *status = st.status == ST_CONVERGED ? EDGE_OK : (st.status == ST_NAN ? EDGE_ENAN : EDGE_ENOCONV);
+    return EDGE_OK;
+}
+
+int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
+    if (!handle || !r || !z) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    cudaStream_t st = (cudaStream_t)stream;
+    Ctx c = s->ctx;
+    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
+    // status = running, mean = 0, setup flag off so the z.r epilogue is inert
+    SolveState* hs = s->st_host;
+    CK(cudaMemcpyAsync(hs, c.st, sizeof(SolveState), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    hs->status = ST_RUNNING;
+    hs->mean = 0.0f;
+    hs->setup = 1;
+    hs->max_iters = 1;
+    hs->abs_tol = 0.0;
+    hs->rel_tol = 0.0;
+    CK(cudaMemcpyAsync(c.st, hs, sizeof(SolveState), cudaMemcpyHostToDevice, st));
+    k_copy<<<grid_for(n), 256, 0, st>>>(r, c.lv[0].r, n);
+    // outside a graph cudaGraphSetConditional must not be called: use a V-cycle
+    // without the z.r epilogue
+    s->ctx.cond = 0;
+    int Lb = c.L - 1;
+    for (int l = 0; l < Lb; l++) {
+        const Lvl& L = c.lv[l];
+        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
+        k_sweep<true, false, false><<<g, 256, 0, st>>>(c, l, 0);
+        k_sweep<false, false, false><<<g, 256, 0, st>>>(c, l, 0);
+        const Lvl& C = c.lv[l + 1];
+        k_restrict<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, st>>>(c, l);
+    }
+    const Lvl& B = c.lv[Lb];
+    k_bottom<<<1, 1024, 2 * B.n0 * B.n1 * B.n2 * sizeof(float), st>>>(c, Lb, 20);
+    for (int l = Lb - 1; l >= 0; l--) {
+        const Lvl& L = c.lv[l];
+        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
+        k_sweep<false, true, false><<<g, 256, 0, st>>>(c, l, 1);
+        k_sweep<false, false, false><<<g, 256, 0, st>>>(c, l, 1);
+    }
+    k_copy<<<grid_for(n), 256, 0, st>>>(c.lv[0].z, z, n);
+    return cu(cudaPeekAtLastError());
+}
+
+__global__ void k_apply_A(Ctx c, const float* p, float* Ap) {
+    const Lvl& L = c.lv[0];
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    if (!is_fluid(L.bm, e)) { Ap[e] = 0.0f; return; }
+    int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+    int stride[3] = {L.n1 * L.n2, L.n2, 1};
+    float ns = 0.0f;
+    for (int a = 0; a < 3; a++) {
+        if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += p[e + stride[a]];
+        if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
+    }
+    Ap[e] = n_fluid(c, L, i, j, k) * p[e] - ns;
+}
+
+int edge_mgpcg_apply_A(void* handle, const float* p, float* Ap, void* stream) {
+    if (!handle || !p || !Ap) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& L = s->ctx.lv[0];
+    k_apply_A<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx, p, Ap);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_get(void* handle, int which, float* dst, void* stream) {
+    if (!handle || !dst) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& L = s->ctx.lv[0];
+    size_t n = (size_t)L.n0 * L.n1 * L.n2;
+    const float* src = which == 0 ? s->ctx.div : (which == 1 ? s->ctx.x : nullptr);
+    if (!src) return EDGE_EINVAL;
+    return cu(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,232 @@
+"""The EDGE / ED4 / ED8 substep on one B200 (run_edge.py:588-712,
+run_ed4.py:402-484, run_ed8.py:365-451), on device-resident state.
+
+Differences from the reference's orchestration that do not change results:
+  * the flow-map state is ping-ponged between two buffer sets instead of being
+    marched into temporaries and copied back (hermite.py:1515-1521);
+  * right after a reinitialisation the EDGE march composes with the identity
+    map analytically instead of reading a reset map;
+  * the Hermite evaluations of psi and grad psi at the face centres, which
+    map_u_psi, map_smoke_psi and clamp_smoke_psi each recompute
+    (run_edge.py:377-505), are evaluated once per step into face buffers, and
+    the pullbacks read them (the value accumulation of the gradient
+    interpolant is the value interpolant, hermite.py:299-456);
+  * the BFECC add/scale passes (run_edge.py:675-688) are fused into the
+    pullback kernels, and copies become buffer swaps.
+"""
+import math
+
+import torch
+
+from . import _native as N
+from . import ops
+from .fields import face_shapes, zeros_cells, zeros_faces
+from .projection import Projection
+
+VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL}
+
+
+class EdgeSim:
+    def __init__(self, res, dx, variant="edge", cfl=0.5, reinit_every=12, ed_eps=None, base_level=3,
+                 bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda"):
+        if variant not in VARIANTS:
+            raise ValueError(f"variant must be one of {sorted(VARIANTS)}")
+        N.load()
+        self.res = tuple(int(n) for n in res)
+        self.dx = float(dx)
+        self.variant = variant
+        self.hv = VARIANTS[variant]
+        self.cfl = float(cfl)
+        self.reinit_every = int(reinit_every)
+        self.ed_eps = float(ed_eps) if ed_eps is not None else 0.025 * self.dx
+        self.bfecc_clamp = bool(bfecc_clamp)
+        self.visualize_dt = float(visualize_dt)
+        self.abs_tol, self.rel_tol = abs_tol, rel_tol
+        r = self.res
+        # velocity (faces) and dye (cells)
+        self.u = zeros_faces(r)
+        self.tmp_u = zeros_faces(r)
+        self.init_u = zeros_faces(r)
+        self.err_u = zeros_faces(r)
+        self.smoke = zeros_cells(r, 4)
+        self.init_smoke = zeros_cells(r, 4)
+        self.err_smoke = zeros_cells(r, 4)
+        # backward map state, two sets (ping-pong)
+        self.maps = [self._map_set() for _ in range(2)]
+        self.cur = 0
+        # forward map on the faces
+        self.phi = zeros_faces(r, 3)
+        self.F = zeros_faces(r, 3)
+        # per-step face evaluation of the backward map
+        self.fpsi = zeros_faces(r, 3)
+        self.fcol = zeros_faces(r, 3)
+        self.max_speed_dev = torch.zeros(1, dtype=torch.float32, device=device)
+        self.max_speed_host = torch.zeros(1, dtype=torch.float32).pin_memory()
+        self.proj = Projection(r, base_level=base_level)
+        self.i = -1
+        self.sub_t = 0.0
+        self.frame_idx = 0
+        self.last_dt = 0.0
+        self.last_iters = (None, None)
+
+    def _map_set(self):
+        r = self.res
+        m = {"psi": zeros_cells(r, 3), "T": [zeros_cells(r, 3) for _ in range(3)]}
+        if self.variant in ("edge", "ed8"):
+            m["dT"] = [zeros_cells(r, 3) for _ in range(3)]
+        if self.variant == "ed8":
+            m["d2T"] = [zeros_cells(r) for _ in range(3)]
+        return m
+
+    @property
+    def map(self):
+        return self.maps[self.cur]
+
+    # -- state I/O --------------------------------------------------------------
+    def set_velocity(self, u_x, u_y, u_z):
+        for d, s in zip(self.u, (u_x, u_y, u_z)):
+            d.copy_(s)
+
+    def set_smoke(self, smoke):
+        self.smoke.copy_(smoke)
+
+    # -- dt (run_edge.py:595-614) -------------------------------------------------
+    def next_dt(self):
+        ops.max_speed(self.u, self.max_speed_dev)
+        self.max_speed_host.copy_(self.max_speed_dev, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        ms = float(self.max_speed_host[0])
+        curr = self.cfl * self.dx / ms
+        if self.sub_t + curr >= self.visualize_dt:
+            curr = self.visualize_dt - self.sub_t
+            self.sub_t = 0.0
+            self.frame_idx += 1
+        elif self.sub_t + curr * 2 >= self.visualize_dt:
+            curr = (self.visualize_dt - self.sub_t) / 2
+            self.sub_t += curr
+        else:
+            self.sub_t += curr
+        return curr
+
+    # -- the substep ---------------------------------------------------------------
+    def step(self, dt=None, timers=None):
+        tm = timers if timers is not None else _NoTimer()
+        tm.start("substep")
+        tm.start("pre-advect")
+        self.i += 1
+        j = self.i % self.reinit_every
+        curr_dt = self.next_dt() if dt is None else float(dt)
+        self.last_dt = curr_dt
+        dx = self.dx
+        reinit = j == 0
+        if reinit:
+            # run_edge.py:616-625
+            ops.reset_faces(self.res, dx, self.phi, self.F)
+            for a, b in zip(self.init_u, self.u):
+                ops.copy(b, a)
+            ops.copy(self.smoke, self.init_smoke)
+        # midpoint velocity (run_edge.py:650-654)
+        ops.advect_u_sl(self.u, dx, 0.5 * curr_dt, self.tmp_u)
+        self.u, self.tmp_u = self.tmp_u, self.u
+        tm.stop("pre-advect")
+        self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol)
+        tm.start("advect")
+        self._march(curr_dt, reinit)
+        ops.advance_map(self.u, dx, curr_dt, self.phi, self.F)          # run_edge.py:660
+        m = self.map
+        ops.face_map(self.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), self.fpsi, self.fcol)
+        # u = (grad psi)^T u_init(psi), smoke = smoke_init(psi)        run_edge.py:669-670
+        ops.pullback_u(self.init_u, dx, self.fpsi, self.fcol, self.u)
+        ops.pullback_dye(self.init_smoke, dx, self.fpsi, self.smoke)
+        # err = 0.5*(F^T u(phi) - u_init)                             run_edge.py:671-682
+        ops.pullback_u(self.u, dx, self.phi, self.F, self.err_u, init=self.init_u, scale=0.5)
+        ops.pullback_dye(self.smoke, dx, self.phi, self.err_smoke, init=self.init_smoke, scale=0.5)
+        # u - (grad psi)^T err(psi); smoke - err(psi), clamped           run_edge.py:683-689
+        ops.pullback_u(self.err_u, dx, self.fpsi, self.fcol, self.tmp_u, sub=self.u)
+        ops.pullback_dye(self.err_smoke, dx, self.fpsi, self.smoke, sub=self.smoke, clampsrc=self.init_smoke)
+        if self.bfecc_clamp:
+            ops.clamp_u(self.tmp_u, self.u, self.tmp_u)                  # run_edge.py:690-696
+        self.u, self.tmp_u = self.tmp_u, self.u
+        tm.stop("advect")
+        self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol)
+        tm.stop("substep")
+        return curr_dt
+
+    def _march(self, dt, reinit):
+        dx, eps = self.dx, self.ed_eps
+        src, dst = self.maps[self.cur], self.maps[self.cur ^ 1]
+        if self.variant == "edge":
+            ops.march_edge(self.u, dx, dt, eps, src["psi"], src["T"], src["dT"], dst["psi"], dst["T"], dst["dT"],
+                           identity=reinit)
+        else:
+            if reinit:
+                ops.reset_cells(dx, src["psi"], src["T"], src.get("dT"), src.get("d2T"))
+            if self.variant == "ed4":
+                ops.march_ed4(self.u, dx, dt, eps, src["psi"], src["T"], dst["psi"], dst["T"])
+            else:
+                ops.march_ed8(self.u, dx, dt, eps, src["psi"], src["T"], src["dT"], src["d2T"], dst["psi"],
+                              dst["T"], dst["dT"], dst["d2T"])
+        self.cur ^= 1
+
+
+class _NoTimer:
+    def start(self, k):
+        pass
+
+    def stop(self, k, skip=0):
+        pass
+
+
+# -- initial conditions of the benchmark cases ---------------------------------------
+def four_vortex_init(res, dx, num_samples=500, device="cuda"):
+    """init_four_vorts (init_conditions.py:38-67) with the long axis along x:
+    the reference's (x, y, z) ring geometry is mapped to (z, y, x), so the rings
+    travel along x on an (nx, ny, nz) = (2N, N, N) grid.  Returns face
+    velocities (after split_central_vector) and the 4-channel dye."""
+    u_c = zeros_cells(res, 3, device)
+    smoke = zeros_cells(res, 4, device)
+    tmp = zeros_cells(res, 4, device)
+    x_off = y_off = 0.16
+    size = 0.15
+    c45 = math.cos(math.pi / 4)
+    perm = lambda v: (v[2], v[1], v[0])  # noqa: E731  reference (x,y,z) -> ours (z,y,x)
+    Lz = res[0] * dx  # long axis
+    mid = Lz / 2.0
+    rings = [
+        (2.e-2, (0.5 - x_off, 0.5 - y_off, mid), (-c45, c45, 0.), (1, 0, 0)),
+        (-2.e-2, (0.5 + x_off, 0.5 - y_off, mid), (c45, c45, 0.), (0, 1, 0)),
+        (2.e-2, (0.5 - x_off, 0.5 + y_off, mid), (c45, c45, 0.), (0, 0, 1)),
+        (-2.e-2, (0.5 + x_off, 0.5 + y_off, mid), (-c45, c45, 0.), (0, 0, 0)),
+    ]
+    for q, (w, c, ex, color) in enumerate(rings):
+        n = math.sqrt(sum(v * v for v in ex))
+        ex = tuple(v / n for v in ex)
+        target = smoke if q == 0 else tmp
+        if q > 0:
+            tmp.zero_()
+        ops.add_vortex_ring(dx, w, size, 0.024, perm(c), perm(ex), perm((0., 0., 1.)), u_c, target, color,
+                            num_samples)
+        if q > 0:
+            ops.axpy(smoke, tmp, 1.0, smoke)
+    u = zeros_faces(res, None, device)
+    ops.split_central_vector(u_c, u)
+    return u, smoke
+
+
+def leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.03, circulation=1.0, x_start=0.3, num_samples=2000,
+                  device="cuda"):
+    """Two coaxial rings along x (add_vortex_ring_and_smoke, init_conditions.py:11-36;
+    init_vorts_leapfrog geometry, init_conditions.py:70-86, with the radii,
+    core and centre of the 64x32x32 leapfrogging benchmark)."""
+    u_c = zeros_cells(res, 3, device)
+    smoke = zeros_cells(res, 4, device)
+    tmp = zeros_cells(res, 4, device)
+    gap = 0.625 * radii[0]
+    for q, (rad, col) in enumerate(zip(radii, ((1., 0., 0.), (0., 0., 1.)))):
+        target = smoke if q == 0 else tmp
+        ops.add_vortex_ring(dx, circulation, rad, sigma, (x_start + q * gap, 0.5, 0.5), (0., 0., -1.), (0., 1., 0.),
+                            u_c, target, col, num_samples)
+    ops.axpy(smoke, tmp, 1.0, smoke)
+    u = zeros_faces(res, None, device)
+    ops.split_central_vector(u_c, u)
+    return u, smoke

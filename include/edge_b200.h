@@ -1,0 +1,241 @@
+/*
+ * edge_b200.h — C ABI of libedgeb200.so, the sm_100a implementation of the
+ * EDGE flow-map solver's per-step hot path.
+ *
+ * The reference (pfm-gatech/EDGE-Flow-Maps) is Python + Taichi; its "FFI" for
+ * this path is the set of Taichi kernels and solver methods the run_*.py
+ * drivers call.  Each entry point below names the reference function (file
+ * and lines inside that project) that it replaces; the Python modules under
+ * edge-flow-maps_b200/sim keep the reference's names and arguments and call
+ * these through ctypes.
+ *
+ * Conventions
+ *  - All pointers are device pointers (cudaMalloc'd or torch-owned); the
+ *    library never frees caller memory.  Solver workspaces live in an opaque
+ *    handle (edge_mgpcg_create / edge_mgpcg_destroy).
+ *  - Fields are float32, row-major (i, j, k) with k fastest.  vec3 / vec4
+ *    fields store their components last (the order of Taichi's to_numpy()).
+ *    vec4 dye fields must be 16-byte aligned.
+ *  - Face grids of an (nx, ny, nz) cell grid: u_x (nx+1, ny, nz),
+ *    u_y (nx, ny+1, nz), u_z (nx, ny, nz+1).
+ *  - `stream` is a cudaStream_t (0 = legacy default stream).  Calls are
+ *    asynchronous unless stated otherwise.
+ *  - Return value: 0 on success, a positive cudaError_t on a CUDA error, or a
+ *    negative EDGE_E* code.  No call aborts the process.
+ */
+#ifndef EDGE_B200_H
+#define EDGE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDGE_OK 0
+#define EDGE_EINVAL (-1)     /* bad sizes, null pointer, unsupported option */
+#define EDGE_EALIGN (-2)     /* misaligned pointer (vec4 fields need 16 B) */
+#define EDGE_ENOCONV (-3)    /* solver stopped at max_iters without converging */
+#define EDGE_ENAN (-4)       /* non-finite residual */
+#define EDGE_ESTALL (-5)     /* residual stalled (flexible PCG fallback taken) */
+#define EDGE_ESTATE (-6)     /* call order / handle state error */
+
+/* Hermite variants (sim/hermite.py) */
+#define EDGE_HERMITE_FD 0    /* interp_(grad_)hermite_fd_unroll, hermite.py:65-295 (ED4) */
+#define EDGE_HERMITE_GARM 1  /* interp_(grad_)hermite_garm_fd_unroll, hermite.py:299-456 (EDGE) */
+#define EDGE_HERMITE_FULL 2  /* interp_(grad_)hermite, hermite.py:460-607 (ED8) */
+
+/* ---- library ---------------------------------------------------------- */
+int edge_version(void);
+const char *edge_error_string(int code);
+
+/* ---- point samplers (util/taichi_utils.py, sim/hermite.py) ------------- */
+/* interp_u_MAC / interp_u_MAC_grad, taichi_utils.py:322-341, at n points
+ * pts (n x 3): v (n x 3), vg (n x 3, value of the grad variant), g (n x 3 x 3,
+ * rows = grad u_x, grad u_y, grad u_z). */
+int edge_points_mac(int nx, int ny, int nz, float dx, const float *ux, const float *uy, const float *uz,
+                    const float *pts, int n, float *v, float *vg, float *g, void *stream);
+/* interp_1 and sample_min_max_1 on a 4-channel cell field,
+ * taichi_utils.py:172-227 */
+int edge_points_dye(int nx, int ny, int nz, float dx, const float *smoke, const float *pts, int n, float *lin,
+                    float *mn, float *mx, void *stream);
+/* the Hermite interpolants of all three components of psi at n points:
+ * val (value-only function), gval/grad (grad function), hermite.py:65-607.
+ * dT may be NULL for EDGE_HERMITE_FD; d2T is only read by EDGE_HERMITE_FULL. */
+int edge_points_hermite(int variant, int nx, int ny, int nz, float dx, const float *psi, const float *Tx,
+                        const float *Ty, const float *Tz, const float *dTx, const float *dTy, const float *dTz,
+                        const float *d2Tx, const float *d2Ty, const float *d2Tz, const float *pts, int n,
+                        float *val, float *gval, float *grad, void *stream);
+
+/* ---- map state -------------------------------------------------------- */
+/* reset_to_identity_1/2/3, hermite.py:642-700: psi = X, T = I, dT = 0,
+ * d2T = 0 (the dT and d2T pointers may be NULL). */
+int edge_reset_cells(int nx, int ny, int nz, float dx, float *psi, float *Tx, float *Ty, float *Tz, float *dTx,
+                     float *dTy, float *dTz, float *d2Tx, float *d2Ty, float *d2Tz, void *stream);
+/* reset_to_identity, run_edge.py:306-320: phi_a = X_a, F_a = e_a on the faces */
+int edge_reset_faces(int nx, int ny, int nz, float dx, float *phix, float *phiy, float *phiz, float *Fx,
+                     float *Fy, float *Fz, void *stream);
+
+/* ---- flow-map marches -------------------------------------------------- */
+/* advect_psi_garm_ed4_fusion_unroll, hermite.py:1426-1521 (EDGE): one RK4
+ * step (-dt) of the cell centre and 4 epsilon points with Jacobians, composed
+ * with the accumulated map (psi, T, dT); results to the o* buffers, which
+ * must not alias the inputs.  If `identity` is non-zero the accumulated map
+ * is taken to be the identity (the step right after a reinitialisation) and
+ * psi/T/dT are not read. */
+int edge_march_edge(int nx, int ny, int nz, float dx, float dt, float epsilon, const float *ux, const float *uy,
+                    const float *uz, const float *psi, const float *Tx, const float *Ty, const float *Tz,
+                    const float *dTx, const float *dTy, const float *dTz, float *opsi, float *oTx, float *oTy,
+                    float *oTz, float *odTx, float *odTy, float *odTz, int identity, void *stream);
+/* advect_ps_hermite_ed4_fd_unroll, hermite.py:1375-1395 (ED4) */
+int edge_march_ed4(int nx, int ny, int nz, float dx, float dt, float epsilon, const float *ux, const float *uy,
+                   const float *uz, const float *psi, const float *Tx, const float *Ty, const float *Tz, float *opsi,
+                   float *oTx, float *oTy, float *oTz, void *stream);
+/* advect_ps_hermite_ed8, hermite.py:1290-1338 (ED8) */
+int edge_march_ed8(int nx, int ny, int nz, float dx, float dt, float epsilon, const float *ux, const float *uy,
+                   const float *uz, const float *psi, const float *Tx, const float *Ty, const float *Tz,
+                   const float *dTx, const float *dTy, const float *dTz, const float *d2Tx, const float *d2Ty,
+                   const float *d2Tz, float *opsi, float *oTx, float *oTy, float *oTz, float *odTx, float *odTy,
+                   float *odTz, float *od2Tx, float *od2Ty, float *od2Tz, void *stream);
+/* Hermite psi and Jacobian column a at every face of grid a:
+ *  - EDGE_HERMITE_FULL: split_psi_hermite, run_ed8.py:191-224
+ *  - EDGE_HERMITE_GARM / _FD: the face evaluations shared by map_u_psi
+ *    (run_edge.py:377-417, run_ed4.py:219-260) and split_to_mac
+ *    (run_edge.py:430-440, run_ed4.py:279-289).
+ * fpsi* / fcol* are vec3 face fields. */
+int edge_face_map(int variant, int nx, int ny, int nz, float dx, const float *psi, const float *Tx, const float *Ty,
+                  const float *Tz, const float *dTx, const float *dTy, const float *dTz, const float *d2Tx,
+                  const float *d2Ty, const float *d2Tz, float *fpsix, float *fpsiy, float *fpsiz, float *fcolx,
+                  float *fcoly, float *fcolz, void *stream);
+/* forward map on the faces, advance_map x3, run_edge.py:330-357 (in place) */
+int edge_advance_map(int nx, int ny, int nz, float dx, float dt, const float *ux, const float *uy, const float *uz,
+                     float *phix, float *phiy, float *phiz, float *Fx, float *Fy, float *Fz, void *stream);
+
+/* ---- velocity / dye transport ------------------------------------------ */
+/* advect_u_semi_lagrangian, hermite.py:1578-1621 (dt as passed; the driver
+ * passes 0.5*dt).  u1 must not alias u0. */
+int edge_advect_u_sl(int nx, int ny, int nz, float dx, float dt, const float *ux0, const float *uy0,
+                     const float *uz0, float *ux1, float *uy1, float *uz1, void *stream);
+/* Pull a face velocity back through face maps (position pos_a, Jacobian
+ * column col_a): out_a = col_a . u0(pos_a).  This is map_u
+ * (run_edge.py:361-373, pos = phi, col = F) and, with the face_map outputs,
+ * map_u_psi (run_edge.py:377-417).  Fused BFECC options (NULL = off):
+ *   init_*: out = scale * (out - init)         (run_edge.py:675-682)
+ *   sub_*:  out = sub - out                      (run_edge.py:685-687) */
+int edge_pullback_u(int nx, int ny, int nz, float dx, const float *ux0, const float *uy0, const float *uz0,
+                    const float *posx, const float *posy, const float *posz, const float *colx, const float *coly,
+                    const float *colz, const float *initx, const float *inity, const float *initz, float scale,
+                    const float *subx, const float *suby, const float *subz, float *ux1, float *uy1, float *uz1,
+                    void *stream);
+/* map_u_psi computed directly from the cell map (no face buffers),
+ * run_edge.py:377-417 (EDGE_HERMITE_GARM) / run_ed4.py:219-260 (_FD) */
+int edge_map_u_psi(int variant, int nx, int ny, int nz, float dx, const float *ux0, const float *uy0,
+                   const float *uz0, float *ux1, float *uy1, float *uz1, const float *psi, const float *Tx,
+                   const float *Ty, const float *Tz, const float *dTx, const float *dTy, const float *dTz,
+                   void *stream);
+/* Dye pullback through a face map pos_a (cell centre = mean of its six face
+ * positions): out = interp_1(smoke0, centre).  This is map_smoke
+ * (run_edge.py:421-427, pos = phi) and, with face_map outputs, map_smoke_psi
+ * (run_edge.py:444-466).  Fused options (NULL = off), applied in order:
+ *   init:     out = scale * (out - init)        (run_edge.py:678-682)
+ *   sub:      out = sub - out                   (run_edge.py:688)
+ *   clampsrc: out = clamp(out, min/max of clampsrc's 8 corners at the centre)
+ *             (clamp_smoke(_psi), run_edge.py:470-505)
+ * If `inplace_clamp` is non-zero the kernel instead clamps out's own value
+ * (clamp_smoke semantics: smoke1 = clamp(smoke1, ...)). */
+int edge_pullback_dye(int nx, int ny, int nz, float dx, const float *smoke0, const float *posx, const float *posy,
+                      const float *posz, const float *init, float scale, const float *sub, const float *clampsrc,
+                      int inplace_clamp, float *out, void *stream);
+/* map_smoke_psi / clamp_smoke_psi computed directly from the cell map,
+ * run_edge.py:444-505, run_ed4.py:293-336.  mode 0: out = map; mode 1:
+ * out = clamp(out, minmax(smoke0)). */
+int edge_smoke_psi(int variant, int mode, int nx, int ny, int nz, float dx, const float *smoke0, float *out,
+                   const float *psi, const float *Tx, const float *Ty, const float *Tz, const float *dTx,
+                   const float *dTy, const float *dTz, void *stream);
+/* clamp_u on all three face grids, run_edge.py:509-519:
+ * u2 = clamp(u, min/max of u1's six neighbours) */
+int edge_clamp_u(int nx, int ny, int nz, const float *ux, const float *uy, const float *uz, const float *u1x,
+                 const float *u1y, const float *u1z, float *u2x, float *u2y, float *u2z, void *stream);
+/* calc_max_speed, run_edge.py:296-303: max |u_centre| (>= 1e-3) into
+ * out_max (one float, device memory) */
+int edge_max_speed(int nx, int ny, int nz, const float *ux, const float *uy, const float *uz, float *out_max,
+                   void *stream);
+/* The driver's dt rule (run_edge.py:595-614) on the device: reads
+ * max_speed, updates the double state sub_t (and frame bookkeeping) and writes
+ * dt (float) and dt/2 (float).  state: double[4] = {sub_t, frame_idx,
+ * output_frame, last dt}. */
+int edge_compute_dt(const float *max_speed, float cfl, float dx, double visualize_dt, double *state, float *dt,
+                    float *half_dt, void *stream);
+/* add_fields / scale_field, taichi_utils.py:6-15: dest = f1 + a*f2 (f2 may
+ * be NULL: dest = a*f1) over n floats */
+int edge_axpy(long long n, const float *f1, const float *f2, float a, float *dest, void *stream);
+/* copy_from over n floats */
+int edge_copy(long long n, const float *src, float *dst, void *stream);
+
+/* ---- pressure projection (sim/mgpcg.py, sim/mgpcg_solid.py) ------------ */
+/* MGPCG_3 / MGPCG_Solid_3 constructors, mgpcg.py:364-371, mgpcg_solid.py:313-324.
+ * bt: boundary_types as int[6] = {x-, x+, y-, y+, z-, z+} (2 = wall).
+ * mask / bvel (device, int32 cells / vec3 cells) select the solid solver;
+ * both NULL for the plain one.  precision: 0 = float32 V-cycle (the
+ * reference), 1 = mixed (bf16 smoother storage, float32 residuals). */
+int edge_mgpcg_create(void **handle, int nx, int ny, int nz, int base_level, const int *bt, const int *mask,
+                      const float *bvel, int precision);
+int edge_mgpcg_destroy(void *handle);
+/* Poisson (mgpcg.py:440-445), Poisson_with_buffer (mgpcg.py:481-486; f* non-
+ * NULL) and MGPCG_Solid_3.Poisson (mgpcg_solid.py:418-427), in place on u.
+ * max_iters < 0 uses the reference's (400 plain, 100 solid).  The whole
+ * solve runs on the stream without host synchronisation (CUDA graph with a
+ * device-side while loop); read the outcome with edge_mgpcg_result. */
+int edge_mgpcg_poisson(void *handle, float *ux, float *uy, float *uz, float *fx, float *fy, float *fz,
+                       double abs_tol, double rel_tol, int max_iters, void *stream);
+/* Solve A x = b (A: the solver's 7-point operator) from x = 0 with the same
+ * MGPCG loop; b is not modified. */
+int edge_mgpcg_solve(void *handle, const float *b, float *x, double abs_tol, double rel_tol, int max_iters,
+                     void *stream);
+/* Outcome of the last solve (synchronises the stream): iters as the reference
+ * prints it, final r.r, status (0 converged, EDGE_ENOCONV, EDGE_ENAN). */
+int edge_mgpcg_result(void *handle, int *iters, double *rTr, int *status, void *stream);
+/* One V-cycle z = M^-1 r (apply_preconditioner, mgpcg.py:177-195) and
+ * Ap = A p (compute_Ap, mgpcg.py:112-117), for testing. */
+int edge_mgpcg_vcycle(void *handle, const float *r, float *z, void *stream);
+int edge_mgpcg_apply_A(void *handle, const float *p, float *Ap, void *stream);
+/* Copy the divergence (u_div) or pressure (p) of the last Poisson call. */
+int edge_mgpcg_get(void *handle, int which, float *dst, void *stream);
+/* Number of multigrid levels (mgpcg.py:34). */
+int edge_mgpcg_levels(void *handle);
+
+/* ---- laden particles (sim/lp.py) ---------------------------------------- */
+/* update_particles_acc, lp.py:6-29 (acc zeroed for all nmax particles) */
+int edge_lp_acc(int nx, int ny, int nz, float dx, const float *ux, const float *uy, const float *uz,
+                const float *vel, const float *pos, float *acc, int num, int nmax, float dt, float St,
+                float gravity, void *stream);
+/* update_particles_velocity, lp.py:32-70 */
+int edge_lp_velocity(const float *acc, float *vel, const float *pos, float dt, float dx, int num, float Lx,
+                     float Ly, float Lz, void *stream);
+/* calculate_velocity_diff, lp.py:73-97 */
+int edge_lp_vel_diff(int nx, int ny, int nz, float dx, const float *ux, const float *uy, const float *uz,
+                     const float *vel, float *vdiff, const float *pos, int num, float St, float density_ratio,
+                     float epiral_radius_ratio, void *stream);
+/* laden_particles_back_with_computing_particle, lp.py:100-156 (P2G drag
+ * scatter; drag fields are zeroed first) */
+int edge_lp_p2g(int nx, int ny, int nz, float dx, float *dragx, float *dragy, float *dragz, const float *vdiff,
+                const float *pos, const float *rad, int num, float laden_radius, float Lx, float Ly, float Lz,
+                void *stream);
+/* update_particles_position, lp.py:158-181 */
+int edge_lp_position(const float *vel, float *pos, float dt, int num, float Lx, float Ly, float Lz, void *stream);
+/* calculate_viscous_force, lp.py:183-219, on all three face grids */
+int edge_lp_viscous(int nx, int ny, int nz, float dx, float Re, const float *ux, const float *uy, const float *uz,
+                    float *visx, float *visy, float *visz, void *stream);
+
+/* ---- initial conditions (sim/init_conditions.py, util/taichi_utils.py) -- */
+/* add_vortex_ring_and_smoke, init_conditions.py:11-36: accumulates into u
+ * (vec3 cells) and smoke (vec4 cells); c, ex, ey, color are host float[3]. */
+int edge_add_vortex_ring(int nx, int ny, int nz, float dx, float w, float rad, float delta, const float *c,
+                         const float *ex, const float *ey, float *u, float *smoke, const float *color,
+                         int num_samples, void *stream);
+/* split_central_vector, taichi_utils.py:103-116 */
+int edge_split_central_vector(int nx, int ny, int nz, const float *vc, float *ux, float *uy, float *uz,
+                              void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDGE_B200_H */
