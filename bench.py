@@ -118,11 +118,31 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_sim(variant="edge"):
+def max_over_ranks(value, world, device):
+    """Max of a per-rank float over all ranks (the job's time is its slowest
+    rank's)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0])
+
+
+def replica_throughput(world, steps, ms_max):
+    """Whole-job steps/s of `world` independent replicas, each timing `steps`
+    steps, bounded by the slowest rank."""
+    return world * steps * 1000.0 / ms_max
+
+
+def make_sim(variant="edge", res=None):
     from edgeb200.sim import EdgeSim, four_vortex_init
-    sim = EdgeSim(RES, DX, variant=variant, cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * DX,
-                  base_level=BASE_LEVEL, bfecc_clamp=True, visualize_dt=0.1)
-    u, smoke = four_vortex_init(RES, DX)
+    res = tuple(res) if res else RES
+    dx = 1.0 / res[1]
+    base = BASE_LEVEL - (int(math.log2(RES[1])) - int(math.log2(res[1])))  # keep the coarsest level's size
+    sim = EdgeSim(res, dx, variant=variant, cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * dx,
+                  base_level=max(base, 1), bfecc_clamp=True, visualize_dt=0.1)
+    u, smoke = four_vortex_init(res, dx)
     sim.set_velocity(*u)
     sim.set_smoke(smoke)
     sim.proj.poisson(*sim.u)  # run_edge.py:557 projection of the initial field
@@ -287,7 +307,9 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     from edgeb200 import ops
-    sim = make_sim(args.variant)
+    sim = make_sim(args.variant, args.res)
+    if args.res and tuple(args.res) != RES:
+        args.no_cpu_baseline = True  # profiling runs on a smaller grid
     for _ in range(args.warmup):
         sim.step()
     torch.cuda.synchronize()
@@ -297,6 +319,8 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    from edgeb200 import ops as _ops
+    launches0 = _ops.launch_count()
     with ClockSampler(local_rank) as clk:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -307,12 +331,9 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t[0])
-    value = world * args.steps * 1000.0 / ms_max
+    launches = _ops.launch_count() - launches0
+    ms_max = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
+    value = replica_throughput(world, args.steps, ms_max)
     # end to end through the public API with host buffers: every step copies
     # the velocity and dye in from pinned host memory and reads them back
     e2e = None
@@ -337,11 +358,9 @@ def run_ours(args, rank, world, local_rank):
             host_s.copy_(sim.smoke, non_blocking=True)
         e3.record()
         torch.cuda.synchronize()
-        t2 = torch.tensor([e2.elapsed_time(e3)], device="cuda")
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        t2 = max_over_ranks(e2.elapsed_time(e3), world, "cuda")
         nbytes = sum(h.numel() * 4 for h in host_u) + host_s.numel() * 4
-        e2e = {"value": world * args.e2e_steps * 1000.0 / float(t2[0]), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+        e2e = {"value": replica_throughput(world, args.e2e_steps, t2), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -372,7 +391,7 @@ def run_ours(args, rank, world, local_rank):
             "stages_ms": {k: round(v, 4) for k, v in stages.items()},
             "mgpcg_iters": list(iters),
             "clocks": clk.summary(),
-            "gpu_launches": None,
+            "gpu_launches": launches,
         }
         if e2e:
             line["e2e"] = e2e
@@ -394,6 +413,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=2)
+    ap.add_argument("--res", type=int, nargs=3, default=None,
+                    help="grid override for profiling a smaller case (not a bench line)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -37,6 +37,7 @@ struct SolveState {
     int it, max_iters, status, setup;
     int pcur, all_neumann, n_fluid, pad1;
     unsigned int counter[8];
+    unsigned long long kernels;  // kernels of this solver run so far (launch accounting)
 };
 
 constexpr int TX = 4, TY = 8, TZ = 32;  // smoothing tile (cells), 256 threads
@@ -59,7 +60,12 @@ struct Ctx {  // everything a kernel needs, passed by value
     double* partials;
     SolveState* st;
     cudaGraphConditionalHandle cond;
+    int use_cond;  // 0: kernels run outside a graph (eager mode), no loop condition
 };
+
+EDGE_D void set_cond(const Ctx& c, unsigned v) {
+    if (c.use_cond) cudaGraphSetConditional(c.cond, v);
+}
 
 EDGE_D bool is_fluid(const int* bm, int e) { return bm == nullptr || __ldg(bm + e) <= 0; }
 
@@ -150,6 +156,12 @@ EDGE_D void final_sum(const Ctx& c, int slot, double (&out)[N]) {
 
 EDGE_D bool running(const Ctx& c) { return *((volatile int*)&c.st->status) == ST_RUNNING; }
 
+// every solver kernel counts itself once (block 0, thread 0), including the
+// ones that return early once the loop has finished
+EDGE_D void count_launch(SolveState* st) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) atomicAdd(&st->kernels, 1ull);
+}
+
 // ---------------------------------------------------------------------------
 // set-up: apply_bc, divergence, solid correction, recentering mean
 // ---------------------------------------------------------------------------
@@ -160,6 +172,7 @@ struct Faces {
 
 // mgpcg.py:374-392 apply_bc (walls)
 __global__ void k_apply_walls(Ctx c, int nx, int ny, int nz, Faces U) {
+    count_launch(c.st);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(nx, ny, nz)) return;
     FaceIdx f = face_decompose(t, nx, ny, nz);
@@ -170,7 +183,8 @@ __global__ void k_apply_walls(Ctx c, int nx, int ny, int nz, Faces U) {
 }
 
 // mgpcg_solid.py:344-356: solid-cell velocities on their six faces
-__global__ void k_apply_solid(int nx, int ny, int nz, const int* bm, const float* bvel, Faces U) {
+__global__ void k_apply_solid(SolveState* st, int nx, int ny, int nz, const int* bm, const float* bvel, Faces U) {
+    count_launch(st);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nx * ny * nz || bm[e] <= 0) return;
     int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
@@ -187,6 +201,7 @@ __global__ void k_apply_solid(int nx, int ny, int nz, const int* bm, const float
 // mgpcg_solid.py:359-372 (fluid-only divergence, its sum and count).  With
 // rhs != NULL the right-hand side is taken from rhs instead (edge_mgpcg_solve).
 __global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, double rel_tol, int max_iters) {
+    count_launch(c.st);
     const Lvl& L = c.lv[0];
     int n = L.n0 * L.n1 * L.n2;
     int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -244,6 +259,7 @@ __global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, do
 // mgpcg_solid.py:374-383, 422-424: if the fluid divergence sums to > 0,
 // subtract its mean from every fluid cell; then the recentering mean.
 __global__ void k_solid_fix(Ctx c) {
+    count_launch(c.st);
     const Lvl& L = c.lv[0];
     int n = L.n0 * L.n1 * L.n2;
     int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,7 +286,8 @@ __global__ void k_solid_fix(Ctx c) {
 }
 
 // mgpcg_solid.py:87-97 downsample_bm: coarse solid iff all 8 children solid
-__global__ void k_downsample_bm(const int* fine, int* coarse, int c0, int c1, int c2, int f1, int f2) {
+__global__ void k_downsample_bm(SolveState* st, const int* fine, int* coarse, int c0, int c1, int c2, int f1, int f2) {
+    count_launch(st);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= c0 * c1 * c2) return;
     int K = e % c2, J = (e / c2) % c1, I = e / (c1 * c2);
@@ -289,10 +306,11 @@ __global__ void k_downsample_bm(const int* fine, int* coarse, int c0, int c1, in
 // p_new = z + beta p_old on the fly (also at the stencil neighbours), Ap,
 // and the p.Ap partials; the last block forms alpha (mgpcg.py:237-240).
 __global__ void __launch_bounds__(256) k_cg_ap(Ctx c) {
+    count_launch(c.st);
     // The loop stops unless the iteration's last kernel completes its
     // reduction and asks to continue: a lost reduction can never spin.
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        cudaGraphSetConditional(c.cond, 0);
+        set_cond(c, 0);
         if (c.st->it > c.st->max_iters + 8) c.st->status = ST_NOCONV;  // hard cap
     }
     if (!running(c)) return;
@@ -347,6 +365,7 @@ __global__ void __launch_bounds__(256) k_cg_ap(Ctx c) {
 // convergence test (mgpcg.py:254) and the recentering sum (mgpcg.py:169-175).
 // Solid cells only take the recentering (mgpcg_solid.py:197-202).
 __global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
+    count_launch(c.st);
     if (!running(c)) return;
     const Lvl& L = c.lv[0];
     int n = L.n0 * L.n1 * L.n2;
@@ -391,13 +410,13 @@ __global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
 //           end-of-iteration logic (beta, iteration count, loop condition)
 template <bool FIRST, bool PROLONG, bool ZR>
 __global__ void __launch_bounds__(256) k_sweep(Ctx c, int l, int phase0) {
+    count_launch(c.st);
     constexpr int RX = TX + 4, RY = TY + 4, RZ = TZ + 4;
     __shared__ float zs[RX * RY * RZ];
     __shared__ float rs[RX * RY * RZ];
     __shared__ unsigned char fs[RX * RY * RZ];  // 1 = fluid cell inside the grid
     if (!running(c)) {
-        if (ZR && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0)
-            cudaGraphSetConditional(c.cond, 0);
+        if (ZR && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) set_cond(c, 0);
         return;
     }
     const Lvl& L = c.lv[l];
@@ -479,7 +498,7 @@ __global__ void __launch_bounds__(256) k_sweep(Ctx c, int l, int phase0) {
                     st->it += 1;
                     if (st->it >= st->max_iters) st->status = ST_NOCONV;
                 }
-                cudaGraphSetConditional(c.cond, st->status == ST_RUNNING ? 1u : 0u);
+                set_cond(c, st->status == ST_RUNNING ? 1u : 0u);
             }
         }
     }
@@ -488,6 +507,7 @@ __global__ void __launch_bounds__(256) k_sweep(Ctx c, int l, int phase0) {
 // restrict (mgpcg.py:147-153): r[l+1] = sum over the 8 children of
 // (r - A z) / (dim - 1), solid children skipped (mgpcg_solid.py:168-174)
 __global__ void __launch_bounds__(256) k_restrict(Ctx c, int l) {
+    count_launch(c.st);
     if (!running(c)) return;
     const Lvl& L = c.lv[l];
     const Lvl& C = c.lv[l + 1];
@@ -520,6 +540,7 @@ __global__ void __launch_bounds__(256) k_restrict(Ctx c, int l) {
 // bottom smoothing (mgpcg.py:186-189): 20 red-black sweeps from z = 0 on the
 // coarsest level, one thread block, shared memory
 __global__ void __launch_bounds__(1024) k_bottom(Ctx c, int l, int iters) {
+    count_launch(c.st);
     extern __shared__ float sh[];
     if (!running(c)) return;
     const Lvl& L = c.lv[l];
@@ -556,11 +577,12 @@ __global__ void __launch_bounds__(1024) k_bottom(Ctx c, int l, int iters) {
 // end of the set-up V-cycle when it ran on a single level (L == 1): z.r and
 // the same bookkeeping as k_sweep<ZR>
 __global__ void k_zr_single(Ctx c) {
+    count_launch(c.st);
     const Lvl& L = c.lv[0];
     int n = L.n0 * L.n1 * L.n2;
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (!running(c)) {
-        if (e == 0) cudaGraphSetConditional(c.cond, 0);
+        if (e == 0) set_cond(c, 0);
         return;
     }
     double v[1] = {0.0};
@@ -584,7 +606,7 @@ __global__ void k_zr_single(Ctx c) {
                 st->it += 1;
                 if (st->it >= st->max_iters) st->status = ST_NOCONV;
             }
-            cudaGraphSetConditional(c.cond, st->status == ST_RUNNING ? 1u : 0u);
+            set_cond(c, st->status == ST_RUNNING ? 1u : 0u);
         }
     }
 }
@@ -592,6 +614,7 @@ __global__ void k_zr_single(Ctx c) {
 // mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
 // wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479)
 __global__ void k_grad_p(Ctx c, int nx, int ny, int nz, Faces U) {
+    count_launch(c.st);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(nx, ny, nz)) return;
     FaceIdx f = face_decompose(t, nx, ny, nz);
@@ -611,7 +634,8 @@ __global__ void k_grad_p(Ctx c, int nx, int ny, int nz, Faces U) {
     if (U.f[a]) U.f[a][f.e] = -g;
 }
 
-__global__ void k_copy(const float* a, float* b, int n) {
+__global__ void k_copy(SolveState* st, const float* a, float* b, int n) {
+    if (st) count_launch(st);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e < n) b[e] = a[e];
 }
@@ -710,6 +734,7 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     cudaGraphConditionalHandle handle;
     CK(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
     s->ctx.cond = handle;
+    s->ctx.use_cond = 1;
     Ctx& c = s->ctx;
     int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
     int nx = s->nx, ny = s->ny, nz = s->nz;
@@ -717,13 +742,13 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     CK(cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     if (!rhs) {
         k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(nx, ny, nz, c.lv[0].bm, s->bvel, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
     }
     if (s->solid) {
         for (int l = 1; l < c.L; l++) {
             const Lvl& F = c.lv[l - 1];
             const Lvl& C = c.lv[l];
-            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(F.bm, (int*)C.bm, C.n0, C.n1,
+            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(c.st, F.bm, (int*)C.bm, C.n0, C.n1,
                                                                                     C.n2, F.n1, F.n2);
         }
     }
@@ -761,9 +786,9 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     CK(cudaStreamBeginCaptureToGraph(cs, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     if (!rhs) {
         k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(nx, ny, nz, c.lv[0].bm, s->bvel, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
     } else {
-        k_copy<<<grid_for(n), 256, 0, cs>>>(c.x, xout, n);
+        k_copy<<<grid_for(n), 256, 0, cs>>>(c.st, c.x, xout, n);
     }
     CK(cudaStreamEndCapture(cs, &g2));
     int r = cu(cudaGraphInstantiate(exec, graph, 0));
@@ -772,8 +797,49 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     return r;
 }
 
+// The same kernels driven by a host loop (one status read per iteration, as
+// the reference does); selected with EDGE_MGPCG_EAGER=1 for profiling tools
+// that replay kernels one by one.
+int run_solve_eager(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
+                    cudaStream_t cs) {
+    s->ctx.use_cond = 0;
+    Ctx& c = s->ctx;
+    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
+    int nx = s->nx, ny = s->ny, nz = s->nz;
+    if (!rhs) {
+        k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
+    }
+    if (s->solid)
+        for (int l = 1; l < c.L; l++) {
+            const Lvl& F = c.lv[l - 1];
+            const Lvl& C = c.lv[l];
+            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(c.st, F.bm, (int*)C.bm, C.n0,
+                                                                                    C.n1, C.n2, F.n1, F.n2);
+        }
+    CK(cudaMemsetAsync(c.st->counter, 0, sizeof(c.st->counter), cs));
+    k_setup_rhs<<<grid_for(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
+    if (s->solid && !rhs) k_solid_fix<<<grid_for(n), 256, 0, cs>>>(c);
+    enqueue_vcycle(s, cs, true);
+    for (int it = 0; it <= max_iters + 8; it++) {
+        CK(cudaMemcpyAsync(&s->st_host->status, &c.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
+        CK(cudaStreamSynchronize(cs));
+        if (s->st_host->status != ST_RUNNING) break;
+        enqueue_iteration(s, cs);
+    }
+    if (!rhs) {
+        k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
+    } else {
+        k_copy<<<grid_for(n), 256, 0, cs>>>(c.st, c.x, xout, n);
+    }
+    return cu(cudaPeekAtLastError());
+}
+
 int run_solve(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
               cudaStream_t stream) {
+    static const bool eager = getenv("EDGE_MGPCG_EAGER") && getenv("EDGE_MGPCG_EAGER")[0] == '1';
+    if (eager) return run_solve_eager(s, U, rhs, xout, abs_tol, rel_tol, max_iters, stream);
     GraphKey key;
     memset(&key, 0, sizeof(key));
     key.a[0] = U.u[0]; key.a[1] = U.u[1]; key.a[2] = U.u[2];
@@ -877,6 +943,15 @@ int edge_mgpcg_destroy(void* handle) {
 
 int edge_mgpcg_levels(void* handle) { return handle ? ((Solver*)handle)->ctx.L : EDGE_EINVAL; }
 
+int edge_mgpcg_kernel_count(void* handle, long long* count, void* stream) {
+    if (!handle || !count) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    CK(cudaMemcpyAsync(s->st_host, s->ctx.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    *count = (long long)s->st_host->kernels;
+    return EDGE_OK;
+}
+
 int edge_mgpcg_poisson(void* handle, float* ux, float* uy, float* uz, float* fx, float* fy, float* fz,
                        double abs_tol, double rel_tol, int max_iters, void* stream) {
     if (!handle || !ux || !uy || !uz) return EDGE_EINVAL;
@@ -926,10 +1001,9 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
     hs->abs_tol = 0.0;
     hs->rel_tol = 0.0;
     CK(cudaMemcpyAsync(c.st, hs, sizeof(SolveState), cudaMemcpyHostToDevice, st));
-    k_copy<<<grid_for(n), 256, 0, st>>>(r, c.lv[0].r, n);
-    // outside a graph cudaGraphSetConditional must not be called: use a V-cycle
-    // without the z.r epilogue
-    s->ctx.cond = 0;
+    k_copy<<<grid_for(n), 256, 0, st>>>(nullptr, r, c.lv[0].r, n);
+    // outside a graph there is no loop condition to set
+    c.use_cond = 0;
     int Lb = c.L - 1;
     for (int l = 0; l < Lb; l++) {
         const Lvl& L = c.lv[l];
@@ -947,7 +1021,7 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
         k_sweep<false, true, false><<<g, 256, 0, st>>>(c, l, 1);
         k_sweep<false, false, false><<<g, 256, 0, st>>>(c, l, 1);
     }
-    k_copy<<<grid_for(n), 256, 0, st>>>(c.lv[0].z, z, n);
+    k_copy<<<grid_for(n), 256, 0, st>>>(nullptr, c.lv[0].z, z, n);
     return cu(cudaPeekAtLastError());
 }
 

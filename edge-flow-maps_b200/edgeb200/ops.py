@@ -14,6 +14,23 @@ from .fields import NULL, cell_dims, dims_from_faces, ptr, stream
 
 F = ctypes.c_float
 
+# kernels each entry point launches (memcpy/memset nodes are not counted)
+_KERNELS = {"edge_max_speed": 2, "edge_copy": 0}
+_launched = [0]
+
+
+def _call(name, *args):
+    N.call(name, *args)
+    _launched[0] += _KERNELS.get(name, 1)
+
+
+def launch_count():
+    """Kernels of libedgeb200.so launched so far by this process: the direct
+    entry points plus what every live MGPCG solver counted on the device
+    (synchronises)."""
+    from .projection import live_solvers
+    return _launched[0] + sum(p.kernel_count() for p in live_solvers())
+
 
 def _p3(ts):
     return [ptr(t) for t in ts] if ts is not None else [NULL, NULL, NULL]
@@ -26,7 +43,7 @@ def points_mac(u, dx, pts):
     v = torch.empty((n, 3), device=pts.device)
     vg = torch.empty((n, 3), device=pts.device)
     g = torch.empty((n, 3, 3), device=pts.device)
-    N.call("edge_points_mac", nx, ny, nz, F(dx), *_p3(u), ptr(pts), n, ptr(v), ptr(vg), ptr(g), stream())
+    _call("edge_points_mac", nx, ny, nz, F(dx), *_p3(u), ptr(pts), n, ptr(v), ptr(vg), ptr(g), stream())
     return v, vg, g
 
 
@@ -34,7 +51,7 @@ def points_dye(smoke, dx, pts):
     nx, ny, nz = cell_dims(smoke)
     n = pts.shape[0]
     out = [torch.empty((n, 4), device=pts.device) for _ in range(3)]
-    N.call("edge_points_dye", nx, ny, nz, F(dx), ptr(smoke), ptr(pts), n, *[ptr(o) for o in out], stream())
+    _call("edge_points_dye", nx, ny, nz, F(dx), ptr(smoke), ptr(pts), n, *[ptr(o) for o in out], stream())
     return out
 
 
@@ -44,7 +61,7 @@ def points_hermite(variant, psi, T, dT, d2T, dx, pts):
     val = torch.empty((n, 3), device=pts.device)
     gval = torch.empty((n, 3), device=pts.device)
     grad = torch.empty((n, 3, 3), device=pts.device)
-    N.call("edge_points_hermite", variant, nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), ptr(pts), n,
+    _call("edge_points_hermite", variant, nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), ptr(pts), n,
            ptr(val), ptr(gval), ptr(grad), stream())
     return val, gval, grad
 
@@ -52,130 +69,130 @@ def points_hermite(variant, psi, T, dT, d2T, dx, pts):
 # ---- map state ----------------------------------------------------------------
 def reset_cells(dx, psi, T, dT=None, d2T=None):
     nx, ny, nz = cell_dims(psi)
-    N.call("edge_reset_cells", nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), stream())
+    _call("edge_reset_cells", nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), stream())
 
 
 def reset_faces(res, dx, phi, Fm):
-    N.call("edge_reset_faces", *res, F(dx), *_p3(phi), *_p3(Fm), stream())
+    _call("edge_reset_faces", *res, F(dx), *_p3(phi), *_p3(Fm), stream())
 
 
 def march_edge(u, dx, dt, eps, psi, T, dT, opsi, oT, odT, identity=False):
     nx, ny, nz = cell_dims(opsi)
-    N.call("edge_march_edge", nx, ny, nz, F(dx), F(dt), F(eps), *_p3(u), ptr(psi), *_p3(T), *_p3(dT), ptr(opsi),
+    _call("edge_march_edge", nx, ny, nz, F(dx), F(dt), F(eps), *_p3(u), ptr(psi), *_p3(T), *_p3(dT), ptr(opsi),
            *_p3(oT), *_p3(odT), int(bool(identity)), stream())
 
 
 def march_ed4(u, dx, dt, eps, psi, T, opsi, oT):
     nx, ny, nz = cell_dims(opsi)
-    N.call("edge_march_ed4", nx, ny, nz, F(dx), F(dt), F(eps), *_p3(u), ptr(psi), *_p3(T), ptr(opsi), *_p3(oT),
+    _call("edge_march_ed4", nx, ny, nz, F(dx), F(dt), F(eps), *_p3(u), ptr(psi), *_p3(T), ptr(opsi), *_p3(oT),
            stream())
 
 
 def march_ed8(u, dx, dt, eps, psi, T, dT, d2T, opsi, oT, odT, od2T):
     nx, ny, nz = cell_dims(opsi)
-    N.call("edge_march_ed8", nx, ny, nz, F(dx), F(dt), F(eps), *_p3(u), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T),
+    _call("edge_march_ed8", nx, ny, nz, F(dx), F(dt), F(eps), *_p3(u), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T),
            ptr(opsi), *_p3(oT), *_p3(odT), *_p3(od2T), stream())
 
 
 def face_map(variant, dx, psi, T, dT, d2T, fpsi, fcol):
     nx, ny, nz = cell_dims(psi)
-    N.call("edge_face_map", variant, nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), *_p3(fpsi),
+    _call("edge_face_map", variant, nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), *_p3(fpsi),
            *_p3(fcol), stream())
 
 
 def advance_map(u, dx, dt, phi, Fm):
     nx, ny, nz = dims_from_faces(*u)
-    N.call("edge_advance_map", nx, ny, nz, F(dx), F(dt), *_p3(u), *_p3(phi), *_p3(Fm), stream())
+    _call("edge_advance_map", nx, ny, nz, F(dx), F(dt), *_p3(u), *_p3(phi), *_p3(Fm), stream())
 
 
 # ---- transport ----------------------------------------------------------------
 def advect_u_sl(u0, dx, dt, u1):
     nx, ny, nz = dims_from_faces(*u0)
-    N.call("edge_advect_u_sl", nx, ny, nz, F(dx), F(dt), *_p3(u0), *_p3(u1), stream())
+    _call("edge_advect_u_sl", nx, ny, nz, F(dx), F(dt), *_p3(u0), *_p3(u1), stream())
 
 
 def pullback_u(u0, dx, pos, col, out, init=None, scale=1.0, sub=None):
     nx, ny, nz = dims_from_faces(*u0)
-    N.call("edge_pullback_u", nx, ny, nz, F(dx), *_p3(u0), *_p3(pos), *_p3(col), *_p3(init), F(scale), *_p3(sub),
+    _call("edge_pullback_u", nx, ny, nz, F(dx), *_p3(u0), *_p3(pos), *_p3(col), *_p3(init), F(scale), *_p3(sub),
            *_p3(out), stream())
 
 
 def map_u_psi(variant, u0, out, dx, psi, T, dT):
     nx, ny, nz = cell_dims(psi)
-    N.call("edge_map_u_psi", variant, nx, ny, nz, F(dx), *_p3(u0), *_p3(out), ptr(psi), *_p3(T), *_p3(dT), stream())
+    _call("edge_map_u_psi", variant, nx, ny, nz, F(dx), *_p3(u0), *_p3(out), ptr(psi), *_p3(T), *_p3(dT), stream())
 
 
 def pullback_dye(smoke0, dx, pos, out, init=None, scale=1.0, sub=None, clampsrc=None, inplace_clamp=False):
     nx, ny, nz = cell_dims(out)
-    N.call("edge_pullback_dye", nx, ny, nz, F(dx), ptr(smoke0), *_p3(pos), ptr(init), F(scale), ptr(sub),
+    _call("edge_pullback_dye", nx, ny, nz, F(dx), ptr(smoke0), *_p3(pos), ptr(init), F(scale), ptr(sub),
            ptr(clampsrc), int(bool(inplace_clamp)), ptr(out), stream())
 
 
 def smoke_psi(variant, mode, smoke0, out, dx, psi, T, dT):
     nx, ny, nz = cell_dims(psi)
-    N.call("edge_smoke_psi", variant, mode, nx, ny, nz, F(dx), ptr(smoke0), ptr(out), ptr(psi), *_p3(T), *_p3(dT),
+    _call("edge_smoke_psi", variant, mode, nx, ny, nz, F(dx), ptr(smoke0), ptr(out), ptr(psi), *_p3(T), *_p3(dT),
            stream())
 
 
 def clamp_u(u, u1, u2):
     nx, ny, nz = dims_from_faces(*u)
-    N.call("edge_clamp_u", nx, ny, nz, *_p3(u), *_p3(u1), *_p3(u2), stream())
+    _call("edge_clamp_u", nx, ny, nz, *_p3(u), *_p3(u1), *_p3(u2), stream())
 
 
 def max_speed(u, out):
     nx, ny, nz = dims_from_faces(*u)
-    N.call("edge_max_speed", nx, ny, nz, *_p3(u), ptr(out), stream())
+    _call("edge_max_speed", nx, ny, nz, *_p3(u), ptr(out), stream())
 
 
 def axpy(f1, f2, a, dest):
-    N.call("edge_axpy", ctypes.c_longlong(dest.numel()), ptr(f1), ptr(f2), F(a), ptr(dest), stream())
+    _call("edge_axpy", ctypes.c_longlong(dest.numel()), ptr(f1), ptr(f2), F(a), ptr(dest), stream())
 
 
 def copy(src, dst):
     if src.numel() != dst.numel():
         raise ValueError("copy: size mismatch")
-    N.call("edge_copy", ctypes.c_longlong(dst.numel()), ptr(src), ptr(dst), stream())
+    _call("edge_copy", ctypes.c_longlong(dst.numel()), ptr(src), ptr(dst), stream())
 
 
 # ---- initial conditions ----------------------------------------------------------
 def add_vortex_ring(dx, w, rad, delta, c, ex, ey, u, smoke, color, num_samples):
     nx, ny, nz = cell_dims(u)
     f3 = lambda v: (ctypes.c_float * 3)(*[float(a) for a in v])  # noqa: E731
-    N.call("edge_add_vortex_ring", nx, ny, nz, F(dx), F(w), F(rad), F(delta), f3(c), f3(ex), f3(ey), ptr(u),
+    _call("edge_add_vortex_ring", nx, ny, nz, F(dx), F(w), F(rad), F(delta), f3(c), f3(ex), f3(ey), ptr(u),
            ptr(smoke), f3(color), int(num_samples), stream())
 
 
 def split_central_vector(vc, u):
     nx, ny, nz = cell_dims(vc)
-    N.call("edge_split_central_vector", nx, ny, nz, ptr(vc), *_p3(u), stream())
+    _call("edge_split_central_vector", nx, ny, nz, ptr(vc), *_p3(u), stream())
 
 
 # ---- particles ----------------------------------------------------------------
 def lp_acc(u, dx, vel, pos, acc, num, dt, St, gravity):
     nx, ny, nz = dims_from_faces(*u)
-    N.call("edge_lp_acc", nx, ny, nz, F(dx), *_p3(u), ptr(vel), ptr(pos), ptr(acc), int(num), int(acc.shape[0]),
+    _call("edge_lp_acc", nx, ny, nz, F(dx), *_p3(u), ptr(vel), ptr(pos), ptr(acc), int(num), int(acc.shape[0]),
            F(dt), F(St), F(gravity), stream())
 
 
 def lp_velocity(acc, vel, pos, dt, dx, num, L):
-    N.call("edge_lp_velocity", ptr(acc), ptr(vel), ptr(pos), F(dt), F(dx), int(num), *[F(v) for v in L], stream())
+    _call("edge_lp_velocity", ptr(acc), ptr(vel), ptr(pos), F(dt), F(dx), int(num), *[F(v) for v in L], stream())
 
 
 def lp_vel_diff(u, dx, vel, vdiff, pos, num, St, density_ratio, epiral_radius_ratio):
     nx, ny, nz = dims_from_faces(*u)
-    N.call("edge_lp_vel_diff", nx, ny, nz, F(dx), *_p3(u), ptr(vel), ptr(vdiff), ptr(pos), int(num), F(St),
+    _call("edge_lp_vel_diff", nx, ny, nz, F(dx), *_p3(u), ptr(vel), ptr(vdiff), ptr(pos), int(num), F(St),
            F(density_ratio), F(epiral_radius_ratio), stream())
 
 
 def lp_p2g(res, dx, drag, vdiff, pos, rad, num, laden_radius, L):
-    N.call("edge_lp_p2g", *res, F(dx), *_p3(drag), ptr(vdiff), ptr(pos), ptr(rad), int(num), F(laden_radius),
+    _call("edge_lp_p2g", *res, F(dx), *_p3(drag), ptr(vdiff), ptr(pos), ptr(rad), int(num), F(laden_radius),
            *[F(v) for v in L], stream())
 
 
 def lp_position(vel, pos, dt, num, L):
-    N.call("edge_lp_position", ptr(vel), ptr(pos), F(dt), int(num), *[F(v) for v in L], stream())
+    _call("edge_lp_position", ptr(vel), ptr(pos), F(dt), int(num), *[F(v) for v in L], stream())
 
 
 def lp_viscous(u, dx, Re, vis):
     nx, ny, nz = dims_from_faces(*u)
-    N.call("edge_lp_viscous", nx, ny, nz, F(dx), F(Re), *_p3(u), *_p3(vis), stream())
+    _call("edge_lp_viscous", nx, ny, nz, F(dx), F(Re), *_p3(u), *_p3(vis), stream())

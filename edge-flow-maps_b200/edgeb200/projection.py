@@ -4,11 +4,19 @@ solve graphs; ``poisson`` runs the whole projection on the current stream
 with no host synchronisation.
 """
 import ctypes
+import weakref
 
 import torch
 
 from . import _native as N
 from .fields import ptr, require, stream
+
+
+_LIVE = weakref.WeakSet()
+
+
+def live_solvers():
+    return [p for p in list(_LIVE) if getattr(p, "_h", None)]
 
 
 def boundary_array(boundary_types):
@@ -40,6 +48,7 @@ class Projection:
                int(precision))
         self._h = h
         self.levels = N.load().edge_mgpcg_levels(h)
+        _LIVE.add(self)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -69,6 +78,12 @@ class Projection:
         st = ctypes.c_int()
         N.call("edge_mgpcg_result", self._h, ctypes.byref(it), ctypes.byref(rtr), ctypes.byref(st), stream())
         return it.value, rtr.value, st.value
+
+    def kernel_count(self):
+        """Kernels this solver has run (counted on the device; synchronises)."""
+        c = ctypes.c_longlong()
+        N.call("edge_mgpcg_kernel_count", self._h, ctypes.byref(c), stream())
+        return c.value
 
     def vcycle(self, r, z):
         N.call("edge_mgpcg_vcycle", self._h, ptr(r), ptr(z), stream())

