@@ -1061,3 +1061,137 @@ int edge_mgpcg_get(void* handle, int which, float* dst, void* stream) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Projection without any device allocation
+// ===========================================================================
+// For callers that cannot allocate device memory while they run: code
+// embedded in another runtime that owns the whole device heap (a host
+// framework with its own caching allocator, or a CUDA-graph-replaying engine
+// that forbids cudaMalloc after warm-up), or a plugin that is handed only its
+// input/output buffers.  The solver's scratch (level pyramid, CG vectors,
+// reduction partials, loop state) lives in file-scope __device__ arrays sized
+// for at most 262144 cells (64^3); every GPU that loads the library holds them
+// (about 8 MB) until the process exits.  Solves run on the host-driven loop
+// (one status read per iteration, as the reference's solve does).
+namespace {
+
+constexpr long long kNoAllocMaxCells = 262144;  // 64^3 cells
+constexpr long long kNoAllocFloats = 7 * kNoAllocMaxCells + kNoAllocMaxCells / 2 + 4096;
+constexpr int kNoAllocMaxBlocks = 4096;
+
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
+static __device__ __align__(256) double g_noalloc_partials[3 * kNoAllocMaxBlocks];
+static __device__ __align__(256) SolveState g_noalloc_state;
+
+struct NoAllocAddrs {
+    float* scratch;
+    double* partials;
+    SolveState* state;
+    bool ready;
+};
+constexpr int kMaxDevices = 64;
+NoAllocAddrs g_noalloc_addrs[kMaxDevices];
+
+// Host code may not use the arrays' names as device addresses: resolve them
+// once per device (with that device current).
+int noalloc_addrs(NoAllocAddrs** out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return EDGE_EINVAL;
+    NoAllocAddrs& a = g_noalloc_addrs[dev];
+    if (!a.ready) {
+        CK(cudaGetSymbolAddress((void**)&a.scratch, g_noalloc_scratch));
+        CK(cudaGetSymbolAddress((void**)&a.partials, g_noalloc_partials));
+        CK(cudaGetSymbolAddress((void**)&a.state, g_noalloc_state));
+        a.ready = true;
+    }
+    *out = &a;
+    return EDGE_OK;
+}
+
+}  // namespace
+
+extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level, const int* bt, float* ux, float* uy,
+                                          float* uz, double abs_tol, double rel_tol, int max_iters, int* iters,
+                                          double* rTr, int* status, void* stream) {
+    if (!bt || !ux || !uy || !uz || nx < 2 || ny < 2 || nz < 2) return EDGE_EINVAL;
+    long long n = (long long)nx * ny * nz;
+    if (n > kNoAllocMaxCells) return EDGE_EINVAL;  // beyond the static scratch
+    int mn = std::min(nx, std::min(ny, nz));
+    int lg = 0;
+    while ((1 << (lg + 1)) <= mn) lg++;
+    int L = lg - base_level + 1;  // mgpcg.py:34
+    if (L < 1 || L > 16) return EDGE_EINVAL;
+    for (int l = 1; l < L; l++)
+        if (nx % (1 << l) || ny % (1 << l) || nz % (1 << l)) return EDGE_EINVAL;
+    if ((long long)(nx >> (L - 1)) * (ny >> (L - 1)) * (nz >> (L - 1)) * 2 * sizeof(float) > 48 * 1024)
+        return EDGE_EINVAL;  // coarsest level must fit the bottom smoother's default shared memory
+    if ((n + 255) / 256 > kNoAllocMaxBlocks) return EDGE_EINVAL;
+    if (max_iters < 0) max_iters = 400;
+    NoAllocAddrs* A = nullptr;
+    int r = noalloc_addrs(&A);
+    if (r != EDGE_OK) return r;
+    cudaStream_t cs = (cudaStream_t)stream;
+    // carve the scratch: 256-byte aligned slices
+    Solver s;  // host-side description only; its containers stay empty
+    s.nx = nx; s.ny = ny; s.nz = nz;
+    s.solid = false;
+    s.bvel = nullptr;
+    s.precision = 0;
+    s.st_host = nullptr;
+    Ctx& c = s.ctx;
+    memset(&c, 0, sizeof(c));
+    c.L = L;
+    for (int q = 0; q < 6; q++) c.bt[q] = bt[q];
+    long long off = 0;
+    auto take = [&](long long count) {
+        float* p = A->scratch + off;
+        off += (count + 63) / 64 * 64;
+        return p;
+    };
+    for (int l = 0; l < L; l++) {
+        Lvl& V = c.lv[l];
+        V.n0 = nx >> l; V.n1 = ny >> l; V.n2 = nz >> l;
+        long long m = (long long)V.n0 * V.n1 * V.n2;
+        V.r = take(m);
+        V.z = take(m);
+        V.bm = nullptr;
+    }
+    c.x = take(n);
+    c.p[0] = take(n);
+    c.p[1] = take(n);
+    c.Ap = take(n);
+    c.div = take(n);
+    if (off > kNoAllocFloats) return EDGE_EINVAL;
+    c.partials = A->partials;
+    c.st = A->state;
+    c.use_cond = 0;
+    // the loop state starts clean on every call (the arrays keep the last
+    // call's contents); x and p are zeroed by the set-up kernel
+    SolveState init;
+    memset(&init, 0, sizeof(init));
+    init.all_neumann = (bt[0] + bt[1] + bt[2] + bt[3] + bt[4] + bt[5]) == 12;
+    CK(cudaMemcpyAsync(c.st, &init, sizeof(init), cudaMemcpyHostToDevice, cs));
+    Faces U = {{ux, uy, uz}, {nullptr, nullptr, nullptr}};
+    int N = (int)n;
+    k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+    k_setup_rhs<<<grid_for(N), 256, 0, cs>>>(c, U, nullptr, abs_tol, rel_tol, max_iters);
+    enqueue_vcycle(&s, cs, true);
+    int st_status = ST_RUNNING;
+    for (int it = 0; it <= max_iters + 8; it++) {
+        CK(cudaMemcpyAsync(&st_status, &c.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
+        CK(cudaStreamSynchronize(cs));
+        if (st_status != ST_RUNNING) break;
+        enqueue_iteration(&s, cs);
+    }
+    k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+    CK(cudaPeekAtLastError());
+    SolveState fin;
+    CK(cudaMemcpyAsync(&fin, c.st, sizeof(fin), cudaMemcpyDeviceToHost, cs));
+    CK(cudaStreamSynchronize(cs));
+    if (iters) *iters = fin.it;
+    if (rTr) *rTr = fin.rTr;
+    if (status) *status = fin.status == ST_CONVERGED ? EDGE_OK : (fin.status == ST_NAN ? EDGE_ENAN : EDGE_ENOCONV);
+    return EDGE_OK;
+}

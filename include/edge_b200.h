@@ -206,6 +206,23 @@ int edge_mgpcg_levels(void *handle);
  * reference counterpart: launch accounting for benchmarks. */
 int edge_mgpcg_kernel_count(void *handle, long long *count, void *stream);
 
+/* The plain (wall-bounded, no solid mask) Poisson projection of
+ * edge_mgpcg_poisson for callers that cannot allocate device memory while
+ * they run, e.g. code hosted inside a runtime that owns the device heap or a
+ * graph-replaying engine that forbids cudaMalloc after warm-up.  It has no
+ * counterpart in the reference.  It allocates nothing: its scratch is a set
+ * of file-scope __device__ arrays sized for at most 262144 cells (64^3),
+ * about 8 MB held by every GPU that loads the library until the process
+ * exits; larger grids return EDGE_EINVAL.  The first call on a device looks
+ * up the arrays' device addresses (with that device current) and should come
+ * before any stream capture.  All calls share the arrays, so calls that
+ * overlap on the GPU (other streams, other threads) race; the call returns
+ * after the solve (it reads the loop state each iteration) with iters, r.r
+ * and status as edge_mgpcg_result reports them (each may be NULL). */
+int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level, const int *bt, float *ux, float *uy,
+                               float *uz, double abs_tol, double rel_tol, int max_iters, int *iters, double *rTr,
+                               int *status, void *stream);
+
 /* ---- laden particles (sim/lp.py) ---------------------------------------- */
 /* update_particles_acc, lp.py:6-29 (acc zeroed for all nmax particles) */
 int edge_lp_acc(int nx, int ny, int nz, float dx, const float *ux, const float *uy, const float *uz,
