@@ -564,6 +564,34 @@ __global__ void k_split_central(int nx, int ny, int nz, const float* __restrict_
     o[f.e] = 0.5f * (r + l);
 }
 
+// emit_smoke_delta (init_conditions.py:177-232): cells whose centre lies
+// within `radius` of an emitter take its colour; later emitters win, as the
+// reference's sequence of ifs does.
+struct Emitters {
+    float c[16][3];
+    float col[16][4];
+    int k;
+    float radius;
+};
+__global__ void k_emit_spheres(int nx, int ny, int nz, float dx, Emitters E, float4* smoke) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nx * ny * nz) return;
+    int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
+    float X[3];
+    cell_pos(i, j, k, dx, X);
+    for (int q = 0; q < E.k; q++) {
+        float d0 = X[0] - E.c[q][0], d1 = X[1] - E.c[q][1], d2 = X[2] - E.c[q][2];
+        if (sqrtf(d0 * d0 + d1 * d1 + d2 * d2) < E.radius)
+            smoke[e] = make_float4(E.col[q][0], E.col[q][1], E.col[q][2], E.col[q][3]);
+    }
+}
+
+// clamp_smoke_density (init_conditions.py:234-243)
+__global__ void k_clamp_max(long long n, float hi, float* x) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        if (x[e] > hi) x[e] = hi;
+}
+
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 }  // namespace
@@ -857,6 +885,29 @@ int edge_add_vortex_ring(int nx, int ny, int nz, float dx, float w, float rad, f
         R.c[a] = c[a]; R.ex[a] = ex[a]; R.ey[a] = ey[a]; R.color[a] = color[a];
     }
     k_vortex_ring<<<grid_for(nx * ny * nz), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, R, u, smoke);
+    return launch_status();
+}
+
+int edge_emit_smoke(int nx, int ny, int nz, float dx, const float* centers, const float* colors, int k, float radius,
+                    float* smoke, void* stream) {
+    if (!dims_ok(nx, ny, nz) || !centers || !colors || !smoke || k < 0 || k > 16) return EDGE_EINVAL;
+    if (!al16(smoke)) return EDGE_EALIGN;
+    Emitters E;
+    E.k = k;
+    E.radius = radius;
+    for (int q = 0; q < k; q++) {
+        for (int a = 0; a < 3; a++) E.c[q][a] = centers[3 * q + a];
+        for (int a = 0; a < 4; a++) E.col[q][a] = colors[4 * q + a];
+    }
+    k_emit_spheres<<<grid_for(nx * ny * nz), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, E, (float4*)smoke);
+    return launch_status();
+}
+
+int edge_clamp_max(long long n, float hi, float* x, void* stream) {
+    if (n < 0 || (n && !x)) return EDGE_EINVAL;
+    if (n == 0) return EDGE_OK;
+    int blocks = (int)std::min<long long>(grid_for(n), 148LL * 16);
+    k_clamp_max<<<blocks, kBlock, 0, S(stream)>>>(n, hi, x);
     return launch_status();
 }
 

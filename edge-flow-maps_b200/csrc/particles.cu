@@ -3,6 +3,8 @@
 // particle-to-grid drag scatter and the face-grid viscous Laplacian.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "edge_common.cuh"
 
 using namespace edge;
@@ -140,9 +142,29 @@ __global__ void k_lp_viscous(int nx, int ny, int nz, float dx, float nu, const f
                    s(i, j, k - 1) + -6.0f * s(i, j, k)) / dx / dx;
 }
 
+// calc_max_particle_speed (run_edge.py:256-261): max |v| over the live
+// particles, at least 1e-3 (bits of non-negative floats order as integers)
+__global__ void k_lp_init_max(float* out) { *out = 1.0e-3f; }
+__global__ void k_lp_max_speed(const float* __restrict__ vel, int num, float* out) {
+    float best = 0.0f;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < num; e += gridDim.x * blockDim.x) {
+        float a = vel[3 * e], b = vel[3 * e + 1], c = vel[3 * e + 2];
+        best = fmaxf(best, sqrtf(a * a + b * b + c * c));
+    }
+    for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(best));
+}
+
 }  // namespace
 
 extern "C" {
+
+int edge_lp_max_speed(const float* vel, int num, float* out, void* stream) {
+    if (num < 0 || !out || (num && !vel)) return EDGE_EINVAL;
+    k_lp_init_max<<<1, 1, 0, S(stream)>>>(out);
+    if (num > 0) k_lp_max_speed<<<std::min(grid_for(num), 148 * 8), 256, 0, S(stream)>>>(vel, num, out);
+    return st();
+}
 
 int edge_lp_acc(int nx, int ny, int nz, float dx, const float* ux, const float* uy, const float* uz, const float* vel,
                 const float* pos, float* acc, int num, int nmax, float dt, float St, float gravity, void* stream) {

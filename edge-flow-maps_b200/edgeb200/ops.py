@@ -15,7 +15,7 @@ from .fields import NULL, cell_dims, dims_from_faces, ptr, stream
 F = ctypes.c_float
 
 # kernels each entry point launches (memcpy/memset nodes are not counted)
-_KERNELS = {"edge_max_speed": 2, "edge_copy": 0}
+_KERNELS = {"edge_max_speed": 2, "edge_copy": 0, "edge_lp_max_speed": 2}
 _launched = [0]
 
 
@@ -162,6 +162,18 @@ def add_vortex_ring(dx, w, rad, delta, c, ex, ey, u, smoke, color, num_samples):
            ptr(smoke), f3(color), int(num_samples), stream())
 
 
+def emit_smoke(dx, centers, colors, radius, smoke):
+    nx, ny, nz = cell_dims(smoke)
+    k = len(centers)
+    c = (ctypes.c_float * (3 * k))(*[float(v) for p in centers for v in p])
+    col = (ctypes.c_float * (4 * k))(*[float(v) for p in colors for v in p])
+    _call("edge_emit_smoke", nx, ny, nz, F(dx), c, col, k, F(radius), ptr(smoke), stream())
+
+
+def clamp_max(x, hi):
+    _call("edge_clamp_max", ctypes.c_longlong(x.numel()), F(hi), ptr(x), stream())
+
+
 def split_central_vector(vc, u):
     nx, ny, nz = cell_dims(vc)
     _call("edge_split_central_vector", nx, ny, nz, ptr(vc), *_p3(u), stream())
@@ -187,6 +199,10 @@ def lp_vel_diff(u, dx, vel, vdiff, pos, num, St, density_ratio, epiral_radius_ra
 def lp_p2g(res, dx, drag, vdiff, pos, rad, num, laden_radius, L):
     _call("edge_lp_p2g", *res, F(dx), *_p3(drag), ptr(vdiff), ptr(pos), ptr(rad), int(num), F(laden_radius),
            *[F(v) for v in L], stream())
+
+
+def lp_max_speed(vel, num, out):
+    _call("edge_lp_max_speed", ptr(vel), int(num), ptr(out), stream())
 
 
 def lp_position(vel, pos, dt, num, L):

@@ -28,7 +28,8 @@ VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL}
 
 class EdgeSim:
     def __init__(self, res, dx, variant="edge", cfl=0.5, reinit_every=12, ed_eps=None, base_level=3,
-                 bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda"):
+                 bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda", solid=None,
+                 emitters=None):
         if variant not in VARIANTS:
             raise ValueError(f"variant must be one of {sorted(VARIANTS)}")
         N.load()
@@ -62,7 +63,19 @@ class EdgeSim:
         self.fcol = zeros_faces(r, 3)
         self.max_speed_dev = torch.zeros(1, dtype=torch.float32, device=device)
         self.max_speed_host = torch.zeros(1, dtype=torch.float32).pin_memory()
-        self.proj = Projection(r, base_level=base_level)
+        # solid obstacles (MGPCG_Solid_3 path, run_edge.py:166-173) and dye
+        # emitters re-injected through the forward map every step
+        # (run_edge.py:643-648)
+        self.solid = solid is not None
+        if self.solid:
+            mask, bvel = solid
+            self.proj = Projection(r, base_level=base_level, mask=mask, bvel=bvel)
+            self.abs_tol, self.rel_tol, self.max_iters = 1e-12, 0.0, 100  # mgpcg_solid.py:413-416
+        else:
+            self.proj = Projection(r, base_level=base_level)
+            self.max_iters = 400  # mgpcg.py:434-438
+        self.emitters = emitters
+        self.particles = None
         self.i = -1
         self.sub_t = 0.0
         self.frame_idx = 0
@@ -90,9 +103,26 @@ class EdgeSim:
     def set_smoke(self, smoke):
         self.smoke.copy_(smoke)
 
+    def add_particles(self, pos, vel, rad, domain, St, gravity, density_ratio, epiral_radius_ratio, Re,
+                      laden_radius):
+        """Two-way coupled laden particles (the `lp` branch of the driver,
+        run_edge.py:627-641, 662-667, 704-708; sim/lp.py).  pos, vel: (N, 3);
+        rad: (N,); domain: (Lx, Ly, Lz)."""
+        n = pos.shape[0]
+        self.particles = dict(pos=pos, vel=vel, rad=rad, acc=torch.zeros_like(vel), vdiff=torch.zeros_like(vel),
+                              num=n, L=tuple(float(v) for v in domain), St=St, gravity=gravity,
+                              density_ratio=density_ratio, erad=epiral_radius_ratio, Re=Re, lrad=laden_radius,
+                              drag=zeros_faces(self.res), vis=zeros_faces(self.res),
+                              max_dev=torch.zeros(1, dtype=torch.float32, device=pos.device))
+
     # -- dt (run_edge.py:595-614) -------------------------------------------------
     def next_dt(self):
         ops.max_speed(self.u, self.max_speed_dev)
+        if self.particles is not None:
+            P = self.particles
+            ops.lp_max_speed(P["vel"], P["num"], P["max_dev"])
+            # dt = min(CFL dx / max|u|, CFL dx / max|v_particle|)
+            torch.maximum(self.max_speed_dev, P["max_dev"], out=self.max_speed_dev)
         self.max_speed_host.copy_(self.max_speed_dev, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         ms = float(self.max_speed_host[0])
@@ -125,14 +155,30 @@ class EdgeSim:
             for a, b in zip(self.init_u, self.u):
                 ops.copy(b, a)
             ops.copy(self.smoke, self.init_smoke)
+        if self.emitters is not None:
+            centers, colors, radius = self.emitters
+            self.smoke.zero_()
+            ops.emit_smoke(dx, centers, colors, radius, self.smoke)
+            ops.pullback_dye(self.smoke, dx, self.phi, self.err_smoke)
+            ops.axpy(self.init_smoke, self.err_smoke, 1.0, self.init_smoke)
+            ops.clamp_max(self.init_smoke, 1.0)
+        if self.particles is not None:
+            self._particles_forces(curr_dt)
         # midpoint velocity (run_edge.py:650-654)
         ops.advect_u_sl(self.u, dx, 0.5 * curr_dt, self.tmp_u)
         self.u, self.tmp_u = self.tmp_u, self.u
         tm.stop("pre-advect")
-        self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol)
+        self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
         tm.start("advect")
         self._march(curr_dt, reinit)
         ops.advance_map(self.u, dx, curr_dt, self.phi, self.F)          # run_edge.py:660
+        if self.particles is not None:
+            # the forcing integrated into the map's origin velocity through the
+            # forward map (run_edge.py:662-667)
+            P = self.particles
+            ops.pullback_u(P["vis"], dx, self.phi, self.F, self.tmp_u)
+            for a, t in zip(self.init_u, self.tmp_u):
+                ops.axpy(a, t, curr_dt, a)
         m = self.map
         ops.face_map(self.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), self.fpsi, self.fcol)
         # u = (grad psi)^T u_init(psi), smoke = smoke_init(psi)        run_edge.py:669-670
@@ -148,9 +194,30 @@ class EdgeSim:
             ops.clamp_u(self.tmp_u, self.u, self.tmp_u)                  # run_edge.py:690-696
         self.u, self.tmp_u = self.tmp_u, self.u
         tm.stop("advect")
-        self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol)
+        if self.particles is not None:
+            # Poisson_with_buffer: vis receives -grad p (run_edge.py:704-708)
+            P = self.particles
+            for v in P["vis"]:
+                v.zero_()
+            self.proj.poisson(*self.u, f=P["vis"], abs_tol=self.abs_tol, rel_tol=self.rel_tol,
+                              max_iters=self.max_iters)
+        else:
+            self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
         tm.stop("substep")
         return curr_dt
+
+    def _particles_forces(self, dt):
+        """run_edge.py:627-641: G2P, particle update, P2G drag, viscous force."""
+        P = self.particles
+        dx, u = self.dx, self.u
+        ops.lp_acc(u, dx, P["vel"], P["pos"], P["acc"], P["num"], dt, P["St"], P["gravity"])
+        ops.lp_velocity(P["acc"], P["vel"], P["pos"], dt, dx, P["num"], P["L"])
+        ops.lp_vel_diff(u, dx, P["vel"], P["vdiff"], P["pos"], P["num"], P["St"], P["density_ratio"], P["erad"])
+        ops.lp_p2g(self.res, dx, P["drag"], P["vdiff"], P["pos"], P["rad"], P["num"], P["lrad"], P["L"])
+        ops.lp_position(P["vel"], P["pos"], dt, P["num"], P["L"])
+        ops.lp_viscous(u, dx, P["Re"], P["vis"])
+        for v, d in zip(P["vis"], P["drag"]):
+            ops.axpy(v, d, 1.0, v)
 
     def _march(self, dt, reinit):
         dx, eps = self.dx, self.ed_eps
@@ -230,3 +297,58 @@ def leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.03, circulation=1.0, x_st
     u = zeros_faces(res, None, device)
     ops.split_central_vector(u_c, u)
     return u, smoke
+
+
+def wedge_mask(res, dx, apex=(0.1, 0.5, 0.2), chord=1.0, half_angle_deg=15.0, aoa_deg=0.0, thickness_cells=4,
+               shell_vel=(0.6 * math.cos(math.radians(20)), 0.0, 0.6 * math.sin(math.radians(20))), device="cuda"):
+    """Solid mask and solid velocities of the delta-wing case
+    (set_boundary_mask_delta, init_conditions.py:139-167 and
+    set_boundary_mask_delta_kernel, 128-136): a triangular plate with its apex
+    at `apex`, extending `chord` downstream along x (tilted by `aoa_deg` about
+    the y axis), half angle `half_angle_deg`, `thickness_cells` cells thick,
+    plus a solid outer shell of cells carrying `shell_vel` (the inflow).  The
+    reference voxelises the triangle with trimesh (not installed); here a cell
+    is solid when its centre is within the plate's thickness and inside the
+    triangle widened by half a cell."""
+    import numpy as np
+    nx, ny, nz = res
+    idx = np.indices(res).astype(np.float64)
+    X = (idx + 0.5) * dx
+    rel = [X[0] - apex[0], X[1] - apex[1], X[2] - apex[2]]
+    a = math.radians(aoa_deg)
+    # plate coordinates: s along the chord, n normal to the plate
+    s_ = rel[0] * math.cos(a) + rel[2] * math.sin(a)
+    n_ = -rel[0] * math.sin(a) + rel[2] * math.cos(a)
+    t = math.tan(math.radians(half_angle_deg))
+    inside = (s_ >= -0.5 * dx) & (s_ <= chord * math.cos(math.radians(half_angle_deg)) + 0.5 * dx) & \
+             (np.abs(rel[1]) <= s_ * t + 0.5 * dx) & (n_ >= 0.0) & (n_ < thickness_cells * dx)
+    mask = inside.astype(np.int32)
+    bvel = np.zeros(tuple(res) + (3,), np.float32)
+    shell = np.zeros(res, bool)
+    shell[0, :, :] = shell[-1, :, :] = True
+    shell[:, 0, :] = shell[:, -1, :] = True
+    shell[:, :, 0] = shell[:, :, -1] = True
+    mask[shell] = 1
+    bvel[shell] = np.asarray(shell_vel, np.float32)
+    return (torch.from_numpy(mask).to(device), torch.from_numpy(bvel).to(device))
+
+
+def delta_emitters(offset=(0.1, 0.5, 0.25), half_angle_deg=15.0, radius=0.015):
+    """The eight dye emitters of emit_smoke_delta (init_conditions.py:177-232)."""
+    a = math.radians(half_angle_deg)
+    centers, colors = [], []
+    for d, col in ((0.25, (1, 0, 0, 0)), (0.45, (0, 1, 0, 0)), (0.65, (0, 0, 1, 0)), (0.85, (0, 0, 0, 1))):
+        x, y = math.cos(a) * d, math.sin(a) * d
+        for sy in (1, -1):
+            centers.append((x + offset[0], sy * y + offset[1], offset[2]))
+            colors.append(col)
+    return centers, colors, radius
+
+
+def uniform_flow(res, vel, device="cuda"):
+    """init_delta (init_conditions.py:170-175) followed by split_central_vector:
+    a uniform velocity on every face."""
+    u = zeros_faces(res, None, device)
+    for c in range(3):
+        u[c].fill_(float(vel[c]))
+    return u

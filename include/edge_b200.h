@@ -240,6 +240,9 @@ int edge_lp_vel_diff(int nx, int ny, int nz, float dx, const float *ux, const fl
 int edge_lp_p2g(int nx, int ny, int nz, float dx, float *dragx, float *dragy, float *dragz, const float *vdiff,
                 const float *pos, const float *rad, int num, float laden_radius, float Lx, float Ly, float Lz,
                 void *stream);
+/* calc_max_particle_speed, run_edge.py:256-261: max |v| (>= 1e-3) of the
+ * first num particles into out (one float, device memory) */
+int edge_lp_max_speed(const float *vel, int num, float *out, void *stream);
 /* update_particles_position, lp.py:158-181 */
 int edge_lp_position(const float *vel, float *pos, float dt, int num, float Lx, float Ly, float Lz, void *stream);
 /* calculate_viscous_force, lp.py:183-219, on all three face grids */
@@ -252,6 +255,13 @@ int edge_lp_viscous(int nx, int ny, int nz, float dx, float Re, const float *ux,
 int edge_add_vortex_ring(int nx, int ny, int nz, float dx, float w, float rad, float delta, const float *c,
                          const float *ex, const float *ey, float *u, float *smoke, const float *color,
                          int num_samples, void *stream);
+/* emit_smoke_delta, init_conditions.py:177-232: cells within `radius` of one
+ * of k <= 16 emitter centres (host float[k][3]) take its colour (host
+ * float[k][4]); later emitters win. */
+int edge_emit_smoke(int nx, int ny, int nz, float dx, const float *centers, const float *colors, int k,
+                    float radius, float *smoke, void *stream);
+/* clamp_smoke_density, init_conditions.py:234-243: x = min(x, hi) over n floats */
+int edge_clamp_max(long long n, float hi, float *x, void *stream);
 /* split_central_vector, taichi_utils.py:103-116 */
 int edge_split_central_vector(int nx, int ny, int nz, const float *vc, float *ux, float *uy, float *uz,
                               void *stream);

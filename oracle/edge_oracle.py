@@ -398,8 +398,17 @@ class EdgeState:
         self.init_smoke = np.zeros_like(self.smoke)
 
 
+def emit_smoke(res, dx, centers, colors, radius, smoke):
+    """init_conditions.py:177-232 emit_smoke_delta (later emitters win)."""
+    X = center_coords(res, dx).astype(np.float32)
+    for c, col in zip(centers, colors):
+        d = X - np.asarray(c, np.float32)
+        hit = np.sqrt((d * d).sum(-1)) < F32(radius)
+        smoke[hit] = np.asarray(col, np.float32)
+
+
 def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_clamp=True, dt=None,
-                 abs_tol=1e-12, rel_tol=1e-12, variant="edge"):
+                 abs_tol=1e-12, rel_tol=1e-12, variant="edge", solid=None, emitters=None, particles=None):
     """One iteration of run_edge.py:588-712 (variant "edge"), run_ed4.py:
     402-484 ("ed4") or run_ed8.py:365-451 ("ed8"); no particles, no solids,
     no frame bookkeeping: dt = CFL*dx/max_speed unless given.  Returns
@@ -411,8 +420,18 @@ def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_
     st.i += 1
     j = st.i % reinit_every
     if dt is None:
-        dt = cfl * dx / calc_max_speed(st.u)  # run_edge.py:595-614 (Python double)
+        ms = calc_max_speed(st.u)
+        if particles is not None:  # run_edge.py:598-600
+            P = particles
+            v = P["vel"][:P["num"]].astype(np.float32)
+            ms = max(ms, max(1e-3, float(np.sqrt((v * v).sum(-1)).max()) if len(v) else 1e-3))
+        dt = cfl * dx / ms  # run_edge.py:595-614 (Python double)
     dt32 = F32(dt)
+
+    def project(u, force=None):
+        if solid is not None:
+            return poisson_solid(u, solid[0], solid[1], base_level)[0]
+        return poisson(u, base_level, abs_tol=abs_tol, rel_tol=rel_tol, force=force)[0]
     if j == 0:
         # run_edge.py:616-625
         for a in range(3):
@@ -424,11 +443,34 @@ def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_
             st.dT[c][...] = 0
         st.init_u = [a.copy() for a in st.u]
         st.init_smoke = st.smoke.copy()
+    vis = None
+    if particles is not None:
+        # run_edge.py:627-641
+        P = particles
+        L = P["L"]
+        acc = lp_acc(st.u, dx, P["vel"], P["pos"], P["num"], dt32, P["St"], P["gravity"])
+        lp_velocity(acc, P["vel"], P["pos"], dt32, dx, P["num"], L)
+        vd = lp_vel_diff(st.u, dx, P["vel"], P["pos"], P["num"], P["St"], P["density_ratio"], P["erad"])
+        drag = lp_p2g(st.res, dx, vd, P["pos"], P["rad"], P["num"], P["lrad"], L)
+        lp_position(P["vel"], P["pos"], dt32, P["num"], L)
+        vis = lp_viscous(st.u, dx, P["Re"])
+        vis = [v + F32(1.0) * d for v, d in zip(vis, drag)]
+    if emitters is not None:
+        # run_edge.py:643-648
+        centers, colors, radius = emitters
+        st.smoke = np.zeros_like(st.smoke)
+        emit_smoke(st.res, dx, centers, colors, radius, st.smoke)
+        err = map_smoke(st.smoke, st.phi, dx)
+        st.init_smoke = np.minimum(st.init_smoke + F32(1.0) * err, F32(1.0))
     st.u = advect_u_semi_lagrangian(st.u, dx, F32(0.5 * dt))
-    it1 = poisson(st.u, base_level, abs_tol=abs_tol, rel_tol=rel_tol)[0]
+    it1 = project(st.u)
     st.psi, st.T, st.dT = march_edge(st.u, st.psi, st.T, st.dT, dx, dt32, eps)
     for a in range(3):
         advance_map(st.u, st.phi[a], st.F[a], a, dx, dt32)
+    if vis is not None:
+        # run_edge.py:662-667
+        tmp = map_u(vis, st.F, st.phi, dx)
+        st.init_u = [a + dt32 * t for a, t in zip(st.init_u, tmp)]
     u_new = map_u_psi(HV_GARM, st.init_u, st.psi, st.T, st.dT, dx)
     smoke_new = map_smoke_psi(HV_GARM, st.init_smoke, st.psi, st.T, st.dT, dx)
     err_u = map_u(u_new, st.F, st.phi, dx)
@@ -447,7 +489,11 @@ def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_
     else:
         st.u = err_u
     st.smoke = smoke_new
-    it2 = poisson(st.u, base_level, abs_tol=abs_tol, rel_tol=rel_tol)[0]
+    if vis is not None:
+        particles["vis"] = [np.zeros_like(a) for a in st.u]
+        it2 = project(st.u, force=particles["vis"])
+    else:
+        it2 = project(st.u)
     return dt, (it1, it2)
 
 

@@ -55,3 +55,59 @@ def test_steps_vs_oracle(variant):
             assert rel_l2(N_(sim.u[c]), st.u[c]) < 5e-4, (variant, i, c)
         assert rel_l2(N_(sim.smoke), st.smoke) < 5e-4, (variant, i)
         assert rel_l2(N_(sim.map["psi"]), st.psi) < 1e-5
+
+
+def test_solid_emitter_steps_vs_oracle():
+    """The solid-obstacle (MGPCG_Solid_3) and dye-emitter path of the delta
+    case (run_edge.py:643-648, 704-710) against the oracle's substep."""
+    from edgeb200.sim import EdgeSim, delta_emitters, uniform_flow, wedge_mask
+    res = (32, 16, 16)
+    dx = 1.0 / 16
+    mask, bvel = wedge_mask(res, dx, apex=(0.35, 0.5, 0.4), chord=0.6, thickness_cells=2)
+    u = uniform_flow(res, (0.6 * 0.94, 0.0, 0.6 * 0.34))
+    em = delta_emitters(offset=(0.3, 0.5, 0.45), radius=0.1)
+    sim = EdgeSim(res, dx, variant="edge", reinit_every=4, base_level=2, visualize_dt=1e9, solid=(mask, bvel),
+                  emitters=em)
+    sim.set_velocity(*u)
+    st = O.EdgeState(res, dx, [N_(t) for t in u], np.zeros(res + (4,), np.float32))
+    m_h, b_h = N_(mask), N_(bvel)
+    for i in range(3):
+        dt = sim.step()
+        O.edge_substep(st, reinit_every=4, base_level=2, dt=dt, solid=(m_h, b_h), emitters=em)
+        for c in range(3):
+            assert rel_l2(N_(sim.u[c]), st.u[c]) < 1e-3, (i, c)
+        assert rel_l2(N_(sim.init_smoke), st.init_smoke) < 1e-4, i
+        assert rel_l2(N_(sim.smoke), st.smoke) < 1e-3, i
+        assert sim.proj.result()[2] == 0
+
+
+def test_particle_coupled_steps_vs_oracle():
+    """Two-way laden-particle coupling (run_edge.py:627-667, 704-708)."""
+    from edgeb200.sim import EdgeSim, leapfrog_init
+    rng = np.random.default_rng(9)
+    res = (32, 16, 16)
+    dx = 1.0
+    L = tuple(r * dx for r in res)
+    u, smoke = leapfrog_init(res, 1.0 / 16, radii=(0.21, 0.28), sigma=0.06, circulation=0.2, num_samples=200)
+    n = 2000
+    pos = rng.uniform(0.2, 0.8, size=(n, 3)) * np.array(L)
+    vel = rng.normal(size=(n, 3)) * 0.05
+    rad = rng.uniform(0.005, 0.015, size=n)
+    params = dict(St=6.6e-2, gravity=0.01, density_ratio=2.0 / 3, epiral_radius_ratio=35.0, Re=5.5,
+                  laden_radius=0.01)
+    sim = EdgeSim(res, dx, variant="edge", reinit_every=3, base_level=2, visualize_dt=1e9)
+    sim.set_velocity(*u)
+    sim.set_smoke(smoke)
+    sim.add_particles(T_(pos), T_(vel), T_(rad), L, **params)
+    P = dict(pos=pos.astype(np.float32), vel=vel.astype(np.float32), rad=rad.astype(np.float32), num=n, L=L,
+             St=params["St"], gravity=params["gravity"], density_ratio=params["density_ratio"],
+             erad=params["epiral_radius_ratio"], Re=params["Re"], lrad=params["laden_radius"])
+    st = O.EdgeState(res, dx, [N_(t) for t in u], N_(smoke))
+    for i in range(3):
+        dt = sim.step()
+        O.edge_substep(st, reinit_every=3, base_level=2, dt=dt, particles=P)
+        assert rel_l2(N_(sim.particles["pos"]), P["pos"]) < 1e-5, i
+        assert rel_l2(N_(sim.particles["vel"]), P["vel"]) < 1e-4, i
+        for c in range(3):
+            assert rel_l2(N_(sim.u[c]), st.u[c]) < 1e-3, (i, c)
+            assert rel_l2(N_(sim.particles["vis"][c]), P["vis"][c]) < 1e-3, (i, c)
