@@ -135,13 +135,13 @@ def replica_throughput(world, steps, ms_max):
     return world * steps * 1000.0 / ms_max
 
 
-def make_sim(variant="edge", res=None):
+def make_sim(variant="edge", res=None, packed=False):
     from edgeb200.sim import EdgeSim, four_vortex_init
     res = tuple(res) if res else RES
     dx = 1.0 / res[1]
     base = BASE_LEVEL - (int(math.log2(RES[1])) - int(math.log2(res[1])))  # keep the coarsest level's size
     sim = EdgeSim(res, dx, variant=variant, cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * dx,
-                  base_level=max(base, 1), bfecc_clamp=True, visualize_dt=0.1)
+                  base_level=max(base, 1), bfecc_clamp=True, visualize_dt=0.1, packed=packed)
     u, smoke = four_vortex_init(res, dx)
     sim.set_velocity(*u)
     sim.set_smoke(smoke)
@@ -210,8 +210,11 @@ def instrumented_step(sim):
     mark("march_edge")
     ops.advance_map(sim.u, dx, dt, sim.phi, sim.F)
     mark("advance_map")
-    m = sim.map
-    ops.face_map(sim.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), sim.fpsi, sim.fcol)
+    if sim.packed:
+        ops.face_map_packed(sim.hv, dx, sim.pmaps[sim.cur], sim.res, sim.fpsi, sim.fcol)
+    else:
+        m = sim.map
+        ops.face_map(sim.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), sim.fpsi, sim.fcol)
     mark("face_map")
     ops.pullback_u(sim.init_u, dx, sim.fpsi, sim.fcol, sim.u)
     ops.pullback_u(sim.u, dx, sim.phi, sim.F, sim.err_u, init=sim.init_u, scale=0.5)
@@ -307,7 +310,7 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     from edgeb200 import ops
-    sim = make_sim(args.variant, args.res)
+    sim = make_sim(args.variant, args.res, packed=args.packed)
     if args.res and tuple(args.res) != RES:
         args.no_cpu_baseline = True  # profiling runs on a smaller grid
     for _ in range(args.warmup):
@@ -413,6 +416,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=2)
+    ap.add_argument("--packed", action="store_true", help="float4-plane map layout in the device driver")
     ap.add_argument("--res", type=int, nargs=3, default=None,
                     help="grid override for profiling a smaller case (not a bench line)")
     args = ap.parse_args()

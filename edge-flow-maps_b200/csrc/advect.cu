@@ -192,6 +192,185 @@ __global__ void __launch_bounds__(128) k_march_edge(Mac mac, MapF m, float dt, f
     }
 }
 
+// EDGE march on the packed layout (same algorithm as k_march_edge); output
+// planes 0-6 of `out` (n cells per plane).
+template <bool IDENT>
+__global__ void __launch_bounds__(128) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = m.n;
+    if (e >= n) return;
+    int k = e % m.nz, j = (e / m.nz) % m.ny, i = e / (m.ny * m.nz);
+    float X[3];
+    cell_pos(i, j, k, m.dx, X);
+    float dA[3][3], dB[3][3];
+    float Pc[3], Tc[3][3];
+#pragma unroll 1
+    for (int q = 0; q < 5; q++) {
+        float P[3], C[3][3];
+        for (int c = 0; c < 3; c++) {
+            P[c] = q == 0 ? X[c] : X[c] + c_ed4_off[q - 1][c] * eps;
+            for (int d = 0; d < 3; d++) C[c][d] = c == d ? 1.0f : 0.0f;
+        }
+        rk4_jac<3>(mac, P, C, -dt);
+        float T[3][3];
+        if (IDENT) {
+            for (int c = 0; c < 3; c++) {
+                float u = P[c] / m.dx - 0.5f;
+                float s = fmaxf(1.0f, fminf(u, m.hi[c]));
+                P[c] = (s + 0.5f) * m.dx;
+                for (int d = 0; d < 3; d++) T[c][d] = C[d][c];
+            }
+        } else {
+            float val[3], G[3][3];
+            hermite3p<HV_GARM, true>(m, P, val, G);
+            for (int r = 0; r < 3; r++)
+                for (int d = 0; d < 3; d++) T[r][d] = G[r][0] * C[d][0] + G[r][1] * C[d][1] + G[r][2] * C[d][2];
+            for (int c = 0; c < 3; c++) P[c] = val[c];
+        }
+        if (q == 0) {
+            for (int c = 0; c < 3; c++) {
+                Pc[c] = P[c];
+                for (int d = 0; d < 3; d++) Tc[c][d] = T[c][d];
+            }
+        } else {
+            float sx = c_ed4_off[q - 1][0], sy = c_ed4_off[q - 1][1], sz = c_ed4_off[q - 1][2];
+            for (int c = 0; c < 3; c++) {
+                float a0 = sz * T[c][1], b0 = sy * T[c][2];
+                float a1 = sz * T[c][0], b1 = sx * T[c][2];
+                float a2 = sy * T[c][0], b2 = sx * T[c][1];
+                if (q == 1) {
+                    dA[c][0] = a0; dB[c][0] = b0; dA[c][1] = a1; dB[c][1] = b1; dA[c][2] = a2; dB[c][2] = b2;
+                } else {
+                    dA[c][0] += a0; dB[c][0] += b0; dA[c][1] += a1; dB[c][1] += b1; dA[c][2] += a2; dB[c][2] += b2;
+                }
+            }
+        }
+    }
+    out[e] = make_float4(Pc[0], Pc[1], Pc[2], 0.f);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        out[(size_t)(1 + d) * n + e] = make_float4(Tc[0][d], Tc[1][d], Tc[2][d], 0.f);
+        out[(size_t)(4 + d) * n + e] = make_float4((dA[0][d] + dB[0][d]) / 8.0f / eps, (dA[1][d] + dB[1][d]) / 8.0f / eps,
+                                                   (dA[2][d] + dB[2][d]) / 8.0f / eps, 0.f);
+    }
+}
+
+// ED4 march on the packed layout; output planes 0-3.
+__global__ void __launch_bounds__(128) k_march_ed4_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = m.n;
+    if (e >= n) return;
+    int k = e % m.nz, j = (e / m.nz) % m.ny, i = e / (m.ny * m.nz);
+    float X[3];
+    cell_pos(i, j, k, m.dx, X);
+    float P[4][3];
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) {
+        float p[3];
+        for (int c = 0; c < 3; c++) p[c] = X[c] + c_ed4_off[q][c] * eps;
+        rk4_pos(mac, p, -dt);
+        float v[3];
+        hermite3p<HV_FD, false>(m, p, v, nullptr);
+        for (int c = 0; c < 3; c++) P[q][c] = v[c];
+    }
+    float o[4][3];
+    for (int c = 0; c < 3; c++) {
+        o[0][c] = (P[0][c] + P[1][c] + P[2][c] + P[3][c]) / 4.0f;
+        o[1][c] = (-P[0][c] + P[1][c] - P[2][c] + P[3][c]) / 4.0f / eps;
+        o[2][c] = (-P[0][c] + P[1][c] + P[2][c] - P[3][c]) / 4.0f / eps;
+        o[3][c] = (-P[0][c] - P[1][c] + P[2][c] + P[3][c]) / 4.0f / eps;
+    }
+    for (int q = 0; q < 4; q++) out[(size_t)q * n + e] = make_float4(o[q][0], o[q][1], o[q][2], 0.f);
+}
+
+// ED8 march on the packed layout; output planes 0-7.
+__global__ void __launch_bounds__(128) k_march_ed8_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = m.n;
+    if (e >= n) return;
+    int k = e % m.nz, j = (e / m.nz) % m.ny, i = e / (m.ny * m.nz);
+    float X[3];
+    cell_pos(i, j, k, m.dx, X);
+    float P[8][3];
+#pragma unroll 1
+    for (int q = 0; q < 8; q++) {
+        float p[3];
+        for (int c = 0; c < 3; c++) p[c] = X[c] + c_ed8_off[q][c] * eps;
+        rk4_pos(mac, p, -dt);
+        float v[3];
+        hermite3p<HV_FULL, false>(m, p, v, nullptr);
+        for (int c = 0; c < 3; c++) P[q][c] = v[c];
+    }
+    float o[8][3];
+    for (int c = 0; c < 3; c++) {
+        float a0 = P[0][c], a1 = P[1][c], a2 = P[2][c], a3 = P[3][c];
+        float a4 = P[4][c], a5 = P[5][c], a6 = P[6][c], a7 = P[7][c];
+        o[0][c] = (a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7) / 8.0f;
+        o[1][c] = (-a0 + a1 - a2 + a3 - a4 + a5 - a6 + a7) / 8.0f / eps;
+        o[2][c] = (-a0 - a1 + a2 + a3 - a4 - a5 + a6 + a7) / 8.0f / eps;
+        o[3][c] = (-a0 - a1 - a2 - a3 + a4 + a5 + a6 + a7) / 8.0f / eps;
+        o[4][c] = (a0 + a1 - a2 - a3 - a4 - a5 + a6 + a7) / 8.0f / eps / eps;
+        o[5][c] = (a0 - a1 + a2 - a3 - a4 + a5 - a6 + a7) / 8.0f / eps / eps;
+        o[6][c] = (a0 - a1 - a2 + a3 + a4 - a5 - a6 + a7) / 8.0f / eps / eps;
+        o[7][c] = (-a0 + a1 + a2 - a3 + a4 - a5 - a6 + a7) / 8.0f / eps / eps / eps;
+    }
+    for (int q = 0; q < 8; q++) out[(size_t)q * n + e] = make_float4(o[q][0], o[q][1], o[q][2], 0.f);
+}
+
+// face map on the packed layout
+template <int V>
+__global__ void __launch_bounds__(128) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
+                                                    float* fcy, float* fcz) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_faces(m.nx, m.ny, m.nz)) return;
+    FaceIdx f = face_decompose(t, m.nx, m.ny, m.nz);
+    float X[3], val[3], G[3][3];
+    face_pos(f.axis, f.i, f.j, f.k, m.dx, X);
+    hermite3p<V, true>(m, X, val, G);
+    float* fp = f.axis == 0 ? fpx : (f.axis == 1 ? fpy : fpz);
+    float* fc = f.axis == 0 ? fcx : (f.axis == 1 ? fcy : fcz);
+    for (int c = 0; c < 3; c++) {
+        fp[3 * f.e + c] = val[c];
+        fc[3 * f.e + c] = G[c][f.axis];
+    }
+}
+
+// reference layout (psi, T_c rows, dT_c, d2T_c) <-> packed planes
+__global__ void k_map_pack(int n, int planes, const float* psi, const float* Tx, const float* Ty, const float* Tz,
+                           const float* dTx, const float* dTy, const float* dTz, const float* d2x, const float* d2y,
+                           const float* d2z, float4* out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    out[e] = make_float4(psi[3 * e], psi[3 * e + 1], psi[3 * e + 2], 0.f);
+    for (int d = 0; d < 3; d++)
+        out[(size_t)(1 + d) * n + e] = make_float4(Tx[3 * e + d], Ty[3 * e + d], Tz[3 * e + d], 0.f);
+    if (planes >= 7)
+        for (int d = 0; d < 3; d++)
+            out[(size_t)(4 + d) * n + e] = make_float4(dTx[3 * e + d], dTy[3 * e + d], dTz[3 * e + d], 0.f);
+    if (planes >= 8) out[(size_t)7 * n + e] = make_float4(d2x[e], d2y[e], d2z[e], 0.f);
+}
+
+__global__ void k_map_unpack(int n, int planes, const float4* in, float* psi, float* Tx, float* Ty, float* Tz,
+                             float* dTx, float* dTy, float* dTz, float* d2x, float* d2y, float* d2z) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    float4 v = in[e];
+    psi[3 * e] = v.x; psi[3 * e + 1] = v.y; psi[3 * e + 2] = v.z;
+    for (int d = 0; d < 3; d++) {
+        float4 g = in[(size_t)(1 + d) * n + e];
+        Tx[3 * e + d] = g.x; Ty[3 * e + d] = g.y; Tz[3 * e + d] = g.z;
+    }
+    if (planes >= 7)
+        for (int d = 0; d < 3; d++) {
+            float4 g = in[(size_t)(4 + d) * n + e];
+            dTx[3 * e + d] = g.x; dTy[3 * e + d] = g.y; dTz[3 * e + d] = g.z;
+        }
+    if (planes >= 8) {
+        float4 g = in[(size_t)7 * n + e];
+        d2x[e] = g.x; d2y[e] = g.y; d2z[e] = g.z;
+    }
+}
+
 // ED4 march (hermite.py:1375-1395): 4 epsilon points, RK4 of the position,
 // FD-Hermite composition, calc_ed4_1 (hermite.py:1154-1177).
 __global__ void __launch_bounds__(128) k_march_ed4(Mac mac, MapF m, float dt, float eps, float* __restrict__ opsi,
@@ -722,6 +901,76 @@ int edge_march_ed8(int nx, int ny, int nz, float dx, float dt, float epsilon, co
     int n = nx * ny * nz;
     k_march_ed8<<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, epsilon, opsi,
                                                         oTx, oTy, oTz, odTx, odTy, odTz, od2Tx, od2Ty, od2Tz);
+    return launch_status();
+}
+
+static int planes_of(int variant) {
+    return variant == HV_FD ? kPlanesED4 : (variant == HV_GARM ? kPlanesEDGE : (variant == HV_FULL ? kPlanesED8 : -1));
+}
+
+int edge_map_pack(int variant, int nx, int ny, int nz, const float* psi, const float* Tx, const float* Ty,
+                  const float* Tz, const float* dTx, const float* dTy, const float* dTz, const float* d2Tx,
+                  const float* d2Ty, const float* d2Tz, float* packed, void* stream) {
+    int pl = planes_of(variant);
+    if (!dims_ok(nx, ny, nz) || pl < 0 || !psi || !Tx || !Ty || !Tz || !packed) return EDGE_EINVAL;
+    if (pl >= 7 && (!dTx || !dTy || !dTz)) return EDGE_EINVAL;
+    if (pl >= 8 && (!d2Tx || !d2Ty || !d2Tz)) return EDGE_EINVAL;
+    if (!al16(packed)) return EDGE_EALIGN;
+    int n = nx * ny * nz;
+    k_map_pack<<<grid_for(n), kBlock, 0, S(stream)>>>(n, pl, psi, Tx, Ty, Tz, dTx, dTy, dTz, d2Tx, d2Ty, d2Tz,
+                                                      (float4*)packed);
+    return launch_status();
+}
+
+int edge_map_unpack(int variant, int nx, int ny, int nz, const float* packed, float* psi, float* Tx, float* Ty,
+                    float* Tz, float* dTx, float* dTy, float* dTz, float* d2Tx, float* d2Ty, float* d2Tz,
+                    void* stream) {
+    int pl = planes_of(variant);
+    if (!dims_ok(nx, ny, nz) || pl < 0 || !psi || !Tx || !Ty || !Tz || !packed) return EDGE_EINVAL;
+    if (pl >= 7 && (!dTx || !dTy || !dTz)) return EDGE_EINVAL;
+    if (pl >= 8 && (!d2Tx || !d2Ty || !d2Tz)) return EDGE_EINVAL;
+    if (!al16(packed)) return EDGE_EALIGN;
+    int n = nx * ny * nz;
+    k_map_unpack<<<grid_for(n), kBlock, 0, S(stream)>>>(n, pl, (const float4*)packed, psi, Tx, Ty, Tz, dTx, dTy,
+                                                        dTz, d2Tx, d2Ty, d2Tz);
+    return launch_status();
+}
+
+int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, float epsilon, const float* ux,
+                      const float* uy, const float* uz, const float* in_packed, float* out_packed, int identity,
+                      void* stream) {
+    int pl = planes_of(variant);
+    if (!dims_ok(nx, ny, nz) || pl < 0 || !ux || !uy || !uz || !out_packed) return EDGE_EINVAL;
+    if (!identity && !in_packed) return EDGE_EINVAL;
+    if (identity && variant != HV_GARM) return EDGE_EINVAL;
+    if (in_packed == out_packed) return EDGE_EINVAL;
+    if (!al16(in_packed) || !al16(out_packed)) return EDGE_EALIGN;
+    MapP m = make_mapp(in_packed, nx, ny, nz, dx);
+    Mac mac = make_mac(ux, uy, uz, nx, ny, nz, dx);
+    int n = nx * ny * nz;
+    float4* o = (float4*)out_packed;
+    if (variant == HV_GARM) {
+        if (identity) k_march_edge_p<true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        else k_march_edge_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+    } else if (variant == HV_FD) {
+        k_march_ed4_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+    } else {
+        k_march_ed8_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+    }
+    return launch_status();
+}
+
+int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const float* packed, float* fpsix,
+                         float* fpsiy, float* fpsiz, float* fcolx, float* fcoly, float* fcolz, void* stream) {
+    if (!dims_ok(nx, ny, nz) || planes_of(variant) < 0 || !packed || !fpsix || !fpsiy || !fpsiz || !fcolx ||
+        !fcoly || !fcolz)
+        return EDGE_EINVAL;
+    if (!al16(packed)) return EDGE_EALIGN;
+    MapP m = make_mapp(packed, nx, ny, nz, dx);
+    int g = grid_for(n_faces(nx, ny, nz), 128);
+    if (variant == HV_FD) k_face_map_p<HV_FD><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
+    else if (variant == HV_GARM) k_face_map_p<HV_GARM><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
+    else k_face_map_p<HV_FULL><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
     return launch_status();
 }
 

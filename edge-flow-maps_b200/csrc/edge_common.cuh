@@ -389,6 +389,171 @@ EDGE_D void hermite3(const MapF& m, const float p[3], float val[3], float grad[3
 }
 
 // ---------------------------------------------------------------------------
+// packed map layout: float4 planes, one cell per float4, components (x, y, z)
+// in .x .y .z:
+//   plane 0: psi
+//   planes 1..3: d psi / dx, d psi / dy, d psi / dz   (columns of grad psi)
+//   planes 4..6: psi_yz, psi_xz, psi_xy               (EDGE dT, ED8 dT)
+//   plane 7: psi_xyz                                   (ED8 d2T)
+// One 128-bit load then serves all three components of a Hermite stencil
+// point.
+// ---------------------------------------------------------------------------
+constexpr int kPlanesED4 = 4, kPlanesEDGE = 7, kPlanesED8 = 8;
+
+struct MapP {
+    const float4* __restrict__ g;  // planes, plane q at g + q * n
+    int n;                          // cells
+    int nx, ny, nz;
+    float dx;
+    float hi[3];
+};
+static inline MapP make_mapp(const float* planes, int nx, int ny, int nz, float dx) {
+    MapP m;
+    m.g = reinterpret_cast<const float4*>(planes);
+    m.n = nx * ny * nz;
+    m.nx = nx; m.ny = ny; m.nz = nz; m.dx = dx;
+    m.hi[0] = clamp_bound(nx, 2);
+    m.hi[1] = clamp_bound(ny, 2);
+    m.hi[2] = clamp_bound(nz, 2);
+    return m;
+}
+EDGE_D float4 ldp(const MapP& m, int q, int e) { return __ldg(m.g + (size_t)q * m.n + e); }
+EDGE_D float c4(const float4& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// Coefficients t[comp][8] of the corner (ii, jj, kk) from the packed planes
+// (same terms and scaling as hcoef).
+template <int VARIANT>
+EDGE_D void hcoef_p(const MapP& m, int ii, int jj, int kk, int im, int ip, int jm, int jp, int km, int kp,
+                    float t[3][8]) {
+    const int n1 = m.ny, n2 = m.nz;
+    const float dx = m.dx;
+    const int e = idx3(ii, jj, kk, n1, n2);
+    float4 P = ldp(m, 0, e), G0 = ldp(m, 1, e), G1 = ldp(m, 2, e), G2 = ldp(m, 3, e);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        t[c][0] = c4(P, c);
+        t[c][4] = c4(G0, c) * dx;
+        t[c][2] = c4(G1, c) * dx;
+        t[c][1] = c4(G2, c) * dx;
+    }
+    if (VARIANT == HV_FD) {
+        // hermite.py:104-148: FD of the stored gradient (plane 1+d = d psi/dx_d)
+        const int ekp = idx3(ii, jj, kp, n1, n2), ekm = idx3(ii, jj, km, n1, n2);
+        const int ejp = idx3(ii, jp, kk, n1, n2), ejm = idx3(ii, jm, kk, n1, n2);
+        const int eip = idx3(ip, jj, kk, n1, n2), eim = idx3(im, jj, kk, n1, n2);
+        float4 kp1 = ldp(m, 2, ekp), km1 = ldp(m, 2, ekm), kp0 = ldp(m, 1, ekp), km0 = ldp(m, 1, ekm);
+        float4 jp2 = ldp(m, 3, ejp), jm2 = ldp(m, 3, ejm), jp0 = ldp(m, 1, ejp), jm0 = ldp(m, 1, ejm);
+        float4 ip2 = ldp(m, 3, eip), im2 = ldp(m, 3, eim), ip1 = ldp(m, 2, eip), im1 = ldp(m, 2, eim);
+        // triple term: v30..v35 (hermite.py:128-145)
+        float4 a30 = ldp(m, 2, idx3(ip, jj, kp, n1, n2)), b30 = ldp(m, 2, idx3(ip, jj, km, n1, n2));
+        float4 c30 = ldp(m, 3, idx3(ip, jp, kk, n1, n2)), d30 = ldp(m, 3, idx3(ip, jm, kk, n1, n2));
+        float4 a31 = ldp(m, 2, idx3(im, jj, kp, n1, n2)), b31 = ldp(m, 2, idx3(im, jj, km, n1, n2));
+        float4 c31 = ldp(m, 3, idx3(im, jp, kk, n1, n2)), d31 = ldp(m, 3, idx3(im, jm, kk, n1, n2));
+        float4 a32 = ldp(m, 1, idx3(ii, jp, kp, n1, n2)), b32 = ldp(m, 1, idx3(ii, jp, km, n1, n2));
+        float4 c32 = ldp(m, 3, idx3(ip, jp, kk, n1, n2)), d32 = ldp(m, 3, idx3(im, jp, kk, n1, n2));
+        float4 a33 = ldp(m, 1, idx3(ii, jm, kp, n1, n2)), b33 = ldp(m, 1, idx3(ii, jm, km, n1, n2));
+        float4 c33 = ldp(m, 3, idx3(ip, jm, kk, n1, n2)), d33 = ldp(m, 3, idx3(im, jm, kk, n1, n2));
+        float4 a34 = ldp(m, 1, idx3(ii, jp, kp, n1, n2)), b34 = ldp(m, 1, idx3(ii, jm, kp, n1, n2));
+        float4 c34 = ldp(m, 2, idx3(ip, jj, kp, n1, n2)), d34 = ldp(m, 2, idx3(im, jj, kp, n1, n2));
+        float4 a35 = ldp(m, 1, idx3(ii, jp, km, n1, n2)), b35 = ldp(m, 1, idx3(ii, jm, km, n1, n2));
+        float4 c35 = ldp(m, 2, idx3(ip, jj, km, n1, n2)), d35 = ldp(m, 2, idx3(im, jj, km, n1, n2));
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            t[c][3] = ((c4(kp1, c) - c4(km1, c)) + (c4(jp2, c) - c4(jm2, c))) / 4.0f * dx;
+            t[c][5] = ((c4(kp0, c) - c4(km0, c)) + (c4(ip2, c) - c4(im2, c))) / 4.0f * dx;
+            t[c][6] = ((c4(jp0, c) - c4(jm0, c)) + (c4(ip1, c) - c4(im1, c))) / 4.0f * dx;
+            float v30 = ((c4(a30, c) - c4(b30, c)) + (c4(c30, c) - c4(d30, c))) / 4.0f;
+            float v31 = ((c4(a31, c) - c4(b31, c)) + (c4(c31, c) - c4(d31, c))) / 4.0f;
+            float v32 = ((c4(a32, c) - c4(b32, c)) + (c4(c32, c) - c4(d32, c))) / 4.0f;
+            float v33 = ((c4(a33, c) - c4(b33, c)) + (c4(c33, c) - c4(d33, c))) / 4.0f;
+            float v34 = ((c4(a34, c) - c4(b34, c)) + (c4(c34, c) - c4(d34, c))) / 4.0f;
+            float v35 = ((c4(a35, c) - c4(b35, c)) + (c4(c35, c) - c4(d35, c))) / 4.0f;
+            t[c][7] = (v30 - v31 + v32 - v33 + v34 - v35) / 6.0f * dx;
+        }
+    } else {
+        float4 D0 = ldp(m, 4, e), D1 = ldp(m, 5, e), D2 = ldp(m, 6, e);
+        if (VARIANT == HV_GARM) {
+            float4 xp = ldp(m, 4, idx3(ip, jj, kk, n1, n2)), xm = ldp(m, 4, idx3(im, jj, kk, n1, n2));
+            float4 yp = ldp(m, 5, idx3(ii, jp, kk, n1, n2)), ym = ldp(m, 5, idx3(ii, jm, kk, n1, n2));
+            float4 zp = ldp(m, 6, idx3(ii, jj, kp, n1, n2)), zm = ldp(m, 6, idx3(ii, jj, km, n1, n2));
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                t[c][7] = ((c4(xp, c) - c4(xm, c)) + (c4(yp, c) - c4(ym, c)) + (c4(zp, c) - c4(zm, c))) / 6.0f * dx *
+                          dx;
+        } else {
+            float4 X3 = ldp(m, 7, e);
+#pragma unroll
+            for (int c = 0; c < 3; c++) t[c][7] = c4(X3, c) * dx * dx * dx;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            t[c][3] = c4(D0, c) * dx * dx;
+            t[c][5] = c4(D1, c) * dx * dx;
+            t[c][6] = c4(D2, c) * dx * dx;
+        }
+    }
+}
+
+// hermite3 on the packed layout: the 8 corners are visited once and feed all
+// three components.
+template <int VARIANT, bool GRAD>
+EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[3][3]) {
+    float q[3] = {p[0] / m.dx - 0.5f, p[1] / m.dx - 0.5f, p[2] / m.dx - 0.5f};
+    HAxis X = haxis(q[0], m.hi[0], m.nx), Y = haxis(q[1], m.hi[1], m.ny), Z = haxis(q[2], m.hi[2], m.nz);
+    float v[3] = {0.f, 0.f, 0.f}, gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        int ii = i ? X.cp : X.c0, im = i ? X.c0 : X.cm, ip = i ? X.cpp : X.cp;
+        float Ax[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        float Bx[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        float dAx[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            int jj = j ? Y.cp : Y.c0, jm = j ? Y.c0 : Y.cm, jp = j ? Y.cpp : Y.cp;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                int kk = k ? Z.cp : Z.c0, km = k ? Z.c0 : Z.cm, kp = k ? Z.cpp : Z.cp;
+                float t[3][8];
+                hcoef_p<VARIANT>(m, ii, jj, kk, im, ip, jm, jp, km, kp, t);
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+#pragma unroll
+                    for (int a = 0; a < 2; a++) {
+                        float P0 = Z.f[k] * t[c][a * 4 + 0] + Z.g[k] * t[c][a * 4 + 1];
+                        float P1 = Z.f[k] * t[c][a * 4 + 2] + Z.g[k] * t[c][a * 4 + 3];
+                        Ax[c][a] += Y.f[j] * P0 + Y.g[j] * P1;
+                        if (GRAD) {
+                            float dP0 = Z.df[k] * t[c][a * 4 + 0] + Z.dg[k] * t[c][a * 4 + 1];
+                            float dP1 = Z.df[k] * t[c][a * 4 + 2] + Z.dg[k] * t[c][a * 4 + 3];
+                            Bx[c][a] += Y.df[j] * P0 + Y.dg[j] * P1;
+                            dAx[c][a] += Y.f[j] * dP0 + Y.g[j] * dP1;
+                        }
+                    }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            v[c] += X.f[i] * Ax[c][0] + X.g[i] * Ax[c][1];
+            if (GRAD) {
+                gx[c] += X.df[i] * Ax[c][0] + X.dg[i] * Ax[c][1];
+                gy[c] += X.f[i] * Bx[c][0] + X.g[i] * Bx[c][1];
+                gz[c] += X.f[i] * dAx[c][0] + X.g[i] * dAx[c][1];
+            }
+        }
+    }
+    const float inv = 1.0f / m.dx;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        val[c] = v[c];
+        if (GRAD) {
+            grad[c][0] = gx[c] * inv;
+            grad[c][1] = gy[c] * inv;
+            grad[c][2] = gz[c] * inv;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // RK4 marches (hermite.py:786-860, run_edge.py:337-357)
 // ---------------------------------------------------------------------------
 EDGE_D void rk4_pos(const Mac& mac, float psi[3], float dt) {

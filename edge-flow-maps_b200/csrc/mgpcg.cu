@@ -40,7 +40,7 @@ struct SolveState {
     unsigned long long kernels;  // kernels of this solver run so far (launch accounting)
 };
 
-constexpr int TX = 4, TY = 8, TZ = 32;  // smoothing tile (cells), 256 threads
+constexpr size_t kCoarseSmem = 160 * 1024;  // shared memory for the coarse group
 
 struct Lvl {
     int n0, n1, n2;
@@ -61,6 +61,9 @@ struct Ctx {  // everything a kernel needs, passed by value
     SolveState* st;
     cudaGraphConditionalHandle cond;
     int use_cond;  // 0: kernels run outside a graph (eager mode), no loop condition
+    int lc;        // first level of the shared-memory coarse group (k_coarse)
+    int cmoff;     // float offset of the coarse group's masks in shared memory
+    int csmem;     // dynamic shared memory of k_coarse (bytes)
 };
 
 EDGE_D void set_cond(const Ctx& c, unsigned v) {
@@ -204,9 +207,8 @@ __global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, do
     count_launch(c.st);
     const Lvl& L = c.lv[0];
     int n = L.n0 * L.n1 * L.n2;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
     double v[3] = {0.0, 0.0, 0.0};  // sum div (fluid), fluid count, sum r
-    if (e < n) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
         float d;
         bool fl = is_fluid(L.bm, e);
@@ -229,10 +231,10 @@ __global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, do
         c.p[0][e] = 0.0f;
         c.p[1][e] = 0.0f;
         if (fl) {
-            v[0] = d;
-            v[1] = 1.0;
+            v[0] += d;
+            v[1] += 1.0;
         }
-        v[2] = r;
+        v[2] += r;
     }
     if (last_block<3>(c, 0, v)) {
         double s[3];
@@ -268,7 +270,7 @@ __global__ void k_solid_fix(Ctx c) {
     bool fix = dsum > 0.0f && st->n_fluid > 0;
     float avg = fix ? dsum / (float)st->n_fluid : 0.0f;
     double v[1] = {0.0};
-    if (e < n) {
+    for (; e < n; e += gridDim.x * blockDim.x) {
         float r = L.r[e];
         if (fix && is_fluid(L.bm, e)) {
             float d = c.div[e] - avg;
@@ -276,7 +278,7 @@ __global__ void k_solid_fix(Ctx c) {
             r = d * -1.0f;
             L.r[e] = r;
         }
-        v[0] = r;
+        v[0] += r;
     }
     if (last_block<1>(c, 1, v)) {
         double s[1];
@@ -315,45 +317,38 @@ __global__ void __launch_bounds__(256) k_cg_ap(Ctx c) {
     }
     if (!running(c)) return;
     const Lvl& L = c.lv[0];
-    int n = L.n0 * L.n1 * L.n2;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = L.n0 * L.n1 * L.n2;
     SolveState* st = c.st;
-    int pc = st->pcur;
+    const int pc = st->pcur;
     const float* __restrict__ po = c.p[pc];
     float* __restrict__ pn = c.p[pc ^ 1];
     const float* __restrict__ z = L.z;
-    float beta = st->beta;
+    const float beta = st->beta;
+    const int s0 = L.n1 * L.n2, s1 = L.n2;
     double v[1] = {0.0};
-    if (e < n) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         float pe = 0.0f, ape = 0.0f;
         if (is_fluid(L.bm, e)) {
-            int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+            int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / s0;
             pe = __ldg(z + e) + beta * __ldg(po + e);
             float nsum = 0.0f;
-            int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
-            int stride[3] = {L.n1 * L.n2, L.n2, 1};
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                if (I[a] < D[a] - 1) {
-                    int q = e + stride[a];
-                    if (is_fluid(L.bm, q)) nsum += __ldg(z + q) + beta * __ldg(po + q);
-                }
-                if (I[a] > 0) {
-                    int q = e - stride[a];
-                    if (is_fluid(L.bm, q)) nsum += __ldg(z + q) + beta * __ldg(po + q);
-                }
-            }
+            if (i < L.n0 - 1 && is_fluid(L.bm, e + s0)) nsum += __ldg(z + e + s0) + beta * __ldg(po + e + s0);
+            if (i > 0 && is_fluid(L.bm, e - s0)) nsum += __ldg(z + e - s0) + beta * __ldg(po + e - s0);
+            if (j < L.n1 - 1 && is_fluid(L.bm, e + s1)) nsum += __ldg(z + e + s1) + beta * __ldg(po + e + s1);
+            if (j > 0 && is_fluid(L.bm, e - s1)) nsum += __ldg(z + e - s1) + beta * __ldg(po + e - s1);
+            if (k < L.n2 - 1 && is_fluid(L.bm, e + 1)) nsum += __ldg(z + e + 1) + beta * __ldg(po + e + 1);
+            if (k > 0 && is_fluid(L.bm, e - 1)) nsum += __ldg(z + e - 1) + beta * __ldg(po + e - 1);
             ape = n_fluid(c, L, i, j, k) * pe - nsum;
-            v[0] = (double)pe * (double)ape;
+            v[0] += (double)pe * (double)ape;
         }
         pn[e] = pe;
         c.Ap[e] = ape;
     }
     if (last_block<1>(c, 2, v)) {
-        double s[1];
-        final_sum<1>(c, 2, s);
+        double sm[1];
+        final_sum<1>(c, 2, sm);
         if (threadIdx.x == 0) {
-            double pAp = (double)(float)s[0];
+            double pAp = (double)(float)sm[0];
             st->pAp = pAp;
             st->alpha = (float)(st->zTr / (pAp + 1e-12));
             st->pcur = pc ^ 1;
@@ -374,15 +369,15 @@ __global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
     float alpha = st->alpha, mean = st->mean;
     const float* __restrict__ p = c.p[st->pcur];
     double v[2] = {0.0, 0.0};
-    if (e < n) {
+    for (; e < n; e += gridDim.x * blockDim.x) {
         float r = L.r[e] - mean;
         if (is_fluid(L.bm, e)) {
             c.x[e] += alpha * __ldg(p + e);
             r -= alpha * __ldg(c.Ap + e);
-            v[0] = (double)r * (double)r;
+            v[0] += (double)r * (double)r;
         }
         L.r[e] = r;
-        v[1] = r;
+        v[1] += r;
     }
     if (last_block<2>(c, 3, v)) {
         double s[2];
@@ -401,91 +396,80 @@ __global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
 // ---------------------------------------------------------------------------
 // V-cycle (mgpcg.py:177-195)
 // ---------------------------------------------------------------------------
-// One red-black Gauss-Seidel sweep (mgpcg.py:160-167) of level l on a
-// TX x TY x TZ tile, in shared memory with a 2-cell halo: the first colour
-// is updated on the tile plus a 1-cell rim, the second on the tile.
-//   FIRST : z starts at zero (first sweep after fill(0)); z is not read
-//   PROLONG: z += z[l+1][I/2] on load (mgpcg.py:155-158)
-//   ZR    : also accumulate z.(r-mean) over fluid cells (level 0) and run the
-//           end-of-iteration logic (beta, iteration count, loop condition)
-template <bool FIRST, bool PROLONG, bool ZR>
-__global__ void __launch_bounds__(256) k_sweep(Ctx c, int l, int phase0) {
+// Red-black Gauss-Seidel (mgpcg.py:160-167) runs as half sweeps: a half sweep
+// of colour c updates the cells with (i+j+k)&1 == c and reads only cells of
+// the other colour, so no update depends on another in the same launch, and a
+// cell's own old value is never read.  Hence:
+//   * z = 0 before the first down sweep needs no fill (that half sweep reads
+//     nothing, mode HS_FIRST);
+//   * the prolongation z[l] += z[l+1][I/2] (mgpcg.py:155-158) that precedes
+//     the up sweeps is applied on the fly to the neighbours the first up half
+//     sweep reads (mode HS_PROLONG): every cell is overwritten by a half sweep
+//     before its own value is read again, and solid cells are never read.
+// Levels with more cells than fit in shared memory use one thread per pair
+// of cells along k (the pair holds one cell of each colour); the remaining
+// coarse levels run as one thread block in shared memory (k_coarse).
+enum { HS_FIRST = 0, HS_PLAIN = 1, HS_PROLONG = 2, HS_ZR = 3 };
+
+EDGE_D float nb_val(const Lvl& L, const Lvl* C, int e, int i, int j, int k, bool prolong) {
+    float v = __ldg(L.z + e);
+    if (prolong) v += __ldg(C->z + idx3(i >> 1, j >> 1, k >> 1, C->n1, C->n2));
+    return v;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_hsweep(Ctx c, int l, int color) {
     count_launch(c.st);
-    constexpr int RX = TX + 4, RY = TY + 4, RZ = TZ + 4;
-    __shared__ float zs[RX * RY * RZ];
-    __shared__ float rs[RX * RY * RZ];
-    __shared__ unsigned char fs[RX * RY * RZ];  // 1 = fluid cell inside the grid
     if (!running(c)) {
-        if (ZR && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) set_cond(c, 0);
+        if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(c, 0);
         return;
     }
     const Lvl& L = c.lv[l];
+    const Lvl* C = MODE == HS_PROLONG ? &c.lv[l + 1] : nullptr;
     const float mean = l == 0 ? c.st->mean : 0.0f;
-    const int i0 = blockIdx.z * TX - 2, j0 = blockIdx.y * TY - 2, k0 = blockIdx.x * TZ - 2;
-    // load region
-    for (int s = threadIdx.x; s < RX * RY * RZ; s += blockDim.x) {
-        int kk = s % RZ, jj = (s / RZ) % RY, ii = s / (RZ * RY);
-        int i = i0 + ii, j = j0 + jj, k = k0 + kk;
-        float zv = 0.0f, rv = 0.0f;
-        unsigned char fl = 0;
-        if (i >= 0 && i < L.n0 && j >= 0 && j < L.n1 && k >= 0 && k < L.n2) {
-            int e = idx3(i, j, k, L.n1, L.n2);
-            fl = is_fluid(L.bm, e) ? 1 : 0;
-            rv = __ldg(L.r + e) - mean;
-            if (!FIRST) zv = L.z[e];
-            if (PROLONG) {
-                const Lvl& C = c.lv[l + 1];
-                zv += __ldg(C.z + idx3(i >> 1, j >> 1, k >> 1, C.n1, C.n2));
-            }
-        }
-        zs[s] = zv;
-        rs[s] = rv;
-        fs[s] = fl;
-    }
-    __syncthreads();
-    // two half sweeps: colour phase0 on [1, R-2], colour phase0^1 on [2, R-3]
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-        int lo = h == 0 ? 1 : 2;
-        int ex = RX - 2 * lo, ey = RY - 2 * lo, ez = RZ - 2 * lo;
-        int color = phase0 ^ h;
-        for (int s = threadIdx.x; s < ex * ey * ez; s += blockDim.x) {
-            int kk = s % ez + lo, jj = (s / ez) % ey + lo, ii = s / (ez * ey) + lo;
-            int i = i0 + ii, j = j0 + jj, k = k0 + kk;
-            if (((i + j + k) & 1) != color) continue;
-            int q = (ii * RY + jj) * RZ + kk;
-            if (!fs[q]) continue;
-            if (i < 0 || i >= L.n0 || j < 0 || j >= L.n1 || k < 0 || k >= L.n2) continue;
-            float ns = 0.0f;
-            // neighbours inside the grid that are fluid (fs is 0 outside)
-            ns += fs[q + RY * RZ] ? zs[q + RY * RZ] : 0.0f;
-            ns += fs[q - RY * RZ] ? zs[q - RY * RZ] : 0.0f;
-            ns += fs[q + RZ] ? zs[q + RZ] : 0.0f;
-            ns += fs[q - RZ] ? zs[q - RZ] : 0.0f;
-            ns += fs[q + 1] ? zs[q + 1] : 0.0f;
-            ns += fs[q - 1] ? zs[q - 1] : 0.0f;
-            zs[q] = (rs[q] + ns) / n_fluid(c, L, i, j, k);
-        }
-        __syncthreads();
-    }
-    // write the tile
+    const int h2 = L.n2 >> 1;
+    const int npair = L.n0 * L.n1 * h2;
     double v[1] = {0.0};
-    for (int s = threadIdx.x; s < TX * TY * TZ; s += blockDim.x) {
-        int kk = s % TZ + 2, jj = (s / TZ) % TY + 2, ii = s / (TZ * TY) + 2;
-        int i = i0 + ii, j = j0 + jj, k = k0 + kk;
-        if (i >= L.n0 || j >= L.n1 || k >= L.n2) continue;
-        int q = (ii * RY + jj) * RZ + kk;
-        L.z[idx3(i, j, k, L.n1, L.n2)] = zs[q];
-        if (ZR && fs[q]) v[0] += (double)zs[q] * (double)rs[q];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npair; t += gridDim.x * blockDim.x) {
+        int kk = t % h2, r = t / h2;
+        int j = r % L.n1, i = r / L.n1;
+        int k = 2 * kk + ((i + j + color) & 1);
+        int e = idx3(i, j, k, L.n1, L.n2);
+        const int s1 = L.n2, s0 = L.n1 * L.n2;
+        float rv = __ldg(L.r + e) - mean;
+        float zn = 0.0f;
+        if (is_fluid(L.bm, e)) {
+            float ns = 0.0f;
+            if (MODE != HS_FIRST) {
+                const bool pr = MODE == HS_PROLONG;
+                if (k < L.n2 - 1 && is_fluid(L.bm, e + 1)) ns += nb_val(L, C, e + 1, i, j, k + 1, pr);
+                if (k > 0 && is_fluid(L.bm, e - 1)) ns += nb_val(L, C, e - 1, i, j, k - 1, pr);
+                if (j < L.n1 - 1 && is_fluid(L.bm, e + s1)) ns += nb_val(L, C, e + s1, i, j + 1, k, pr);
+                if (j > 0 && is_fluid(L.bm, e - s1)) ns += nb_val(L, C, e - s1, i, j - 1, k, pr);
+                if (i < L.n0 - 1 && is_fluid(L.bm, e + s0)) ns += nb_val(L, C, e + s0, i + 1, j, k, pr);
+                if (i > 0 && is_fluid(L.bm, e - s0)) ns += nb_val(L, C, e - s0, i - 1, j, k, pr);
+            }
+            // neighbour_sum order differs from the reference's (+x,-x,+y,...):
+            // a rounding-level difference
+            zn = (rv + ns) / n_fluid(c, L, i, j, k);
+            L.z[e] = zn;
+            if (MODE == HS_ZR) v[0] += (double)zn * (double)rv;
+        }
+        if (MODE == HS_ZR) {
+            // the other cell of the pair (final from the previous half sweep)
+            int kp = k ^ 1;
+            int ep = idx3(i, j, kp, L.n1, L.n2);
+            if (is_fluid(L.bm, ep)) v[0] += (double)__ldg(L.z + ep) * (double)(__ldg(L.r + ep) - mean);
+        }
     }
-    if (ZR) {
+    if (MODE == HS_ZR) {
         // mgpcg.py:263-275: z.r, beta, update bookkeeping, loop condition
         if (last_block<1>(c, 4, v)) {
-            double s[1];
-            final_sum<1>(c, 4, s);
+            double sm[1];
+            final_sum<1>(c, 4, sm);
             if (threadIdx.x == 0) {
                 SolveState* st = c.st;
-                double zTr = (double)(float)s[0];
+                double zTr = (double)(float)sm[0];
                 if (st->setup) {
                     st->setup = 0;
                     st->zTr = zTr;
@@ -537,63 +521,171 @@ __global__ void __launch_bounds__(256) k_restrict(Ctx c, int l) {
     C.r[e] = acc;
 }
 
-// bottom smoothing (mgpcg.py:186-189): 20 red-black sweeps from z = 0 on the
-// coarsest level, one thread block, shared memory
-__global__ void __launch_bounds__(1024) k_bottom(Ctx c, int l, int iters) {
-    count_launch(c.st);
-    extern __shared__ float sh[];
-    if (!running(c)) return;
-    const Lvl& L = c.lv[l];
-    int n = L.n0 * L.n1 * L.n2;
-    float* zs = sh;
-    float* rs = sh + n;
-    const float mean = l == 0 ? c.st->mean : 0.0f;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        zs[e] = 0.0f;
-        rs[e] = __ldg(L.r + e) - mean;
-    }
-    __syncthreads();
-    int stride[3] = {L.n1 * L.n2, L.n2, 1};
-    for (int it = 0; it < iters; it++) {
-        for (int color = 0; color < 2; color++) {
-            for (int e = threadIdx.x; e < n; e += blockDim.x) {
-                int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
-                if (((i + j + k) & 1) != color || !is_fluid(L.bm, e)) continue;
-                int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
-                float ns = 0.0f;
-#pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    if (I[d] < D[d] - 1 && is_fluid(L.bm, e + stride[d])) ns += zs[e + stride[d]];
-                    if (I[d] > 0 && is_fluid(L.bm, e - stride[d])) ns += zs[e - stride[d]];
-                }
-                zs[e] = (rs[e] + ns) / n_fluid(c, L, i, j, k);
-            }
-            __syncthreads();
-        }
-    }
-    for (int e = threadIdx.x; e < n; e += blockDim.x) L.z[e] = zs[e];
-}
+// The coarse levels lc..L-1 of a V-cycle in one thread block out of shared
+// memory: down sweeps + restriction, 20 bottom sweeps, prolongation + up
+// sweeps (mgpcg.py:177-195); z[lc] is written back for the prolongation into
+// level lc-1.  With ZR (the whole grid fits, lc == 0) it also forms z.r and
+// runs the end-of-iteration bookkeeping.
+struct CoarseLvl {
+    int n0, n1, n2, off;  // off: float offset of r (z follows) in shared memory
+};
+EDGE_D bool c_fluid(const unsigned char* bm, int e) { return bm == nullptr || bm[e] == 0; }
 
-// end of the set-up V-cycle when it ran on a single level (L == 1): z.r and
-// the same bookkeeping as k_sweep<ZR>
-__global__ void k_zr_single(Ctx c) {
+template <bool ZR>
+__global__ void __launch_bounds__(1024) k_coarse(Ctx c, int lc, int moff) {
+    extern __shared__ float sh[];
     count_launch(c.st);
-    const Lvl& L = c.lv[0];
-    int n = L.n0 * L.n1 * L.n2;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (!running(c)) {
-        if (e == 0) set_cond(c, 0);
+        if (ZR && threadIdx.x == 0) set_cond(c, 0);
         return;
     }
-    double v[1] = {0.0};
-    float mean = c.st->mean;
-    if (e < n && is_fluid(L.bm, e)) v[0] = (double)L.z[e] * (double)(L.r[e] - mean);
-    if (last_block<1>(c, 4, v)) {
-        double s[1];
-        final_sum<1>(c, 4, s);
+    const int L = c.L;
+    const bool solid = c.lv[0].bm != nullptr;
+    unsigned char* bmall = reinterpret_cast<unsigned char*>(sh + moff);
+    const float mean = lc == 0 ? c.st->mean : 0.0f;
+    // layout
+    CoarseLvl cl[16];
+    int off = 0, boff = 0, bo[16];
+    for (int l = lc; l < L; l++) {
+        cl[l].n0 = c.lv[l].n0; cl[l].n1 = c.lv[l].n1; cl[l].n2 = c.lv[l].n2;
+        cl[l].off = off;
+        int n = cl[l].n0 * cl[l].n1 * cl[l].n2;
+        off += 2 * n;
+        bo[l] = boff;
+        boff += n;
+    }
+    // load r[lc] and the masks
+    {
+        int n = cl[lc].n0 * cl[lc].n1 * cl[lc].n2;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) sh[cl[lc].off + e] = __ldg(c.lv[lc].r + e) - mean;
+        if (solid)
+            for (int l = lc; l < L; l++) {
+                int m = cl[l].n0 * cl[l].n1 * cl[l].n2;
+                for (int e = threadIdx.x; e < m; e += blockDim.x) bmall[bo[l] + e] = __ldg(c.lv[l].bm + e) > 0;
+            }
+    }
+    __syncthreads();
+    auto half = [&](int l, int color, int mode) {
+        // mode: 0 from zero, 1 plain, 2 with the prolongation of l+1
+        const CoarseLvl& q = cl[l];
+        float* r = sh + q.off;
+        float* z = r + q.n0 * q.n1 * q.n2;
+        const unsigned char* bm = solid ? bmall + bo[l] : nullptr;
+        const float* zc = mode == 2 ? sh + cl[l + 1].off + cl[l + 1].n0 * cl[l + 1].n1 * cl[l + 1].n2 : nullptr;
+        int n = q.n0 * q.n1 * q.n2;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            int k = e % q.n2, j = (e / q.n2) % q.n1, i = e / (q.n1 * q.n2);
+            if (((i + j + k) & 1) != color || !c_fluid(bm, e)) continue;
+            float ns = 0.0f;
+            if (mode != 0) {
+                int I[3] = {i, j, k}, D[3] = {q.n0, q.n1, q.n2}, S[3] = {q.n1 * q.n2, q.n2, 1};
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    for (int sgn = -1; sgn <= 1; sgn += 2) {
+                        int ni = I[a] + sgn;
+                        if (ni < 0 || ni >= D[a]) continue;
+                        int f = e + sgn * S[a];
+                        if (!c_fluid(bm, f)) continue;
+                        float v = z[f];
+                        if (mode == 2) {
+                            int J[3] = {i, j, k};
+                            J[a] = ni;
+                            const CoarseLvl& u = cl[l + 1];
+                            v += zc[((J[0] >> 1) * u.n1 + (J[1] >> 1)) * u.n2 + (J[2] >> 1)];
+                        }
+                        ns += v;
+                    }
+                }
+            }
+            // num_fluid_neighbors (mgpcg.py:100-110 / mgpcg_solid.py:113-130)
+            float num = 6.0f;
+            {
+                int I[3] = {i, j, k}, D[3] = {q.n0, q.n1, q.n2}, S[3] = {q.n1 * q.n2, q.n2, 1};
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    if (I[a] <= 0 && c.bt[2 * a] == 2) num -= 1.0f;
+                    else if (bm && I[a] > 0 && bm[e - S[a]]) num -= 1.0f;
+                    if (I[a] >= D[a] - 1 && c.bt[2 * a + 1] == 2) num -= 1.0f;
+                    else if (bm && I[a] < D[a] - 1 && bm[e + S[a]]) num -= 1.0f;
+                }
+            }
+            z[e] = (r[e] + ns) / num;
+        }
+        __syncthreads();
+    };
+    // down
+    for (int l = lc; l < L - 1; l++) {
+        half(l, 0, 0);
+        half(l, 1, 1);
+        half(l, 0, 1);
+        half(l, 1, 1);
+        // restrict into r[l+1]
+        const CoarseLvl& q = cl[l];
+        const CoarseLvl& u = cl[l + 1];
+        float* r = sh + q.off;
+        float* z = r + q.n0 * q.n1 * q.n2;
+        float* rc = sh + u.off;
+        const unsigned char* bm = solid ? bmall + bo[l] : nullptr;
+        int m = u.n0 * u.n1 * u.n2;
+        for (int ce = threadIdx.x; ce < m; ce += blockDim.x) {
+            int K = ce % u.n2, J = (ce / u.n2) % u.n1, I = ce / (u.n1 * u.n2);
+            float acc = 0.0f;
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++)
+                    for (int cc = 0; cc < 2; cc++) {
+                        int i = 2 * I + a, j = 2 * J + b, k = 2 * K + cc;
+                        int e = (i * q.n1 + j) * q.n2 + k;
+                        if (!c_fluid(bm, e)) continue;
+                        int Ix[3] = {i, j, k}, D[3] = {q.n0, q.n1, q.n2}, S[3] = {q.n1 * q.n2, q.n2, 1};
+                        float ns = 0.0f, num = 6.0f;
+                        for (int d = 0; d < 3; d++) {
+                            if (Ix[d] < D[d] - 1 && c_fluid(bm, e + S[d])) ns += z[e + S[d]];
+                            if (Ix[d] > 0 && c_fluid(bm, e - S[d])) ns += z[e - S[d]];
+                            if (Ix[d] <= 0 && c.bt[2 * d] == 2) num -= 1.0f;
+                            else if (bm && Ix[d] > 0 && bm[e - S[d]]) num -= 1.0f;
+                            if (Ix[d] >= D[d] - 1 && c.bt[2 * d + 1] == 2) num -= 1.0f;
+                            else if (bm && Ix[d] < D[d] - 1 && bm[e + S[d]]) num -= 1.0f;
+                        }
+                        float res = r[e] - (num * z[e] - ns);
+                        acc += res * 0.5f;
+                    }
+            rc[ce] = acc;
+        }
+        __syncthreads();
+    }
+    // bottom (mgpcg.py:186-189)
+    half(L - 1, 0, 0);
+    half(L - 1, 1, 1);
+    for (int it = 1; it < 20; it++) {
+        half(L - 1, 0, 1);
+        half(L - 1, 1, 1);
+    }
+    // up
+    for (int l = L - 2; l >= lc; l--) {
+        half(l, 1, 2);
+        half(l, 0, 1);
+        half(l, 1, 1);
+        half(l, 0, 1);
+    }
+    // write back z[lc] (solid cells keep their last value, never read)
+    {
+        const CoarseLvl& q = cl[lc];
+        int n = q.n0 * q.n1 * q.n2;
+        const float* z = sh + q.off + n;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) c.lv[lc].z[e] = z[e];
+    }
+    if (ZR) {
+        const CoarseLvl& q = cl[lc];
+        int n = q.n0 * q.n1 * q.n2;
+        const float* r = sh + q.off;
+        const float* z = r + n;
+        double v[1] = {0.0};
+        for (int e = threadIdx.x; e < n; e += blockDim.x)
+            if (c_fluid(solid ? bmall + bo[lc] : nullptr, e)) v[0] += (double)z[e] * (double)r[e];
+        block_sum<1>(v);
         if (threadIdx.x == 0) {
             SolveState* st = c.st;
-            double zTr = (double)(float)s[0];
+            double zTr = (double)(float)v[0];
             if (st->setup) {
                 st->setup = 0;
                 st->zTr = zTr;
@@ -681,45 +773,75 @@ int alloc(Solver* s, void** p, size_t bytes) {
     return EDGE_OK;
 }
 
-// The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
-void enqueue_iteration(Solver* s, cudaStream_t stream);
-
-void enqueue_vcycle(Solver* s, cudaStream_t stream, bool final_zr) {
-    Ctx& c = s->ctx;
-    int Lb = c.L - 1;
-    for (int l = 0; l < Lb; l++) {
-        const Lvl& L = c.lv[l];
-        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
-        k_sweep<true, false, false><<<g, 256, 0, stream>>>(c, l, 0);
-        k_sweep<false, false, false><<<g, 256, 0, stream>>>(c, l, 0);
-        const Lvl& C = c.lv[l + 1];
-        k_restrict<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c, l);
-    }
-    {
-        const Lvl& B = c.lv[Lb];
-        int n = B.n0 * B.n1 * B.n2;
-        k_bottom<<<1, 1024, 2 * n * sizeof(float), stream>>>(c, Lb, 20);
-    }
-    for (int l = Lb - 1; l >= 0; l--) {
-        const Lvl& L = c.lv[l];
-        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
-        k_sweep<false, true, false><<<g, 256, 0, stream>>>(c, l, 1);
-        if (l == 0 && final_zr)
-            k_sweep<false, false, true><<<g, 256, 0, stream>>>(c, l, 1);
-        else
-            k_sweep<false, false, false><<<g, 256, 0, stream>>>(c, l, 1);
-    }
-    if (Lb == 0 && final_zr) {
-        const Lvl& L = c.lv[0];
-        k_zr_single<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, stream>>>(c);
+// The levels lc..L-1 that fit in kCoarseSmem of shared memory together go to
+// k_coarse; the finer ones run half-sweep kernels.
+void plan_coarse(Ctx& c, bool solid) {
+    for (int lc = 0; lc < c.L; lc++) {
+        size_t floats = 0, cells = 0;
+        for (int l = lc; l < c.L; l++) {
+            size_t n = (size_t)c.lv[l].n0 * c.lv[l].n1 * c.lv[l].n2;
+            floats += 2 * n;
+            cells += n;
+        }
+        size_t bytes = floats * sizeof(float) + (solid ? cells : 0) + 16;
+        if (bytes <= kCoarseSmem || lc == c.L - 1) {
+            c.lc = lc;
+            c.cmoff = (int)floats;
+            c.csmem = (int)bytes;
+            return;
+        }
     }
 }
 
+int prepare_coarse_kernels(const Ctx& c) {
+    if ((size_t)c.csmem > kCoarseSmem) return EDGE_EINVAL;  // the coarsest level alone must fit
+    if (c.csmem > 48 * 1024) {
+        CK(cudaFuncSetAttribute(k_coarse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+    }
+    return EDGE_OK;
+}
+
+// One V-cycle (mgpcg.py:177-195); with final_zr the last kernel also forms
+// z.r and the end-of-iteration bookkeeping (mgpcg.py:263-277).
+// reduction and sweep kernels loop over their cells with at most this many
+// blocks (8 per SM), which bounds the last-block atomics
+constexpr int kMaxBlocks = 148 * 8;
+inline int rgrid(long long n) { return (int)std::min<long long>(grid_for(n), kMaxBlocks); }
+
+void enqueue_vcycle_ctx(const Ctx& c, cudaStream_t stream, bool final_zr) {
+    const int lc = c.lc;
+    for (int l = 0; l < lc; l++) {
+        const Lvl& L = c.lv[l];
+        int g = rgrid((long long)L.n0 * L.n1 * (L.n2 / 2));
+        k_hsweep<HS_FIRST><<<g, 256, 0, stream>>>(c, l, 0);
+        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 1);
+        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 0);
+        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 1);
+        const Lvl& C = c.lv[l + 1];
+        k_restrict<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c, l);
+    }
+    if (final_zr && lc == 0) k_coarse<true><<<1, 1024, c.csmem, stream>>>(c, lc, c.cmoff);
+    else k_coarse<false><<<1, 1024, c.csmem, stream>>>(c, lc, c.cmoff);
+    for (int l = lc - 1; l >= 0; l--) {
+        const Lvl& L = c.lv[l];
+        int g = rgrid((long long)L.n0 * L.n1 * (L.n2 / 2));
+        k_hsweep<HS_PROLONG><<<g, 256, 0, stream>>>(c, l, 1);
+        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 0);
+        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 1);
+        if (l == 0 && final_zr) k_hsweep<HS_ZR><<<g, 256, 0, stream>>>(c, l, 0);
+        else k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 0);
+    }
+}
+
+void enqueue_vcycle(Solver* s, cudaStream_t stream, bool final_zr) { enqueue_vcycle_ctx(s->ctx, stream, final_zr); }
+
+// The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
 void enqueue_iteration(Solver* s, cudaStream_t stream) {
     Ctx& c = s->ctx;
     int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
-    k_cg_ap<<<grid_for(n), 256, 0, stream>>>(c);
-    k_cg_xr<<<grid_for(n), 256, 0, stream>>>(c);
+    k_cg_ap<<<rgrid(n), 256, 0, stream>>>(c);
+    k_cg_xr<<<rgrid(n), 256, 0, stream>>>(c);
     enqueue_vcycle(s, stream, true);
 }
 
@@ -753,8 +875,8 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
         }
     }
     CK(cudaMemsetAsync(c.st->counter, 0, sizeof(c.st->counter), cs));  // fresh reduction counters
-    k_setup_rhs<<<grid_for(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
-    if (s->solid && !rhs) k_solid_fix<<<grid_for(n), 256, 0, cs>>>(c);
+    k_setup_rhs<<<rgrid(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
+    if (s->solid && !rhs) k_solid_fix<<<rgrid(n), 256, 0, cs>>>(c);
     enqueue_vcycle(s, cs, true);  // first preconditioner application + z.r + tol
     cudaGraph_t g2;
     CK(cudaStreamEndCapture(cs, &g2));
@@ -818,8 +940,8 @@ int run_solve_eager(Solver* s, Faces U, const float* rhs, float* xout, double ab
                                                                                     C.n1, C.n2, F.n1, F.n2);
         }
     CK(cudaMemsetAsync(c.st->counter, 0, sizeof(c.st->counter), cs));
-    k_setup_rhs<<<grid_for(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
-    if (s->solid && !rhs) k_solid_fix<<<grid_for(n), 256, 0, cs>>>(c);
+    k_setup_rhs<<<rgrid(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
+    if (s->solid && !rhs) k_solid_fix<<<rgrid(n), 256, 0, cs>>>(c);
     enqueue_vcycle(s, cs, true);
     for (int it = 0; it <= max_iters + 8; it++) {
         CK(cudaMemcpyAsync(&s->st_host->status, &c.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
@@ -901,10 +1023,8 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
             else if (r == EDGE_OK) r = alloc(s, (void**)&V.bm, m * sizeof(int));
         }
     }
-    const Lvl& B = c.lv[L - 1];
-    if ((size_t)B.n0 * B.n1 * B.n2 * 2 * sizeof(float) > 200 * 1024) r = EDGE_EINVAL;  // bottom must fit in smem
-    if (r == EDGE_OK && (size_t)B.n0 * B.n1 * B.n2 * 2 * sizeof(float) > 48 * 1024)
-        r = cu(cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    plan_coarse(c, s->solid);
+    if (r == EDGE_OK) r = prepare_coarse_kernels(c);
     if (r == EDGE_OK) r = alloc(s, (void**)&c.x, n * sizeof(float));
     if (r == EDGE_OK) r = alloc(s, (void**)&c.p[0], n * sizeof(float));
     if (r == EDGE_OK) r = alloc(s, (void**)&c.p[1], n * sizeof(float));
@@ -1004,23 +1124,7 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
     k_copy<<<grid_for(n), 256, 0, st>>>(nullptr, r, c.lv[0].r, n);
     // outside a graph there is no loop condition to set
     c.use_cond = 0;
-    int Lb = c.L - 1;
-    for (int l = 0; l < Lb; l++) {
-        const Lvl& L = c.lv[l];
-        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
-        k_sweep<true, false, false><<<g, 256, 0, st>>>(c, l, 0);
-        k_sweep<false, false, false><<<g, 256, 0, st>>>(c, l, 0);
-        const Lvl& C = c.lv[l + 1];
-        k_restrict<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, st>>>(c, l);
-    }
-    const Lvl& B = c.lv[Lb];
-    k_bottom<<<1, 1024, 2 * B.n0 * B.n1 * B.n2 * sizeof(float), st>>>(c, Lb, 20);
-    for (int l = Lb - 1; l >= 0; l--) {
-        const Lvl& L = c.lv[l];
-        dim3 g((L.n2 + TZ - 1) / TZ, (L.n1 + TY - 1) / TY, (L.n0 + TX - 1) / TX);
-        k_sweep<false, true, false><<<g, 256, 0, st>>>(c, l, 1);
-        k_sweep<false, false, false><<<g, 256, 0, st>>>(c, l, 1);
-    }
+    enqueue_vcycle_ctx(c, st, false);
     k_copy<<<grid_for(n), 256, 0, st>>>(nullptr, c.lv[0].z, z, n);
     return cu(cudaPeekAtLastError());
 }
@@ -1125,8 +1229,6 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     if (L < 1 || L > 16) return EDGE_EINVAL;
     for (int l = 1; l < L; l++)
         if (nx % (1 << l) || ny % (1 << l) || nz % (1 << l)) return EDGE_EINVAL;
-    if ((long long)(nx >> (L - 1)) * (ny >> (L - 1)) * (nz >> (L - 1)) * 2 * sizeof(float) > 48 * 1024)
-        return EDGE_EINVAL;  // coarsest level must fit the bottom smoother's default shared memory
     if ((n + 255) / 256 > kNoAllocMaxBlocks) return EDGE_EINVAL;
     if (max_iters < 0) max_iters = 400;
     NoAllocAddrs* A = nullptr;
@@ -1167,6 +1269,9 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     c.partials = A->partials;
     c.st = A->state;
     c.use_cond = 0;
+    plan_coarse(c, false);
+    r = prepare_coarse_kernels(c);
+    if (r != EDGE_OK) return r;
     // the loop state starts clean on every call (the arrays keep the last
     // call's contents); x and p are zeroed by the set-up kernel
     SolveState init;
@@ -1176,7 +1281,7 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     Faces U = {{ux, uy, uz}, {nullptr, nullptr, nullptr}};
     int N = (int)n;
     k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-    k_setup_rhs<<<grid_for(N), 256, 0, cs>>>(c, U, nullptr, abs_tol, rel_tol, max_iters);
+    k_setup_rhs<<<rgrid(N), 256, 0, cs>>>(c, U, nullptr, abs_tol, rel_tol, max_iters);
     enqueue_vcycle(&s, cs, true);
     int st_status = ST_RUNNING;
     for (int it = 0; it <= max_iters + 8; it++) {

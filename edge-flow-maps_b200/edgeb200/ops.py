@@ -94,6 +94,28 @@ def march_ed8(u, dx, dt, eps, psi, T, dT, d2T, opsi, oT, odT, od2T):
            ptr(opsi), *_p3(oT), *_p3(odT), *_p3(od2T), stream())
 
 
+PLANES = {0: 4, 1: 7, 2: 8}  # packed float4 planes per Hermite variant
+
+
+def map_pack(variant, psi, T, dT, d2T, packed):
+    nx, ny, nz = cell_dims(psi)
+    _call("edge_map_pack", variant, nx, ny, nz, ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), ptr(packed), stream())
+
+
+def map_unpack(variant, packed, psi, T, dT, d2T):
+    nx, ny, nz = cell_dims(psi)
+    _call("edge_map_unpack", variant, nx, ny, nz, ptr(packed), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), stream())
+
+
+def march_packed(variant, u, dx, dt, eps, packed_in, packed_out, res, identity=False):
+    _call("edge_march_packed", variant, *res, F(dx), F(dt), F(eps), *_p3(u), ptr(packed_in), ptr(packed_out),
+          int(bool(identity)), stream())
+
+
+def face_map_packed(variant, dx, packed, res, fpsi, fcol):
+    _call("edge_face_map_packed", variant, *res, F(dx), ptr(packed), *_p3(fpsi), *_p3(fcol), stream())
+
+
 def face_map(variant, dx, psi, T, dT, d2T, fpsi, fcol):
     nx, ny, nz = cell_dims(psi)
     _call("edge_face_map", variant, nx, ny, nz, F(dx), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), *_p3(fpsi),

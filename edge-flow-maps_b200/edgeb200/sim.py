@@ -29,7 +29,7 @@ VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL}
 class EdgeSim:
     def __init__(self, res, dx, variant="edge", cfl=0.5, reinit_every=12, ed_eps=None, base_level=3,
                  bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda", solid=None,
-                 emitters=None):
+                 emitters=None, packed=False):
         if variant not in VARIANTS:
             raise ValueError(f"variant must be one of {sorted(VARIANTS)}")
         N.load()
@@ -52,8 +52,15 @@ class EdgeSim:
         self.smoke = zeros_cells(r, 4)
         self.init_smoke = zeros_cells(r, 4)
         self.err_smoke = zeros_cells(r, 4)
-        # backward map state, two sets (ping-pong)
-        self.maps = [self._map_set() for _ in range(2)]
+        # backward map state, two sets (ping-pong); `packed` keeps them as
+        # float4 planes (edge_map_pack layout) instead of the reference layout
+        self.packed = bool(packed)
+        if self.packed:
+            planes = ops.PLANES[self.hv]
+            self.pmaps = [torch.zeros((planes,) + r + (4,), dtype=torch.float32, device=device) for _ in range(2)]
+            self._unpacked = None
+        else:
+            self.maps = [self._map_set() for _ in range(2)]
         self.cur = 0
         # forward map on the faces
         self.phi = zeros_faces(r, 3)
@@ -93,7 +100,13 @@ class EdgeSim:
 
     @property
     def map(self):
-        return self.maps[self.cur]
+        """The current backward map in the reference layout (unpacked on
+        demand when the driver keeps packed planes)."""
+        if not self.packed:
+            return self.maps[self.cur]
+        m = self._map_set()
+        ops.map_unpack(self.hv, self.pmaps[self.cur], m["psi"], m["T"], m.get("dT"), m.get("d2T"))
+        return m
 
     # -- state I/O --------------------------------------------------------------
     def set_velocity(self, u_x, u_y, u_z):
@@ -179,8 +192,11 @@ class EdgeSim:
             ops.pullback_u(P["vis"], dx, self.phi, self.F, self.tmp_u)
             for a, t in zip(self.init_u, self.tmp_u):
                 ops.axpy(a, t, curr_dt, a)
-        m = self.map
-        ops.face_map(self.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), self.fpsi, self.fcol)
+        if self.packed:
+            ops.face_map_packed(self.hv, dx, self.pmaps[self.cur], self.res, self.fpsi, self.fcol)
+        else:
+            m = self.maps[self.cur]
+            ops.face_map(self.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), self.fpsi, self.fcol)
         # u = (grad psi)^T u_init(psi), smoke = smoke_init(psi)        run_edge.py:669-670
         ops.pullback_u(self.init_u, dx, self.fpsi, self.fcol, self.u)
         ops.pullback_dye(self.init_smoke, dx, self.fpsi, self.smoke)
@@ -221,6 +237,16 @@ class EdgeSim:
 
     def _march(self, dt, reinit):
         dx, eps = self.dx, self.ed_eps
+        if self.packed:
+            src, dst = self.pmaps[self.cur], self.pmaps[self.cur ^ 1]
+            if reinit and self.variant != "edge":
+                m = self._map_set()
+                ops.reset_cells(dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"))
+                ops.map_pack(self.hv, m["psi"], m["T"], m.get("dT"), m.get("d2T"), src)
+            ops.march_packed(self.hv, self.u, dx, dt, eps, src, dst, self.res,
+                             identity=reinit and self.variant == "edge")
+            self.cur ^= 1
+            return
         src, dst = self.maps[self.cur], self.maps[self.cur ^ 1]
         if self.variant == "edge":
             ops.march_edge(self.u, dx, dt, eps, src["psi"], src["T"], src["dT"], dst["psi"], dst["T"], dst["dT"],

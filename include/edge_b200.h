@@ -105,6 +105,28 @@ int edge_face_map(int variant, int nx, int ny, int nz, float dx, const float *ps
                   const float *Tz, const float *dTx, const float *dTy, const float *dTz, const float *d2Tx,
                   const float *d2Ty, const float *d2Tz, float *fpsix, float *fpsiy, float *fpsiz, float *fcolx,
                   float *fcoly, float *fcolz, void *stream);
+/* The backward map in the packed layout the device driver keeps: float4
+ * planes of n = nx*ny*nz cells (plane q at packed + 4*q*n floats):
+ * 0 psi, 1-3 the columns d psi/dx, d psi/dy, d psi/dz, 4-6 the mixed
+ * derivatives (psi_yz, psi_xz, psi_xy) per component, 7 psi_xyz; ED4 uses
+ * planes 0-3, EDGE 0-6, ED8 0-7.  pack/unpack convert from/to the reference
+ * layout (psi, T_c rows, dT_c, d2T_c as above; no reference counterpart). */
+int edge_map_pack(int variant, int nx, int ny, int nz, const float *psi, const float *Tx, const float *Ty,
+                  const float *Tz, const float *dTx, const float *dTy, const float *dTz, const float *d2Tx,
+                  const float *d2Ty, const float *d2Tz, float *packed, void *stream);
+int edge_map_unpack(int variant, int nx, int ny, int nz, const float *packed, float *psi, float *Tx, float *Ty,
+                    float *Tz, float *dTx, float *dTy, float *dTz, float *d2Tx, float *d2Ty, float *d2Tz,
+                    void *stream);
+/* The EDGE / ED4 / ED8 marches (hermite.py:1426-1521, 1375-1395, 1290-1338)
+ * on packed maps: in_packed is the accumulated map, out_packed receives the
+ * new one (must not alias).  identity (EDGE only): compose with the identity
+ * map, in_packed is not read. */
+int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, float epsilon, const float *ux,
+                      const float *uy, const float *uz, const float *in_packed, float *out_packed, int identity,
+                      void *stream);
+/* edge_face_map on a packed map */
+int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const float *packed, float *fpsix,
+                         float *fpsiy, float *fpsiz, float *fcolx, float *fcoly, float *fcolz, void *stream);
 /* forward map on the faces, advance_map x3, run_edge.py:330-357 (in place) */
 int edge_advance_map(int nx, int ny, int nz, float dx, float dt, const float *ux, const float *uy, const float *uz,
                      float *phix, float *phiy, float *phiz, float *Fx, float *Fy, float *Fz, void *stream);

@@ -278,3 +278,53 @@ def test_larger_grid_vs_oracle(ops):
     ops.map_u_psi(1, gu, gu1, dx, g[0], g[1:4], g[4:7])
     for i in range(3):
         assert rel_l2(N_(gu1[i]), ou[i]) < 1e-4
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_packed_layout_roundtrip_and_march(ops, variant):
+    """pack -> unpack is the identity, and the packed march / face map equal
+    the reference-layout ones."""
+    rng = np.random.default_rng(21 + variant)
+    res = (24, 16, 12)
+    dx = 1.0 / 16
+    planes = {0: 4, 1: 7, 2: 8}[variant]
+    psi = T_(O.center_coords(res, dx) + 0.3 * dx * rng.uniform(-1, 1, size=res + (3,)))
+    T = [T_(np.eye(3)[c] + 0.05 * rng.normal(size=res + (3,))) for c in range(3)]
+    dT = [T_(0.2 * rng.normal(size=res + (3,))) for _ in range(3)] if variant else None
+    d2T = [T_(0.2 * rng.normal(size=res)) for _ in range(3)] if variant == 2 else None
+    packed = torch.zeros((planes,) + res + (4,), device="cuda")
+    ops.map_pack(variant, psi, T, dT, d2T, packed)
+    psi2 = torch.empty_like(psi)
+    T2 = [torch.empty_like(t) for t in T]
+    dT2 = [torch.empty_like(t) for t in dT] if dT else None
+    d2T2 = [torch.empty_like(t) for t in d2T] if d2T else None
+    ops.map_unpack(variant, packed, psi2, T2, dT2, d2T2)
+    np.testing.assert_array_equal(N_(psi2), N_(psi))
+    for a, b in zip(T2, T):
+        np.testing.assert_array_equal(N_(a), N_(b))
+    u = [T_(0.5 * rng.normal(size=s)) for s in O.face_shapes(res)]
+    out = torch.zeros_like(packed)
+    ops.march_packed(variant, u, dx, 0.02, 0.025 * dx, packed, out, res)
+    o = [torch.empty_like(psi) for _ in range(7)] + [torch.empty(res, device="cuda") for _ in range(3)]
+    if variant == 1:
+        ops.march_edge(u, dx, 0.02, 0.025 * dx, psi, T, dT, o[0], o[1:4], o[4:7])
+    elif variant == 0:
+        ops.march_ed4(u, dx, 0.02, 0.025 * dx, psi, T, o[0], o[1:4])
+    else:
+        ops.march_ed8(u, dx, 0.02, 0.025 * dx, psi, T, dT, d2T, o[0], o[1:4], o[4:7], o[7:10])
+    p2 = torch.empty_like(psi)
+    T3 = [torch.empty_like(t) for t in T]
+    dT3 = [torch.empty_like(t) for t in T] if dT else None
+    d2T3 = [torch.empty(res, device="cuda") for _ in range(3)] if d2T else None
+    ops.map_unpack(variant, out, p2, T3, dT3, d2T3)
+    assert rel_l2(N_(p2), N_(o[0])) < 1e-6
+    for a, b in zip(T3, o[1:4]):
+        assert rel_l2(N_(a), N_(b)) < 1e-5
+    fp = [torch.empty(s + (3,), device="cuda") for s in O.face_shapes(res)]
+    fc = [torch.empty(s + (3,), device="cuda") for s in O.face_shapes(res)]
+    fp2 = [torch.empty_like(t) for t in fp]
+    fc2 = [torch.empty_like(t) for t in fc]
+    ops.face_map(variant, dx, psi, T, dT, d2T, fp, fc)
+    ops.face_map_packed(variant, dx, packed, res, fp2, fc2)
+    for a, b in zip(fp + fc, fp2 + fc2):
+        assert rel_l2(N_(b), N_(a)) < 1e-6

@@ -38,14 +38,15 @@ def test_edge_steps_golden():
         assert rel_l2(N_(sim.smoke), d[f"s{i}_smoke"]) < 2e-4
 
 
+@pytest.mark.parametrize("packed", [False, True])
 @pytest.mark.parametrize("variant", ["edge", "ed4", "ed8"])
-def test_steps_vs_oracle(variant):
+def test_steps_vs_oracle(variant, packed):
     from edgeb200.sim import EdgeSim, leapfrog_init
     res = (32, 16, 16)
     dx = 1.0 / 16
     u, smoke = leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.06, circulation=0.2, num_samples=200)
     st = O.EdgeState(res, dx, [N_(t) for t in u], N_(smoke))
-    sim = EdgeSim(res, dx, variant=variant, reinit_every=3, base_level=2, visualize_dt=1e9)
+    sim = EdgeSim(res, dx, variant=variant, reinit_every=3, base_level=2, visualize_dt=1e9, packed=packed)
     sim.set_velocity(*u)
     sim.set_smoke(smoke)
     for i in range(4):
