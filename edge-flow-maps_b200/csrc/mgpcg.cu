@@ -7,11 +7,18 @@
 // summed in block order, so results are run-to-run deterministic); the body's
 // last kernel sets the loop condition, so a solve makes no host round trip.
 //
-// Arrays: level l holds r[l], z[l] (float32, n>>l per axis); the fine level
-// also holds x, two p buffers (ping-pong, so update_p fuses into the Ap
-// stencil) and Ap.  The all-Neumann recentering (mgpcg.py:169-175) is kept as
-// a pending scalar `mean` that every reader of r[0] subtracts, and that the
-// r update folds into the stored residual.
+// Layout in HBM.  Every level's r and z, and the fine level's x and p, are
+// stored red-black split: cell (i,j,k) of colour c = (i+j+k)&1 lives in plane
+// c at slot (i*n1 + j)*H + (k>>1), H = (n2+1)/2.  The six neighbours of a
+// colour-c cell at slot e are the other plane's slots e +- n1*H, e +- H,
+// e + (k&1) (k+1) and e - 1 + (k&1) (k-1).  A half sweep of colour c therefore
+// reads one plane of r and the other plane of z and writes one plane of z, all
+// with unit stride, and never touches the half of the grid it does not need.
+// The pressure matrix is never stored: A p is recomputed from p where needed.
+//
+// The all-Neumann recentering (mgpcg.py:169-175) is kept as a pending scalar
+// `mean` that every reader of r[0] subtracts and that the r update folds into
+// the stored residual.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,61 +42,148 @@ struct SolveState {
     double zTr, pAp, rTr, rsum, tol, abs_tol, rel_tol, div_sum;
     float alpha, beta, mean, pad0;
     int it, max_iters, status, setup;
-    int pcur, all_neumann, n_fluid, pad1;
+    int pcur, all_neumann, n_fluid, x_valid;
     unsigned int counter[8];
     unsigned long long kernels;  // kernels of this solver run so far (launch accounting)
 };
 
 constexpr size_t kCoarseSmem = 160 * 1024;  // shared memory for the coarse group
 
+// x / d for 0 <= x < 2^31 with one multiply-high (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, unsigned
+// case: l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// q = (mulhi(x, m) + x) >> l; the sum cannot wrap for x < 2^31).
+struct FDiv {
+    unsigned m;
+    int s;
+};
+inline FDiv make_fdiv(unsigned d) {
+    int l = 0;
+    while ((1ull << l) < d) l++;
+    unsigned long long m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
+    return FDiv{(unsigned)m, l};
+}
+EDGE_D int fdiv(int x, FDiv f) { return (int)((__umulhi((unsigned)x, f.m) + (unsigned)x) >> f.s); }
+
+// Per-cell neighbour code of the solid solver: which of the six neighbours
+// enter the neighbour sum (in range and fluid), whether the cell is fluid,
+// and num_fluid_neighbors in bits 8-11 (mgpcg_solid.py:99-130).
+enum { NB_XP = 1, NB_XM = 2, NB_YP = 4, NB_YM = 8, NB_ZP = 16, NB_ZM = 32, CELL_FLUID = 64 };
+
 struct Lvl {
-    int n0, n1, n2;
-    float* r;
-    float* z;
-    const int* bm;  // solid mask (level 0: the caller's; NULL: plain solver)
+    int n0, n1, n2, H;
+    int P;               // slots per colour plane, n0*n1*H
+    FDiv dH, d1, d2;     // division by H, n1, n2 (index decomposition)
+    FDiv dQ;             // division by H/4 (four-slot kernels)
+    int vec;             // H % 4 == 0: the level runs the four-slot (float4) kernels
+    float* r[2];         // residual planes
+    float* z[2];         // preconditioned residual planes
+    unsigned short* code[2];  // solid solver: neighbour codes per plane (else NULL)
+    int* bm;             // solid solver: lexicographic mask (level 0: the caller's)
 };
 
-struct Ctx {  // everything a kernel needs, passed by value
-    Lvl lv[16];
-    int L;
-    int bt[6];
-    float* x;
-    float* p[2];
-    float* Ap;
-    float* div;
-    double* partials;
+struct G {  // what every solver kernel needs
     SolveState* st;
+    double* partials;
     cudaGraphConditionalHandle cond;
     int use_cond;  // 0: kernels run outside a graph (eager mode), no loop condition
-    int lc;        // first level of the shared-memory coarse group (k_coarse)
-    int cmoff;     // float offset of the coarse group's masks in shared memory
-    int csmem;     // dynamic shared memory of k_coarse (bytes)
+    int bt[6];
 };
 
-EDGE_D void set_cond(const Ctx& c, unsigned v) {
-    if (c.use_cond) cudaGraphSetConditional(c.cond, v);
+struct Fine {  // fine-level CG vectors
+    float* x[2];
+    float* p[2][2];  // [ping-pong buffer][plane]
+    float* div;      // lexicographic divergence (edge_mgpcg_get, solid correction)
+};
+
+struct Levels {  // the pyramid, for the shared-memory coarse group
+    Lvl lv[16];
+    int L, lc;
+};
+
+struct Ctx {
+    Levels lv;
+    G g;
+    Fine f;
+    int csmem;  // dynamic shared memory of k_coarse (bytes)
+};
+
+EDGE_D void set_cond(const G& g, unsigned v) {
+    if (g.use_cond) cudaGraphSetConditional(g.cond, v);
 }
 
-EDGE_D bool is_fluid(const int* bm, int e) { return bm == nullptr || __ldg(bm + e) <= 0; }
+EDGE_D bool running(const G& g) { return *((volatile int*)&g.st->status) == ST_RUNNING; }
 
-// mgpcg.py:100-110 num_fluid_neighbors (+ mgpcg_solid.py:113-130 solid faces)
-EDGE_D float n_fluid(const Ctx& c, const Lvl& L, int i, int j, int k) {
+// every solver kernel counts itself once (block 0, thread 0), including the
+// ones that return early once the loop has finished
+EDGE_D void count_launch(SolveState* st) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) atomicAdd(&st->kernels, 1ull);
+}
+
+// slot t of a colour plane -> (i, j, kk)
+struct Slot {
+    int i, j, kk;
+};
+template <class LV>
+EDGE_D Slot slot_of(const LV& L, int t) {
+    int row = fdiv(t, L.dH);
+    int i = fdiv(row, L.d1);
+    return Slot{i, row - i * L.n1, t - row * L.H};
+}
+
+// num_fluid_neighbors of the plain solver (mgpcg.py:100-110)
+template <class LV>
+EDGE_D float nf_walls(const int* bt, const LV& L, int i, int j, int k) {
     float num = 6.0f;
-    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        if (I[a] <= 0 && c.bt[2 * a] == 2) num -= 1.0f;
-        else if (L.bm && I[a] > 0) {
-            int e = idx3(i - (a == 0), j - (a == 1), k - (a == 2), L.n1, L.n2);
-            if (__ldg(L.bm + e) > 0) num -= 1.0f;
-        }
-        if (I[a] >= D[a] - 1 && c.bt[2 * a + 1] == 2) num -= 1.0f;
-        else if (L.bm && I[a] < D[a] - 1) {
-            int e = idx3(i + (a == 0), j + (a == 1), k + (a == 2), L.n1, L.n2);
-            if (__ldg(L.bm + e) > 0) num -= 1.0f;
-        }
-    }
+    if (i <= 0 && bt[0] == 2) num -= 1.0f;
+    if (i >= L.n0 - 1 && bt[1] == 2) num -= 1.0f;
+    if (j <= 0 && bt[2] == 2) num -= 1.0f;
+    if (j >= L.n1 - 1 && bt[3] == 2) num -= 1.0f;
+    if (k <= 0 && bt[4] == 2) num -= 1.0f;
+    if (k >= L.n2 - 1 && bt[5] == 2) num -= 1.0f;
     return num;
+}
+
+// the plain solver's code: every in-range neighbour, every cell fluid
+template <class LV>
+EDGE_D unsigned range_code(const LV& L, int i, int j, int k) {
+    return (i < L.n0 - 1 ? NB_XP : 0) | (i > 0 ? NB_XM : 0) | (j < L.n1 - 1 ? NB_YP : 0) | (j > 0 ? NB_YM : 0) |
+           (k < L.n2 - 1 ? NB_ZP : 0) | (k > 0 ? NB_ZM : 0) | CELL_FLUID;
+}
+
+template <bool SOLID, class LV>
+EDGE_D float nf_of(const int* bt, const LV& L, unsigned code, int i, int j, int k) {
+    return SOLID ? (float)(code >> 8) : nf_walls(bt, L, i, j, k);
+}
+
+// neighbour_sum (mgpcg.py:86-99, mgpcg_solid.py:99-111) in the reference's
+// order (+x, -x, +y, -y, +z, -z) over the other plane; val(slot, direction)
+template <class LV, class F>
+EDGE_D float nbr_sum(const LV& L, unsigned code, int e, int k, F val) {
+    const int sx = L.n1 * L.H;
+    float ret = 0.0f;
+    if (code & NB_XP) ret += val(e + sx, 0);
+    if (code & NB_XM) ret += val(e - sx, 1);
+    if (code & NB_YP) ret += val(e + L.H, 2);
+    if (code & NB_YM) ret += val(e - L.H, 3);
+    if (code & NB_ZP) ret += val(e + (k & 1), 4);
+    if (code & NB_ZM) ret += val(e - 1 + (k & 1), 5);
+    return ret;
+}
+
+EDGE_D void dir_offset(int d, int& di, int& dj, int& dk) {
+    di = d == 0 ? 1 : (d == 1 ? -1 : 0);
+    dj = d == 2 ? 1 : (d == 3 ? -1 : 0);
+    dk = d == 4 ? 1 : (d == 5 ? -1 : 0);
+}
+
+// z of the coarse level at the parent of fine cell (i, j, k) (prolongate,
+// mgpcg.py:155-158: z[l][I] += z[l+1][I // 2])
+template <class LV>
+EDGE_D float parent_z(const LV& C, const float* zc0, const float* zc1, int i, int j, int k) {
+    int I = i >> 1, J = j >> 1, K = k >> 1;
+    int e = (I * C.n1 + J) * C.H + (K >> 1);
+    return ((I + J + K) & 1) ? zc1[e] : zc0[e];
 }
 
 // ---------------------------------------------------------------------------
@@ -123,16 +217,16 @@ EDGE_D void block_sum(double (&v)[N]) {
 // Publish this block's partials; returns true in every thread of the block
 // that arrives last, after which partials[q*nblk + b] hold all blocks' sums.
 template <int N>
-EDGE_D bool last_block(const Ctx& c, int slot, double (&v)[N]) {
+EDGE_D bool last_block(const G& g, int slot, double (&v)[N]) {
     __shared__ bool am_last;
     block_sum<N>(v);
-    int nblk = gridDim.x * gridDim.y * gridDim.z;
-    int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    int nblk = gridDim.x;
+    int b = blockIdx.x;
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < N; q++) c.partials[q * nblk + b] = v[q];
+        for (int q = 0; q < N; q++) g.partials[q * nblk + b] = v[q];
         __threadfence();
-        unsigned t = atomicAdd(&c.st->counter[slot], 1u);
+        unsigned t = atomicAdd(&g.st->counter[slot], 1u);
         am_last = (t == (unsigned)nblk - 1);
     }
     __syncthreads();
@@ -141,29 +235,43 @@ EDGE_D bool last_block(const Ctx& c, int slot, double (&v)[N]) {
 
 // Sum the published partials (fixed order: deterministic) in the last block.
 template <int N>
-EDGE_D void final_sum(const Ctx& c, int slot, double (&out)[N]) {
+EDGE_D void final_sum(const G& g, int slot, double (&out)[N]) {
     __threadfence();
-    int nblk = gridDim.x * gridDim.y * gridDim.z;
+    int nblk = gridDim.x;
     double v[N];
 #pragma unroll
     for (int q = 0; q < N; q++) {
         double s = 0.0;
-        for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(c.partials + q * nblk + b);
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(g.partials + q * nblk + b);
         v[q] = s;
     }
     block_sum<N>(v);
 #pragma unroll
     for (int q = 0; q < N; q++) out[q] = v[q];
-    if (threadIdx.x == 0) c.st->counter[slot] = 0;
+    if (threadIdx.x == 0) g.st->counter[slot] = 0;
 }
 
-EDGE_D bool running(const Ctx& c) { return *((volatile int*)&c.st->status) == ST_RUNNING; }
-
-// every solver kernel counts itself once (block 0, thread 0), including the
-// ones that return early once the loop has finished
-EDGE_D void count_launch(SolveState* st) {
-    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) atomicAdd(&st->kernels, 1ull);
+// end of a preconditioner application: z.r, beta, iteration bookkeeping and
+// the loop condition (mgpcg.py:221-226, 263-277); thread 0 only
+EDGE_D void zr_epilogue(const G& g, double zr) {
+    SolveState* st = g.st;
+    double zTr = (double)(float)zr;
+    if (st->setup) {
+        st->setup = 0;
+        st->zTr = zTr;
+        st->beta = 0.0f;
+        st->tol = fmax(st->abs_tol, zTr * st->rel_tol);
+        if (st->max_iters <= 0) st->status = ST_NOCONV;
+    } else {
+        st->beta = (float)(zTr / (st->zTr + 1e-12));
+        st->zTr = zTr;
+        st->it += 1;
+        if (st->it >= st->max_iters) st->status = ST_NOCONV;
+    }
+    set_cond(g, st->status == ST_RUNNING ? 1u : 0u);
 }
+
+#define GRID_STRIDE(t, n) for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (n); t += gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------------------
 // set-up: apply_bc, divergence, solid correction, recentering mean
@@ -173,16 +281,23 @@ struct Faces {
     float* f[3];
 };
 
-// mgpcg.py:374-392 apply_bc (walls)
-__global__ void k_apply_walls(Ctx c, int nx, int ny, int nz, Faces U) {
-    count_launch(c.st);
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_faces(nx, ny, nz)) return;
-    FaceIdx f = face_decompose(t, nx, ny, nz);
-    int I[3] = {f.i, f.j, f.k};
-    int D[3] = {nx, ny, nz};
-    int a = f.axis;
-    if ((I[a] == 0 && c.bt[2 * a] == 2) || (I[a] == D[a] && c.bt[2 * a + 1] == 2)) U.u[a][f.e] = 0.0f;
+// mgpcg.py:374-392 apply_bc (walls): the wall faces only, one boundary plane
+// per blockIdx.y (side = 2 * axis + high)
+__global__ void k_apply_walls(G g, int nx, int ny, int nz, Faces U) {
+    count_launch(g.st);
+    const int side = blockIdx.y;
+    if (g.bt[side] != 2) return;
+    const int a = side >> 1, hi = side & 1;
+    const int d1 = a == 0 ? ny : nx;  // the plane's two axes, in order
+    const int d2 = a == 2 ? ny : nz;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < d1 * d2; t += gridDim.x * blockDim.x) {
+        const int u = t / d2, w = t - (t / d2) * d2;
+        int e;
+        if (a == 0) e = idx3(hi ? nx : 0, u, w, ny, nz);
+        else if (a == 1) e = idx3(u, hi ? ny : 0, w, ny + 1, nz);
+        else e = idx3(u, w, hi ? nz : 0, ny, nz + 1);
+        U.u[a][e] = 0.0f;
+    }
 }
 
 // mgpcg_solid.py:344-356: solid-cell velocities on their six faces
@@ -203,44 +318,51 @@ __global__ void k_apply_solid(SolveState* st, int nx, int ny, int nz, const int*
 // mgpcg.py:394-404 divergence + init(u_div, -1) (mgpcg.py:67-75); solid:
 // mgpcg_solid.py:359-372 (fluid-only divergence, its sum and count).  With
 // rhs != NULL the right-hand side is taken from rhs instead (edge_mgpcg_solve).
-__global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, double rel_tol, int max_iters) {
-    count_launch(c.st);
-    const Lvl& L = c.lv[0];
-    int n = L.n0 * L.n1 * L.n2;
+// One thread per slot handles the cell pair k = 2kk (plane (i+j)&1) and
+// k = 2kk+1 (the other plane).  x and p need no initialisation: the first
+// iteration writes them without reading them.
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_setup_rhs(G g, Lvl L, Fine f, Faces U, const float* rhs, double abs_tol,
+                                                   double rel_tol, int max_iters) {
+    count_launch(g.st);
+    const int ny = L.n1, nz = L.n2;
     double v[3] = {0.0, 0.0, 0.0};  // sum div (fluid), fluid count, sum r
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
-        float d;
-        bool fl = is_fluid(L.bm, e);
-        if (rhs) {
-            d = -rhs[e];
-        } else if (fl) {
-            const int nx = L.n0, ny = L.n1, nz = L.n2;
-            float vl = U.u[0][idx3(i, j, k, ny, nz)], vr = U.u[0][idx3(i + 1, j, k, ny, nz)];
-            float vb = U.u[1][idx3(i, j, k, ny + 1, nz)], vt = U.u[1][idx3(i, j + 1, k, ny + 1, nz)];
-            float va = U.u[2][idx3(i, j, k, ny, nz + 1)], vc = U.u[2][idx3(i, j, k + 1, ny, nz + 1)];
-            d = vr - vl + vt - vb + vc - va;
-            (void)nx;
-        } else {
-            d = 0.0f;
+    GRID_STRIDE(t, L.P) {
+        Slot s = slot_of(L, t);
+        const int c0 = (s.i + s.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = 2 * s.kk + h;
+            if (k >= nz) break;
+            const int e = idx3(s.i, s.j, k, ny, nz);
+            const bool fl = !SOLID || L.bm[e] <= 0;
+            float d;
+            if (rhs) {
+                d = -rhs[e];
+            } else if (fl) {
+                const int i = s.i, j = s.j;
+                float vl = U.u[0][idx3(i, j, k, ny, nz)], vr = U.u[0][idx3(i + 1, j, k, ny, nz)];
+                float vb = U.u[1][idx3(i, j, k, ny + 1, nz)], vt = U.u[1][idx3(i, j + 1, k, ny + 1, nz)];
+                float va = U.u[2][idx3(i, j, k, ny, nz + 1)], vc = U.u[2][idx3(i, j, k + 1, ny, nz + 1)];
+                d = vr - vl + vt - vb + vc - va;
+            } else {
+                d = 0.0f;
+            }
+            f.div[e] = d;
+            float r = d * -1.0f;
+            L.r[c0 ^ h][t] = r;
+            if (fl) {
+                v[0] += d;
+                v[1] += 1.0;
+            }
+            v[2] += r;
         }
-        c.div[e] = d;
-        float r = d * -1.0f;
-        L.r[e] = r;
-        c.x[e] = 0.0f;
-        c.p[0][e] = 0.0f;
-        c.p[1][e] = 0.0f;
-        if (fl) {
-            v[0] += d;
-            v[1] += 1.0;
-        }
-        v[2] += r;
     }
-    if (last_block<3>(c, 0, v)) {
+    if (last_block<3>(g, 0, v)) {
         double s[3];
-        final_sum<3>(c, 0, s);
+        final_sum<3>(g, 0, s);
         if (threadIdx.x == 0) {
-            SolveState* st = c.st;
+            SolveState* st = g.st;
             st->div_sum = (double)(float)s[0];
             st->n_fluid = (int)s[1];
             st->rsum = s[2];
@@ -253,37 +375,43 @@ __global__ void k_setup_rhs(Ctx c, Faces U, const float* rhs, double abs_tol, do
             st->beta = 0.0f;
             st->alpha = 0.0f;
             st->pcur = 0;
-            st->mean = st->all_neumann ? (float)(s[2] / (double)n) : 0.0f;
+            st->x_valid = 0;
+            st->mean = st->all_neumann ? (float)(s[2] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
         }
     }
 }
 
 // mgpcg_solid.py:374-383, 422-424: if the fluid divergence sums to > 0,
 // subtract its mean from every fluid cell; then the recentering mean.
-__global__ void k_solid_fix(Ctx c) {
-    count_launch(c.st);
-    const Lvl& L = c.lv[0];
-    int n = L.n0 * L.n1 * L.n2;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    SolveState* st = c.st;
+__global__ void __launch_bounds__(256) k_solid_fix(G g, Lvl L, Fine f) {
+    count_launch(g.st);
+    SolveState* st = g.st;
     float dsum = (float)st->div_sum;
     bool fix = dsum > 0.0f && st->n_fluid > 0;
     float avg = fix ? dsum / (float)st->n_fluid : 0.0f;
     double v[1] = {0.0};
-    for (; e < n; e += gridDim.x * blockDim.x) {
-        float r = L.r[e];
-        if (fix && is_fluid(L.bm, e)) {
-            float d = c.div[e] - avg;
-            c.div[e] = d;
-            r = d * -1.0f;
-            L.r[e] = r;
+    GRID_STRIDE(t, L.P) {
+        Slot s = slot_of(L, t);
+        const int c0 = (s.i + s.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = 2 * s.kk + h;
+            if (k >= L.n2) break;
+            const int e = idx3(s.i, s.j, k, L.n1, L.n2);
+            float r = L.r[c0 ^ h][t];
+            if (fix && L.bm[e] <= 0) {
+                float d = f.div[e] - avg;
+                f.div[e] = d;
+                r = d * -1.0f;
+                L.r[c0 ^ h][t] = r;
+            }
+            v[0] += r;
         }
-        v[0] += r;
     }
-    if (last_block<1>(c, 1, v)) {
+    if (last_block<1>(g, 1, v)) {
         double s[1];
-        final_sum<1>(c, 1, s);
-        if (threadIdx.x == 0) st->mean = st->all_neumann ? (float)(s[0] / (double)n) : 0.0f;
+        final_sum<1>(g, 1, s);
+        if (threadIdx.x == 0) st->mean = st->all_neumann ? (float)(s[0] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
     }
 }
 
@@ -301,52 +429,93 @@ __global__ void k_downsample_bm(SolveState* st, const int* fine, int* coarse, in
     coarse[e] = all;
 }
 
+// neighbour codes of one level from its mask: the neighbour_sum conditions
+// (mgpcg_solid.py:99-111) and num_fluid_neighbors (mgpcg_solid.py:113-130)
+__global__ void __launch_bounds__(256) k_codes(G g, Lvl L) {
+    count_launch(g.st);
+    const int n1 = L.n1, n2 = L.n2;
+    GRID_STRIDE(t, L.n0 * L.n1 * L.n2) {
+        int row = fdiv(t, L.d2);
+        int k = t - row * n2;
+        int i = fdiv(row, L.d1);
+        int j = row - i * n1;
+        auto solid = [&](int a, int b, int c) { return L.bm[idx3(a, b, c, n1, n2)] > 0; };
+        unsigned code = solid(i, j, k) ? 0u : (unsigned)CELL_FLUID;
+        int num = 6;
+        int I[3] = {i, j, k}, D[3] = {L.n0, n1, n2};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            int up[3] = {i, j, k}, dn[3] = {i, j, k};
+            up[a] += 1;
+            dn[a] -= 1;
+            bool has_up = I[a] < D[a] - 1, has_dn = I[a] > 0;
+            bool up_solid = has_up && solid(up[0], up[1], up[2]);
+            bool dn_solid = has_dn && solid(dn[0], dn[1], dn[2]);
+            if (has_up && !up_solid) code |= 1u << (2 * a);
+            if (has_dn && !dn_solid) code |= 2u << (2 * a);
+            if (!has_dn && g.bt[2 * a] == 2) num -= 1;
+            else if (dn_solid) num -= 1;
+            if (!has_up && g.bt[2 * a + 1] == 2) num -= 1;
+            else if (up_solid) num -= 1;
+        }
+        code |= (unsigned)num << 8;
+        L.code[(i + j + k) & 1][(i * n1 + j) * L.H + (k >> 1)] = (unsigned short)code;
+    }
+}
+
+template <bool SOLID>
+EDGE_D unsigned code_at(const Lvl& L, int plane, int e, int i, int j, int k) {
+    return SOLID ? (unsigned)L.code[plane][e] : range_code(L, i, j, k);
+}
+
 // ---------------------------------------------------------------------------
-// CG vector kernels
+// CG vector kernels (one thread per slot: the cell pair k = 2kk, 2kk+1)
 // ---------------------------------------------------------------------------
 // update_p (mgpcg.py:143-145) fused into compute_Ap (mgpcg.py:112-117):
-// p_new = z + beta p_old on the fly (also at the stencil neighbours), Ap,
+// p_new = z + beta p_old on the fly (also at the stencil neighbours), A p_new
 // and the p.Ap partials; the last block forms alpha (mgpcg.py:237-240).
-__global__ void __launch_bounds__(256) k_cg_ap(Ctx c) {
-    count_launch(c.st);
+// Products are rounded before the sums (no fused multiply-add), as the
+// reference's separate kernels round them.
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
+    count_launch(g.st);
     // The loop stops unless the iteration's last kernel completes its
     // reduction and asks to continue: a lost reduction can never spin.
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        set_cond(c, 0);
-        if (c.st->it > c.st->max_iters + 8) c.st->status = ST_NOCONV;  // hard cap
+        set_cond(g, 0);
+        if (g.st->it > g.st->max_iters + 8) g.st->status = ST_NOCONV;  // hard cap
     }
-    if (!running(c)) return;
-    const Lvl& L = c.lv[0];
-    const int n = L.n0 * L.n1 * L.n2;
-    SolveState* st = c.st;
+    if (!running(g)) return;
+    SolveState* st = g.st;
     const int pc = st->pcur;
-    const float* __restrict__ po = c.p[pc];
-    float* __restrict__ pn = c.p[pc ^ 1];
-    const float* __restrict__ z = L.z;
+    const bool first = st->it == 0;  // p = 0 before the first update_p (mgpcg.py:61-66)
     const float beta = st->beta;
-    const int s0 = L.n1 * L.n2, s1 = L.n2;
     double v[1] = {0.0};
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        float pe = 0.0f, ape = 0.0f;
-        if (is_fluid(L.bm, e)) {
-            int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / s0;
-            pe = __ldg(z + e) + beta * __ldg(po + e);
-            float nsum = 0.0f;
-            if (i < L.n0 - 1 && is_fluid(L.bm, e + s0)) nsum += __ldg(z + e + s0) + beta * __ldg(po + e + s0);
-            if (i > 0 && is_fluid(L.bm, e - s0)) nsum += __ldg(z + e - s0) + beta * __ldg(po + e - s0);
-            if (j < L.n1 - 1 && is_fluid(L.bm, e + s1)) nsum += __ldg(z + e + s1) + beta * __ldg(po + e + s1);
-            if (j > 0 && is_fluid(L.bm, e - s1)) nsum += __ldg(z + e - s1) + beta * __ldg(po + e - s1);
-            if (k < L.n2 - 1 && is_fluid(L.bm, e + 1)) nsum += __ldg(z + e + 1) + beta * __ldg(po + e + 1);
-            if (k > 0 && is_fluid(L.bm, e - 1)) nsum += __ldg(z + e - 1) + beta * __ldg(po + e - 1);
-            ape = n_fluid(c, L, i, j, k) * pe - nsum;
-            v[0] += (double)pe * (double)ape;
+    GRID_STRIDE(t, L.P) {
+        Slot s = slot_of(L, t);
+        const int c0 = (s.i + s.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = 2 * s.kk + h, pl = c0 ^ h;
+            if (k >= L.n2) break;
+            const unsigned code = code_at<SOLID>(L, pl, t, s.i, s.j, k);
+            float pe = 0.0f;
+            if (code & CELL_FLUID) {
+                const float* __restrict__ zo = L.z[pl ^ 1];
+                const float* __restrict__ po = f.p[pc][pl ^ 1];
+                pe = first ? __ldg(L.z[pl] + t) : __fadd_rn(__ldg(L.z[pl] + t), __fmul_rn(beta, __ldg(f.p[pc][pl] + t)));
+                float ns = nbr_sum(L, code, t, k, [&](int e, int) {
+                    return first ? __ldg(zo + e) : __fadd_rn(__ldg(zo + e), __fmul_rn(beta, __ldg(po + e)));
+                });
+                float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, L, code, s.i, s.j, k), pe), ns);
+                v[0] += (double)pe * (double)ape;
+            }
+            f.p[pc ^ 1][pl][t] = pe;
         }
-        pn[e] = pe;
-        c.Ap[e] = ape;
     }
-    if (last_block<1>(c, 2, v)) {
+    if (last_block<1>(g, 2, v)) {
         double sm[1];
-        final_sum<1>(c, 2, sm);
+        final_sum<1>(g, 2, sm);
         if (threadIdx.x == 0) {
             double pAp = (double)(float)sm[0];
             st->pAp = pAp;
@@ -356,37 +525,53 @@ __global__ void __launch_bounds__(256) k_cg_ap(Ctx c) {
     }
 }
 
-// update_x / update_r (mgpcg.py:133-141), r.r (mgpcg.py:247-249), the
-// convergence test (mgpcg.py:254) and the recentering sum (mgpcg.py:169-175).
-// Solid cells only take the recentering (mgpcg_solid.py:197-202).
-__global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
-    count_launch(c.st);
-    if (!running(c)) return;
-    const Lvl& L = c.lv[0];
-    int n = L.n0 * L.n1 * L.n2;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    SolveState* st = c.st;
-    float alpha = st->alpha, mean = st->mean;
-    const float* __restrict__ p = c.p[st->pcur];
+// update_x / update_r (mgpcg.py:133-141) with A p recomputed from p, r.r
+// (mgpcg.py:247-249), the convergence test (mgpcg.py:254) and the
+// recentering sum (mgpcg.py:169-175).  Solid cells only take the recentering
+// (mgpcg_solid.py:197-202).
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_cg_xr(G g, Lvl L, Fine f) {
+    count_launch(g.st);
+    if (!running(g)) return;
+    SolveState* st = g.st;
+    const float alpha = st->alpha, mean = st->mean;
+    const bool first = st->it == 0;  // x = 0 before the first update_x
+    const int pc = st->pcur;
     double v[2] = {0.0, 0.0};
-    for (; e < n; e += gridDim.x * blockDim.x) {
-        float r = L.r[e] - mean;
-        if (is_fluid(L.bm, e)) {
-            c.x[e] += alpha * __ldg(p + e);
-            r -= alpha * __ldg(c.Ap + e);
-            v[0] += (double)r * (double)r;
+    GRID_STRIDE(t, L.P) {
+        Slot s = slot_of(L, t);
+        const int c0 = (s.i + s.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = 2 * s.kk + h, pl = c0 ^ h;
+            if (k >= L.n2) break;
+            const unsigned code = code_at<SOLID>(L, pl, t, s.i, s.j, k);
+            float r = L.r[pl][t] - mean;
+            float* xp = f.x[pl] + t;
+            if (code & CELL_FLUID) {
+                const float* __restrict__ po = f.p[pc][pl ^ 1];
+                const float pe = __ldg(f.p[pc][pl] + t);
+                *xp = first ? __fmul_rn(alpha, pe) : __fadd_rn(*xp, __fmul_rn(alpha, pe));
+                float ns = nbr_sum(L, code, t, k, [&](int e, int) { return __ldg(po + e); });
+                float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, L, code, s.i, s.j, k), pe), ns);
+                r = __fsub_rn(r, __fmul_rn(alpha, ape));
+                v[0] += (double)r * (double)r;
+            } else if (first) {
+                *xp = 0.0f;
+            }
+            L.r[pl][t] = r;
+            v[1] += r;
         }
-        L.r[e] = r;
-        v[1] += r;
     }
-    if (last_block<2>(c, 3, v)) {
+    if (last_block<2>(g, 3, v)) {
         double s[2];
-        final_sum<2>(c, 3, s);
+        final_sum<2>(g, 3, s);
         if (threadIdx.x == 0) {
             double rTr = (double)(float)s[0];
             st->rTr = rTr;
             st->rsum = s[1];
-            st->mean = st->all_neumann ? (float)(s[1] / (double)n) : 0.0f;
+            st->x_valid = 1;
+            st->mean = st->all_neumann ? (float)(s[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
             if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
             else if (rTr < st->tol) st->status = ST_CONVERGED;
         }
@@ -397,221 +582,205 @@ __global__ void __launch_bounds__(256) k_cg_xr(Ctx c) {
 // V-cycle (mgpcg.py:177-195)
 // ---------------------------------------------------------------------------
 // Red-black Gauss-Seidel (mgpcg.py:160-167) runs as half sweeps: a half sweep
-// of colour c updates the cells with (i+j+k)&1 == c and reads only cells of
-// the other colour, so no update depends on another in the same launch, and a
-// cell's own old value is never read.  Hence:
-//   * z = 0 before the first down sweep needs no fill (that half sweep reads
-//     nothing, mode HS_FIRST);
+// of colour c updates the colour-c cells and reads only cells of the other
+// colour, so no update depends on another in the same launch, and a cell's
+// own old value is never read.  Hence:
+//   * z = 0 before the first down sweep needs no fill: that half sweep reads
+//     nothing (HS_FIRST); below the fine level the restriction writes it;
 //   * the prolongation z[l] += z[l+1][I/2] (mgpcg.py:155-158) that precedes
 //     the up sweeps is applied on the fly to the neighbours the first up half
-//     sweep reads (mode HS_PROLONG): every cell is overwritten by a half sweep
+//     sweep reads (HS_PROLONG): every cell is overwritten by a half sweep
 //     before its own value is read again, and solid cells are never read.
-// Levels with more cells than fit in shared memory use one thread per pair
-// of cells along k (the pair holds one cell of each colour); the remaining
-// coarse levels run as one thread block in shared memory (k_coarse).
 enum { HS_FIRST = 0, HS_PLAIN = 1, HS_PROLONG = 2, HS_ZR = 3 };
 
-EDGE_D float nb_val(const Lvl& L, const Lvl* C, int e, int i, int j, int k, bool prolong) {
-    float v = __ldg(L.z + e);
-    if (prolong) v += __ldg(C->z + idx3(i >> 1, j >> 1, k >> 1, C->n1, C->n2));
-    return v;
-}
-
-template <int MODE>
-__global__ void __launch_bounds__(256) k_hsweep(Ctx c, int l, int color) {
-    count_launch(c.st);
-    if (!running(c)) {
-        if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(c, 0);
+template <int MODE, bool SOLID>
+__global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, int color) {
+    count_launch(g.st);
+    if (!running(g)) {
+        if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
-    const Lvl& L = c.lv[l];
-    const Lvl* C = MODE == HS_PROLONG ? &c.lv[l + 1] : nullptr;
-    const float mean = l == 0 ? c.st->mean : 0.0f;
-    const int h2 = L.n2 >> 1;
-    const int npair = L.n0 * L.n1 * h2;
+    const float mean = level0 ? g.st->mean : 0.0f;
+    const int oc = color ^ 1;
+    const float* __restrict__ rs = L.r[color];
+    const float* __restrict__ zo = L.z[oc];
+    float* __restrict__ zs = L.z[color];
     double v[1] = {0.0};
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npair; t += gridDim.x * blockDim.x) {
-        int kk = t % h2, r = t / h2;
-        int j = r % L.n1, i = r / L.n1;
-        int k = 2 * kk + ((i + j + color) & 1);
-        int e = idx3(i, j, k, L.n1, L.n2);
-        const int s1 = L.n2, s0 = L.n1 * L.n2;
-        float rv = __ldg(L.r + e) - mean;
-        float zn = 0.0f;
-        if (is_fluid(L.bm, e)) {
-            float ns = 0.0f;
-            if (MODE != HS_FIRST) {
-                const bool pr = MODE == HS_PROLONG;
-                if (k < L.n2 - 1 && is_fluid(L.bm, e + 1)) ns += nb_val(L, C, e + 1, i, j, k + 1, pr);
-                if (k > 0 && is_fluid(L.bm, e - 1)) ns += nb_val(L, C, e - 1, i, j, k - 1, pr);
-                if (j < L.n1 - 1 && is_fluid(L.bm, e + s1)) ns += nb_val(L, C, e + s1, i, j + 1, k, pr);
-                if (j > 0 && is_fluid(L.bm, e - s1)) ns += nb_val(L, C, e - s1, i, j - 1, k, pr);
-                if (i < L.n0 - 1 && is_fluid(L.bm, e + s0)) ns += nb_val(L, C, e + s0, i + 1, j, k, pr);
-                if (i > 0 && is_fluid(L.bm, e - s0)) ns += nb_val(L, C, e - s0, i - 1, j, k, pr);
+    GRID_STRIDE(t, L.P) {
+        Slot s = slot_of(L, t);
+        const int k = 2 * s.kk + ((s.i + s.j + color) & 1);
+        if (k < L.n2) {
+            const unsigned code = code_at<SOLID>(L, color, t, s.i, s.j, k);
+            if (code & CELL_FLUID) {
+                const float rv = __ldg(rs + t) - mean;
+                float ns = 0.0f;
+                if (MODE == HS_PROLONG) {
+                    ns = nbr_sum(L, code, t, k, [&](int e, int d) {
+                        int di, dj, dk;
+                        dir_offset(d, di, dj, dk);
+                        return __ldg(zo + e) + parent_z(C, C.z[0], C.z[1], s.i + di, s.j + dj, k + dk);
+                    });
+                } else if (MODE != HS_FIRST) {
+                    ns = nbr_sum(L, code, t, k, [&](int e, int) { return __ldg(zo + e); });
+                }
+                const float zn = (rv + ns) / nf_of<SOLID>(g.bt, L, code, s.i, s.j, k);
+                zs[t] = zn;
+                if (MODE == HS_ZR) v[0] += (double)zn * (double)rv;
             }
-            // neighbour_sum order differs from the reference's (+x,-x,+y,...):
-            // a rounding-level difference
-            zn = (rv + ns) / n_fluid(c, L, i, j, k);
-            L.z[e] = zn;
-            if (MODE == HS_ZR) v[0] += (double)zn * (double)rv;
         }
         if (MODE == HS_ZR) {
-            // the other cell of the pair (final from the previous half sweep)
-            int kp = k ^ 1;
-            int ep = idx3(i, j, kp, L.n1, L.n2);
-            if (is_fluid(L.bm, ep)) v[0] += (double)__ldg(L.z + ep) * (double)(__ldg(L.r + ep) - mean);
+            // the other cell of the slot (final from the previous half sweep)
+            const int ko = 2 * s.kk + ((s.i + s.j + oc) & 1);
+            if (ko < L.n2 && (code_at<SOLID>(L, oc, t, s.i, s.j, ko) & CELL_FLUID))
+                v[0] += (double)__ldg(zo + t) * (double)(__ldg(L.r[oc] + t) - mean);
         }
     }
     if (MODE == HS_ZR) {
         // mgpcg.py:263-275: z.r, beta, update bookkeeping, loop condition
-        if (last_block<1>(c, 4, v)) {
+        if (last_block<1>(g, 4, v)) {
             double sm[1];
-            final_sum<1>(c, 4, sm);
-            if (threadIdx.x == 0) {
-                SolveState* st = c.st;
-                double zTr = (double)(float)sm[0];
-                if (st->setup) {
-                    st->setup = 0;
-                    st->zTr = zTr;
-                    st->beta = 0.0f;
-                    st->tol = fmax(st->abs_tol, zTr * st->rel_tol);
-                    if (st->max_iters <= 0) st->status = ST_NOCONV;
-                } else {
-                    st->beta = (float)(zTr / (st->zTr + 1e-12));
-                    st->zTr = zTr;
-                    st->it += 1;
-                    if (st->it >= st->max_iters) st->status = ST_NOCONV;
-                }
-                set_cond(c, st->status == ST_RUNNING ? 1u : 0u);
-            }
+            final_sum<1>(g, 4, sm);
+            if (threadIdx.x == 0) zr_epilogue(g, sm[0]);
         }
     }
 }
 
 // restrict (mgpcg.py:147-153): r[l+1] = sum over the 8 children of
-// (r - A z) / (dim - 1), solid children skipped (mgpcg_solid.py:168-174)
-__global__ void __launch_bounds__(256) k_restrict(Ctx c, int l) {
-    count_launch(c.st);
-    if (!running(c)) return;
-    const Lvl& L = c.lv[l];
-    const Lvl& C = c.lv[l + 1];
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= C.n0 * C.n1 * C.n2) return;
-    const float mean = l == 0 ? c.st->mean : 0.0f;
-    int K = e % C.n2, J = (e / C.n2) % C.n1, I = e / (C.n1 * C.n2);
-    const float* __restrict__ z = L.z;
-    float acc = 0.0f;
-    int stride[3] = {L.n1 * L.n2, L.n2, 1};
-    for (int a = 0; a < 2; a++)
-        for (int b = 0; b < 2; b++)
-            for (int q = 0; q < 2; q++) {
-                int i = 2 * I + a, j = 2 * J + b, k = 2 * K + q;
-                int f = idx3(i, j, k, L.n1, L.n2);
-                if (!is_fluid(L.bm, f)) continue;
-                int Ix[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
-                float ns = 0.0f;
+// (r - A z) / (dim - 1), solid children skipped (mgpcg_solid.py:168-174).
+// One thread per coarse cell; the children of (I,J,K) all sit at slot
+// (i*n1 + j)*H + K of their planes.  With `first` it also applies the first
+// half sweep of the coarse level (z = r / n_fluid on colour 0).
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0, int first) {
+    count_launch(g.st);
+    if (!running(g)) return;
+    const float mean = level0 ? g.st->mean : 0.0f;
+    GRID_STRIDE(t, C.n0 * C.n1 * C.n2) {
+        const int rowc = fdiv(t, C.d2);
+        const int K = t - rowc * C.n2;
+        const int I = fdiv(rowc, C.d1);
+        const int J = rowc - I * C.n1;
+        float acc = 0.0f;
 #pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    if (Ix[d] < D[d] - 1 && is_fluid(L.bm, f + stride[d])) ns += __ldg(z + f + stride[d]);
-                    if (Ix[d] > 0 && is_fluid(L.bm, f - stride[d])) ns += __ldg(z + f - stride[d]);
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int i = 2 * I + a, j = 2 * J + b, k = 2 * K + q;
+                    const int pl = (i + j + k) & 1;
+                    const int e = (i * F.n1 + j) * F.H + K;
+                    const unsigned code = code_at<SOLID>(F, pl, e, i, j, k);
+                    if (!(code & CELL_FLUID)) continue;
+                    const float* __restrict__ zo = F.z[pl ^ 1];
+                    float ns = nbr_sum(F, code, e, k, [&](int ee, int) { return __ldg(zo + ee); });
+                    float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, F, code, i, j, k), __ldg(F.z[pl] + e)), ns);
+                    float res = (__ldg(F.r[pl] + e) - mean) - az;
+                    acc += res * 0.5f;
                 }
-                float res = (__ldg(L.r + f) - mean) - (n_fluid(c, L, i, j, k) * __ldg(z + f) - ns);
-                acc += res * 0.5f;
-            }
-    C.r[e] = acc;
+        const int pc = (I + J + K) & 1;
+        const int ec = (I * C.n1 + J) * C.H + (K >> 1);
+        C.r[pc][ec] = acc;
+        if (first && pc == 0) {
+            const unsigned cc = code_at<SOLID>(C, 0, ec, I, J, K);
+            if (cc & CELL_FLUID) C.z[0][ec] = (acc + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K);
+        }
+    }
 }
 
 // The coarse levels lc..L-1 of a V-cycle in one thread block out of shared
-// memory: down sweeps + restriction, 20 bottom sweeps, prolongation + up
-// sweeps (mgpcg.py:177-195); z[lc] is written back for the prolongation into
-// level lc-1.  With ZR (the whole grid fits, lc == 0) it also forms z.r and
-// runs the end-of-iteration bookkeeping.
-struct CoarseLvl {
-    int n0, n1, n2, off;  // off: float offset of r (z follows) in shared memory
+// memory (same red-black layout): down sweeps + restriction, 20 bottom
+// sweeps, prolongation + up sweeps (mgpcg.py:177-195); z[lc] is written back
+// for the prolongation into level lc-1.  Levels of at most 32 slots per plane
+// run on one warp.  With ZR (the whole grid fits, lc == 0) it also forms z.r
+// and runs the end-of-iteration bookkeeping.
+struct CLvl {
+    int n0, n1, n2, H, P;
+    FDiv dH, d1, d2;
+    int roff, zoff, coff;  // float offsets of the r and z planes, ushort offset of the codes
 };
-EDGE_D bool c_fluid(const unsigned char* bm, int e) { return bm == nullptr || bm[e] == 0; }
 
-template <bool ZR>
-__global__ void __launch_bounds__(1024) k_coarse(Ctx c, int lc, int moff) {
+template <bool ZR, bool SOLID>
+__global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     extern __shared__ float sh[];
-    count_launch(c.st);
-    if (!running(c)) {
-        if (ZR && threadIdx.x == 0) set_cond(c, 0);
+    __shared__ CLvl cl[16];
+    count_launch(g.st);
+    if (!running(g)) {
+        if (ZR && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
-    const int L = c.L;
-    const bool solid = c.lv[0].bm != nullptr;
-    unsigned char* bmall = reinterpret_cast<unsigned char*>(sh + moff);
-    const float mean = lc == 0 ? c.st->mean : 0.0f;
-    // layout
-    CoarseLvl cl[16];
-    int off = 0, boff = 0, bo[16];
-    for (int l = lc; l < L; l++) {
-        cl[l].n0 = c.lv[l].n0; cl[l].n1 = c.lv[l].n1; cl[l].n2 = c.lv[l].n2;
-        cl[l].off = off;
-        int n = cl[l].n0 * cl[l].n1 * cl[l].n2;
-        off += 2 * n;
-        bo[l] = boff;
-        boff += n;
+    const int L = a.L, lc = a.lc;
+    if (threadIdx.x == 0) {
+        // per level: r plane 0, r plane 1, z plane 0, z plane 1 (floats); the
+        // solid codes (two planes per level) follow all the floats
+        int off = 0;
+        for (int l = lc; l < L; l++) {
+            const Lvl& V = a.lv[l];
+            CLvl q;
+            q.n0 = V.n0; q.n1 = V.n1; q.n2 = V.n2; q.H = V.H; q.P = V.P;
+            q.dH = V.dH; q.d1 = V.d1; q.d2 = V.d2;
+            q.roff = off;
+            q.zoff = off + 2 * V.P;
+            off += 4 * V.P;
+            cl[l] = q;
+        }
+        int coff = 2 * off;  // in unsigned shorts from the start of shared memory
+        for (int l = lc; l < L; l++) {
+            cl[l].coff = coff;
+            coff += 2 * cl[l].P;
+        }
     }
-    // load r[lc] and the masks
+    __syncthreads();
+    unsigned short* codes = reinterpret_cast<unsigned short*>(sh);
+    const float mean = lc == 0 ? g.st->mean : 0.0f;
     {
-        int n = cl[lc].n0 * cl[lc].n1 * cl[lc].n2;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) sh[cl[lc].off + e] = __ldg(c.lv[lc].r + e) - mean;
-        if (solid)
+        const CLvl& q = cl[lc];
+        for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
+            const float* src = e < q.P ? a.lv[lc].r[0] + e : a.lv[lc].r[1] + (e - q.P);
+            sh[q.roff + e] = __ldg(src) - mean;
+        }
+        if (SOLID)
             for (int l = lc; l < L; l++) {
-                int m = cl[l].n0 * cl[l].n1 * cl[l].n2;
-                for (int e = threadIdx.x; e < m; e += blockDim.x) bmall[bo[l] + e] = __ldg(c.lv[l].bm + e) > 0;
+                const CLvl& u = cl[l];
+                for (int e = threadIdx.x; e < 2 * u.P; e += blockDim.x)
+                    codes[u.coff + e] = e < u.P ? a.lv[l].code[0][e] : a.lv[l].code[1][e - u.P];
             }
     }
     __syncthreads();
+    // one half sweep; mode 0: from zero, 1: plain, 2: with the prolongation of l+1
     auto half = [&](int l, int color, int mode) {
-        // mode: 0 from zero, 1 plain, 2 with the prolongation of l+1
-        const CoarseLvl& q = cl[l];
-        float* r = sh + q.off;
-        float* z = r + q.n0 * q.n1 * q.n2;
-        const unsigned char* bm = solid ? bmall + bo[l] : nullptr;
-        const float* zc = mode == 2 ? sh + cl[l + 1].off + cl[l + 1].n0 * cl[l + 1].n1 * cl[l + 1].n2 : nullptr;
-        int n = q.n0 * q.n1 * q.n2;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            int k = e % q.n2, j = (e / q.n2) % q.n1, i = e / (q.n1 * q.n2);
-            if (((i + j + k) & 1) != color || !c_fluid(bm, e)) continue;
-            float ns = 0.0f;
-            if (mode != 0) {
-                int I[3] = {i, j, k}, D[3] = {q.n0, q.n1, q.n2}, S[3] = {q.n1 * q.n2, q.n2, 1};
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    for (int sgn = -1; sgn <= 1; sgn += 2) {
-                        int ni = I[a] + sgn;
-                        if (ni < 0 || ni >= D[a]) continue;
-                        int f = e + sgn * S[a];
-                        if (!c_fluid(bm, f)) continue;
-                        float v = z[f];
-                        if (mode == 2) {
-                            int J[3] = {i, j, k};
-                            J[a] = ni;
-                            const CoarseLvl& u = cl[l + 1];
-                            v += zc[((J[0] >> 1) * u.n1 + (J[1] >> 1)) * u.n2 + (J[2] >> 1)];
-                        }
-                        ns += v;
-                    }
+        const CLvl& q = cl[l];
+        const bool small = q.P <= 32;
+        if (!small || threadIdx.x < 32) {
+            const int step = small ? 32 : blockDim.x;
+            const float* r = sh + q.roff + color * q.P;
+            float* z = sh + q.zoff + color * q.P;
+            const float* zo = sh + q.zoff + (color ^ 1) * q.P;
+            const unsigned short* cd = codes + q.coff + color * q.P;
+            for (int t = threadIdx.x; t < q.P; t += step) {
+                Slot s = slot_of(q, t);
+                const int k = 2 * s.kk + ((s.i + s.j + color) & 1);
+                if (k >= q.n2) continue;
+                const unsigned code = SOLID ? (unsigned)cd[t] : range_code(q, s.i, s.j, k);
+                if (!(code & CELL_FLUID)) continue;
+                float ns = 0.0f;
+                if (mode == 1) {
+                    ns = nbr_sum(q, code, t, k, [&](int e, int) { return zo[e]; });
+                } else if (mode == 2) {
+                    const CLvl& u = cl[l + 1];
+                    const float* zc0 = sh + u.zoff;
+                    const float* zc1 = zc0 + u.P;
+                    ns = nbr_sum(q, code, t, k, [&](int e, int d) {
+                        int di, dj, dk;
+                        dir_offset(d, di, dj, dk);
+                        return zo[e] + parent_z(u, zc0, zc1, s.i + di, s.j + dj, k + dk);
+                    });
                 }
+                z[t] = (r[t] + ns) / nf_of<SOLID>(g.bt, q, code, s.i, s.j, k);
             }
-            // num_fluid_neighbors (mgpcg.py:100-110 / mgpcg_solid.py:113-130)
-            float num = 6.0f;
-            {
-                int I[3] = {i, j, k}, D[3] = {q.n0, q.n1, q.n2}, S[3] = {q.n1 * q.n2, q.n2, 1};
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    if (I[a] <= 0 && c.bt[2 * a] == 2) num -= 1.0f;
-                    else if (bm && I[a] > 0 && bm[e - S[a]]) num -= 1.0f;
-                    if (I[a] >= D[a] - 1 && c.bt[2 * a + 1] == 2) num -= 1.0f;
-                    else if (bm && I[a] < D[a] - 1 && bm[e + S[a]]) num -= 1.0f;
-                }
-            }
-            z[e] = (r[e] + ns) / num;
         }
-        __syncthreads();
+        if (small) __syncwarp();
+        else __syncthreads();
     };
     // down
     for (int l = lc; l < L - 1; l++) {
@@ -619,37 +788,34 @@ __global__ void __launch_bounds__(1024) k_coarse(Ctx c, int lc, int moff) {
         half(l, 1, 1);
         half(l, 0, 1);
         half(l, 1, 1);
+        __syncthreads();
         // restrict into r[l+1]
-        const CoarseLvl& q = cl[l];
-        const CoarseLvl& u = cl[l + 1];
-        float* r = sh + q.off;
-        float* z = r + q.n0 * q.n1 * q.n2;
-        float* rc = sh + u.off;
-        const unsigned char* bm = solid ? bmall + bo[l] : nullptr;
-        int m = u.n0 * u.n1 * u.n2;
+        const CLvl& q = cl[l];
+        const CLvl& u = cl[l + 1];
+        const int m = u.n0 * u.n1 * u.n2;
         for (int ce = threadIdx.x; ce < m; ce += blockDim.x) {
-            int K = ce % u.n2, J = (ce / u.n2) % u.n1, I = ce / (u.n1 * u.n2);
+            const int rowc = fdiv(ce, u.d2);
+            const int K = ce - rowc * u.n2;
+            const int I = fdiv(rowc, u.d1);
+            const int J = rowc - I * u.n1;
             float acc = 0.0f;
-            for (int a = 0; a < 2; a++)
+            for (int aa = 0; aa < 2; aa++)
                 for (int b = 0; b < 2; b++)
                     for (int cc = 0; cc < 2; cc++) {
-                        int i = 2 * I + a, j = 2 * J + b, k = 2 * K + cc;
-                        int e = (i * q.n1 + j) * q.n2 + k;
-                        if (!c_fluid(bm, e)) continue;
-                        int Ix[3] = {i, j, k}, D[3] = {q.n0, q.n1, q.n2}, S[3] = {q.n1 * q.n2, q.n2, 1};
-                        float ns = 0.0f, num = 6.0f;
-                        for (int d = 0; d < 3; d++) {
-                            if (Ix[d] < D[d] - 1 && c_fluid(bm, e + S[d])) ns += z[e + S[d]];
-                            if (Ix[d] > 0 && c_fluid(bm, e - S[d])) ns += z[e - S[d]];
-                            if (Ix[d] <= 0 && c.bt[2 * d] == 2) num -= 1.0f;
-                            else if (bm && Ix[d] > 0 && bm[e - S[d]]) num -= 1.0f;
-                            if (Ix[d] >= D[d] - 1 && c.bt[2 * d + 1] == 2) num -= 1.0f;
-                            else if (bm && Ix[d] < D[d] - 1 && bm[e + S[d]]) num -= 1.0f;
-                        }
-                        float res = r[e] - (num * z[e] - ns);
+                        const int i = 2 * I + aa, j = 2 * J + b, k = 2 * K + cc;
+                        const int pl = (i + j + k) & 1;
+                        const int e = (i * q.n1 + j) * q.H + K;
+                        const unsigned code =
+                            SOLID ? (unsigned)codes[q.coff + pl * q.P + e] : range_code(q, i, j, k);
+                        if (!(code & CELL_FLUID)) continue;
+                        const float* zo = sh + q.zoff + (pl ^ 1) * q.P;
+                        float ns = nbr_sum(q, code, e, k, [&](int ee, int) { return zo[ee]; });
+                        float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, q, code, i, j, k), sh[q.zoff + pl * q.P + e]),
+                                             ns);
+                        float res = sh[q.roff + pl * q.P + e] - az;
                         acc += res * 0.5f;
                     }
-            rc[ce] = acc;
+            sh[u.roff + ((I + J + K) & 1) * u.P + (I * u.n1 + J) * u.H + (K >> 1)] = acc;
         }
         __syncthreads();
     }
@@ -660,76 +826,460 @@ __global__ void __launch_bounds__(1024) k_coarse(Ctx c, int lc, int moff) {
         half(L - 1, 0, 1);
         half(L - 1, 1, 1);
     }
+    __syncthreads();
     // up
     for (int l = L - 2; l >= lc; l--) {
         half(l, 1, 2);
         half(l, 0, 1);
         half(l, 1, 1);
         half(l, 0, 1);
+        __syncthreads();
     }
     // write back z[lc] (solid cells keep their last value, never read)
     {
-        const CoarseLvl& q = cl[lc];
-        int n = q.n0 * q.n1 * q.n2;
-        const float* z = sh + q.off + n;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) c.lv[lc].z[e] = z[e];
+        const CLvl& q = cl[lc];
+        for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
+            float* dst = e < q.P ? a.lv[lc].z[0] + e : a.lv[lc].z[1] + (e - q.P);
+            *dst = sh[q.zoff + e];
+        }
     }
     if (ZR) {
-        const CoarseLvl& q = cl[lc];
-        int n = q.n0 * q.n1 * q.n2;
-        const float* r = sh + q.off;
-        const float* z = r + n;
+        const CLvl& q = cl[lc];
         double v[1] = {0.0};
-        for (int e = threadIdx.x; e < n; e += blockDim.x)
-            if (c_fluid(solid ? bmall + bo[lc] : nullptr, e)) v[0] += (double)z[e] * (double)r[e];
+        for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
+            const int color = e < q.P ? 0 : 1, t = e - color * q.P;
+            Slot s = slot_of(q, t);
+            const int k = 2 * s.kk + ((s.i + s.j + color) & 1);
+            if (k >= q.n2) continue;
+            const bool fl = SOLID ? (codes[q.coff + e] & CELL_FLUID) != 0 : true;
+            if (fl) v[0] += (double)sh[q.zoff + e] * (double)sh[q.roff + e];
+        }
         block_sum<1>(v);
-        if (threadIdx.x == 0) {
-            SolveState* st = c.st;
-            double zTr = (double)(float)v[0];
-            if (st->setup) {
-                st->setup = 0;
-                st->zTr = zTr;
-                st->beta = 0.0f;
-                st->tol = fmax(st->abs_tol, zTr * st->rel_tol);
-                if (st->max_iters <= 0) st->status = ST_NOCONV;
-            } else {
-                st->beta = (float)(zTr / (st->zTr + 1e-12));
-                st->zTr = zTr;
-                st->it += 1;
-                if (st->it >= st->max_iters) st->status = ST_NOCONV;
+        if (threadIdx.x == 0) zr_epilogue(g, v[0]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Four slots per thread (levels with H % 4 == 0): one float4 per plane row
+// segment instead of four scalar loads, same arithmetic in the same order.
+// ---------------------------------------------------------------------------
+EDGE_D void ld4(const float* p, float (&v)[4]) {
+    float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+// coherent load (the thread itself rewrites these words in the same kernel)
+EDGE_D void ld4c(const float* p, float (&v)[4]) {
+    float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+EDGE_D void st4(float* p, const float (&v)[4]) { *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]); }
+
+// slots kk0..kk0+3 of row (i, j); t0 = the first slot's index in a plane
+struct Quad {
+    int i, j, kk0, t0;
+};
+EDGE_D Quad quad_of(const Lvl& L, int t) {
+    int row = fdiv(t, L.dQ);
+    int i = fdiv(row, L.d1);
+    int kk0 = (t - row * (L.H >> 2)) << 2;
+    return Quad{i, row - i * L.n1, kk0, row * L.H + kk0};
+}
+
+// codes of the four cells of plane `plane` (parity p: k = 2 kk + p)
+template <bool SOLID>
+EDGE_D void quad_codes(const Lvl& L, int plane, const Quad& q, int p, unsigned (&code)[4]) {
+    if (SOLID) {
+        ushort4 c = *reinterpret_cast<const ushort4*>(L.code[plane] + q.t0);
+        code[0] = c.x; code[1] = c.y; code[2] = c.z; code[3] = c.w;
+    } else {
+#pragma unroll
+        for (int m = 0; m < 4; m++) code[m] = range_code(L, q.i, q.j, 2 * (q.kk0 + m) + p);
+    }
+}
+
+// neighbour sums of the four cells over the other plane, in the reference's
+// order; v4(slot, out[4]) loads four consecutive other-plane values, v1(slot)
+// one.  With PRO each neighbour also takes the coarse level's z at its parent
+// (the prolongation, added before the neighbour enters the sum).
+template <bool PRO, class V4, class V1>
+EDGE_D void quad_nbr_sum(const Lvl& L, const Lvl& C, const Quad& q, int p, const unsigned (&code)[4], V4 v4, V1 v1,
+                         float (&ns)[4]) {
+    const int sx = L.n1 * L.H;
+    float xp[4] = {0, 0, 0, 0}, xm[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0}, ym[4] = {0, 0, 0, 0};
+    float ov[4], o[6];
+    if (q.i < L.n0 - 1) v4(q.t0 + sx, xp);
+    if (q.i > 0) v4(q.t0 - sx, xm);
+    if (q.j < L.n1 - 1) v4(q.t0 + L.H, yp);
+    if (q.j > 0) v4(q.t0 - L.H, ym);
+    v4(q.t0, ov);
+    o[0] = (p == 0 && q.kk0 > 0) ? v1(q.t0 - 1) : 0.0f;  // slot kk0-1
+    o[1] = ov[0]; o[2] = ov[1]; o[3] = ov[2]; o[4] = ov[3];
+    o[5] = (p == 1 && q.kk0 + 4 < L.H) ? v1(q.t0 + 4) : 0.0f;  // slot kk0+4
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const unsigned c = code[m];
+        const int k = 2 * (q.kk0 + m) + p;
+        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = o[m + 1 + p], vzm = o[m + p];
+        if (PRO) {
+            const float* z0 = C.z[0];
+            const float* z1 = C.z[1];
+            if (c & NB_XP) vxp = vxp + parent_z(C, z0, z1, q.i + 1, q.j, k);
+            if (c & NB_XM) vxm = vxm + parent_z(C, z0, z1, q.i - 1, q.j, k);
+            if (c & NB_YP) vyp = vyp + parent_z(C, z0, z1, q.i, q.j + 1, k);
+            if (c & NB_YM) vym = vym + parent_z(C, z0, z1, q.i, q.j - 1, k);
+            if (c & NB_ZP) vzp = vzp + parent_z(C, z0, z1, q.i, q.j, k + 1);
+            if (c & NB_ZM) vzm = vzm + parent_z(C, z0, z1, q.i, q.j, k - 1);
+        }
+        float r = 0.0f;
+        if (c & NB_XP) r += vxp;
+        if (c & NB_XM) r += vxm;
+        if (c & NB_YP) r += vyp;
+        if (c & NB_YM) r += vym;
+        if (c & NB_ZP) r += vzp;
+        if (c & NB_ZM) r += vzm;
+        ns[m] = r;
+    }
+}
+
+template <int MODE, bool SOLID>
+__global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, int color) {
+    count_launch(g.st);
+    if (!running(g)) {
+        if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
+        return;
+    }
+    const float mean = level0 ? g.st->mean : 0.0f;
+    const int oc = color ^ 1;
+    const float* __restrict__ rs = L.r[color];
+    const float* __restrict__ zo = L.z[oc];
+    float* __restrict__ zs = L.z[color];
+    double v[1] = {0.0};
+    GRID_STRIDE(t, L.n0 * L.n1 * (L.H >> 2)) {
+        const Quad q = quad_of(L, t);
+        const int p = (q.i + q.j + color) & 1;
+        unsigned code[4];
+        quad_codes<SOLID>(L, color, q, p, code);
+        float rv[4], ns[4] = {0.0f, 0.0f, 0.0f, 0.0f}, zn[4];
+        ld4(rs + q.t0, rv);
+        if (MODE != HS_FIRST) {
+            auto v4 = [&](int e, float(&o)[4]) { ld4(zo + e, o); };
+            auto v1 = [&](int e) { return __ldg(zo + e); };
+            quad_nbr_sum<MODE == HS_PROLONG>(L, C, q, p, code, v4, v1, ns);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            rv[m] = rv[m] - mean;
+            zn[m] = (code[m] & CELL_FLUID) ? (rv[m] + ns[m]) / nf_of<SOLID>(g.bt, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
+                                           : 0.0f;
+            if (MODE == HS_ZR && (code[m] & CELL_FLUID)) v[0] += (double)zn[m] * (double)rv[m];
+        }
+        st4(zs + q.t0, zn);
+        if (MODE == HS_ZR) {
+            // the other cells of the slots (final from the previous half sweep)
+            unsigned co[4];
+            quad_codes<SOLID>(L, oc, q, p ^ 1, co);
+            float ro[4], zz[4];
+            ld4(L.r[oc] + q.t0, ro);
+            ld4(zo + q.t0, zz);
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (co[m] & CELL_FLUID) v[0] += (double)zz[m] * (double)(ro[m] - mean);
+        }
+    }
+    if (MODE == HS_ZR) {
+        if (last_block<1>(g, 4, v)) {
+            double sm[1];
+            final_sum<1>(g, 4, sm);
+            if (threadIdx.x == 0) zr_epilogue(g, sm[0]);
+        }
+    }
+}
+
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
+    count_launch(g.st);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        set_cond(g, 0);
+        if (g.st->it > g.st->max_iters + 8) g.st->status = ST_NOCONV;  // hard cap
+    }
+    if (!running(g)) return;
+    SolveState* st = g.st;
+    const int pc = st->pcur;
+    const bool first = st->it == 0;
+    const float beta = st->beta;
+    double v[1] = {0.0};
+    GRID_STRIDE(t, L.n0 * L.n1 * (L.H >> 2)) {
+        const Quad q = quad_of(L, t);
+        const int c0 = (q.i + q.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int pl = c0 ^ h;
+            unsigned code[4];
+            quad_codes<SOLID>(L, pl, q, h, code);
+            const float* __restrict__ zo = L.z[pl ^ 1];
+            const float* __restrict__ po = f.p[pc][pl ^ 1];
+            auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
+                ld4(zz + e, o);
+                if (!first) {
+                    float b[4];
+                    ld4(pp + e, b);
+#pragma unroll
+                    for (int m = 0; m < 4; m++) o[m] = __fadd_rn(o[m], __fmul_rn(beta, b[m]));
+                }
+            };
+            float pe[4], ns[4];
+            pn4(L.z[pl], f.p[pc][pl], q.t0, pe);
+            quad_nbr_sum<false>(
+                L, L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
+                [&](int e) { return first ? __ldg(zo + e) : __fadd_rn(__ldg(zo + e), __fmul_rn(beta, __ldg(po + e))); },
+                ns);
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                if (code[m] & CELL_FLUID) {
+                    float nf = nf_of<SOLID>(g.bt, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
+                    float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
+                    v[0] += (double)pe[m] * (double)ape;
+                } else {
+                    pe[m] = 0.0f;
+                }
             }
-            set_cond(c, st->status == ST_RUNNING ? 1u : 0u);
+            st4(f.p[pc ^ 1][pl] + q.t0, pe);
+        }
+    }
+    if (last_block<1>(g, 2, v)) {
+        double sm[1];
+        final_sum<1>(g, 2, sm);
+        if (threadIdx.x == 0) {
+            double pAp = (double)(float)sm[0];
+            st->pAp = pAp;
+            st->alpha = (float)(st->zTr / (pAp + 1e-12));
+            st->pcur = pc ^ 1;
+        }
+    }
+}
+
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
+    count_launch(g.st);
+    if (!running(g)) return;
+    SolveState* st = g.st;
+    const float alpha = st->alpha, mean = st->mean;
+    const bool first = st->it == 0;
+    const int pc = st->pcur;
+    double v[2] = {0.0, 0.0};
+    GRID_STRIDE(t, L.n0 * L.n1 * (L.H >> 2)) {
+        const Quad q = quad_of(L, t);
+        const int c0 = (q.i + q.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int pl = c0 ^ h;
+            unsigned code[4];
+            quad_codes<SOLID>(L, pl, q, h, code);
+            const float* __restrict__ po = f.p[pc][pl ^ 1];
+            float pe[4], ns[4], r[4], x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            ld4(f.p[pc][pl] + q.t0, pe);
+            ld4c(L.r[pl] + q.t0, r);
+            if (!first) ld4c(f.x[pl] + q.t0, x);
+            quad_nbr_sum<false>(
+                L, L, q, h, code, [&](int e, float(&o)[4]) { ld4(po + e, o); }, [&](int e) { return __ldg(po + e); },
+                ns);
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                r[m] = r[m] - mean;
+                if (code[m] & CELL_FLUID) {
+                    x[m] = first ? __fmul_rn(alpha, pe[m]) : __fadd_rn(x[m], __fmul_rn(alpha, pe[m]));
+                    float nf = nf_of<SOLID>(g.bt, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
+                    float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
+                    r[m] = __fsub_rn(r[m], __fmul_rn(alpha, ape));
+                    v[0] += (double)r[m] * (double)r[m];
+                }
+                v[1] += r[m];
+            }
+            st4(f.x[pl] + q.t0, x);
+            st4(L.r[pl] + q.t0, r);
+        }
+    }
+    if (last_block<2>(g, 3, v)) {
+        double s[2];
+        final_sum<2>(g, 3, s);
+        if (threadIdx.x == 0) {
+            double rTr = (double)(float)s[0];
+            st->rTr = rTr;
+            st->rsum = s[1];
+            st->x_valid = 1;
+            st->mean = st->all_neumann ? (float)(s[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
+            if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
+            else if (rTr < st->tol) st->status = ST_CONVERGED;
+        }
+    }
+}
+
+// restriction, four coarse cells (I, J, K0..K0+3) per thread: their children
+// are slots K0..K0+3 of both planes in the four fine rows (2I+a, 2J+b)
+template <bool SOLID>
+__global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0, int first) {
+    count_launch(g.st);
+    if (!running(g)) return;
+    const float mean = level0 ? g.st->mean : 0.0f;
+    const int nq = F.H >> 2;  // == C.n2 / 4
+    GRID_STRIDE(t, C.n0 * C.n1 * nq) {
+        const int rowc = fdiv(t, F.dQ);
+        const int K0 = (t - rowc * nq) << 2;
+        const int I = fdiv(rowc, C.d1);
+        const int J = rowc - I * C.n1;
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const int i = 2 * I + a, j = 2 * J + b;
+                const Quad q{i, j, K0, (i * F.n1 + j) * F.H + K0};
+                const int c0 = (i + j) & 1;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int pl = c0 ^ h;
+                    unsigned code[4];
+                    quad_codes<SOLID>(F, pl, q, h, code);
+                    const float* __restrict__ zo = F.z[pl ^ 1];
+                    float ns[4], zc[4], rc[4];
+                    quad_nbr_sum<false>(
+                        F, F, q, h, code, [&](int e, float(&o)[4]) { ld4(zo + e, o); },
+                        [&](int e) { return __ldg(zo + e); }, ns);
+                    ld4(F.z[pl] + q.t0, zc);
+                    ld4(F.r[pl] + q.t0, rc);
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        if (!(code[m] & CELL_FLUID)) continue;
+                        float nf = nf_of<SOLID>(g.bt, F, code[m], i, j, 2 * (K0 + m) + h);
+                        float az = __fsub_rn(__fmul_rn(nf, zc[m]), ns[m]);
+                        float res = (rc[m] - mean) - az;
+                        acc[m] += res * 0.5f;
+                    }
+                }
+            }
+        // coarse cells K0, K0+2 sit in plane (I+J)&1, K0+1, K0+3 in the other,
+        // at slots ecb, ecb+1
+        const int ecb = (I * C.n1 + J) * C.H + (K0 >> 1);
+        const int pa = (I + J) & 1;
+        *reinterpret_cast<float2*>(C.r[pa] + ecb) = make_float2(acc[0], acc[2]);
+        *reinterpret_cast<float2*>(C.r[pa ^ 1] + ecb) = make_float2(acc[1], acc[3]);
+        if (first) {
+            // first half sweep of the coarse level: z = r / n_fluid on colour 0
+            const int m0 = pa;  // the colour-0 cells are m0 and m0 + 2
+            float zz[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int m = m0 + 2 * u, K = K0 + m;
+                const unsigned cc = SOLID ? (unsigned)C.code[0][ecb + u] : range_code(C, I, J, K);
+                zz[u] = (cc & CELL_FLUID) ? (acc[m] + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K) : 0.0f;
+            }
+            *reinterpret_cast<float2*>(C.z[0] + ecb) = make_float2(zz[0], zz[1]);
         }
     }
 }
 
 // mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
-// wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479)
-__global__ void k_grad_p(Ctx c, int nx, int ny, int nz, Faces U) {
-    count_launch(c.st);
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_faces(nx, ny, nz)) return;
-    FaceIdx f = face_decompose(t, nx, ny, nz);
-    int a = f.axis;
-    int I[3] = {f.i, f.j, f.k}, D[3] = {nx, ny, nz};
-    int hi[3] = {min(f.i, nx - 1), min(f.j, ny - 1), min(f.k, nz - 1)};
-    int lo[3] = {hi[0], hi[1], hi[2]};
-    lo[a] = max(I[a] - 1, 0);
-    float pr = c.x[idx3(hi[0], hi[1], hi[2], ny, nz)];
-    float pl = c.x[idx3(lo[0], lo[1], lo[2], ny, nz)];
-    if (I[a] - 1 < 0) pl = 0.0f;
-    if (I[a] >= D[a]) pr = 0.0f;
-    float g = pr - pl;
-    float u = U.u[a][f.e] - g;
-    if ((I[a] == 0 && c.bt[2 * a] == 2) || (I[a] == D[a] && c.bt[2 * a + 1] == 2)) u = 0.0f;
-    U.u[a][f.e] = u;
-    if (U.f[a]) U.f[a][f.e] = -g;
+// wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479).
+// One thread per slot: the faces on the low side of its two cells in each
+// axis, and the high boundary faces of cells on the high boundary.
+EDGE_D void face_update(const G& g, Faces& U, int a, int e, float gr, bool wall) {
+    float u = U.u[a][e] - gr;
+    if (wall) u = 0.0f;
+    U.u[a][e] = u;
+    if (U.f[a]) U.f[a][e] = -gr;
 }
 
-__global__ void k_copy(SolveState* st, const float* a, float* b, int n) {
+__global__ void __launch_bounds__(256) k_grad_p(G g, Lvl L, Fine f, Faces U) {
+    count_launch(g.st);
+    const bool xv = g.st->x_valid != 0;  // x = 0 when no iteration ran
+    const int nx = L.n0, ny = L.n1, nz = L.n2, sx = L.n1 * L.H;
+    GRID_STRIDE(t, L.P) {
+        const Slot s = slot_of(L, t);
+        const int i = s.i, j = s.j, c0 = (i + j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = 2 * s.kk + h, pl = c0 ^ h;
+            if (k >= nz) break;
+            const float* xo = f.x[pl ^ 1];
+            const float xc = xv ? f.x[pl][t] : 0.0f;
+            const float xl = (xv && i > 0) ? xo[t - sx] : 0.0f;
+            face_update(g, U, 0, idx3(i, j, k, ny, nz), xc - xl, i == 0 && g.bt[0] == 2);
+            if (i == nx - 1) face_update(g, U, 0, idx3(nx, j, k, ny, nz), 0.0f - xc, g.bt[1] == 2);
+            const float yl = (xv && j > 0) ? xo[t - L.H] : 0.0f;
+            face_update(g, U, 1, idx3(i, j, k, ny + 1, nz), xc - yl, j == 0 && g.bt[2] == 2);
+            if (j == ny - 1) face_update(g, U, 1, idx3(i, ny, k, ny + 1, nz), 0.0f - xc, g.bt[3] == 2);
+            const float zl = (xv && k > 0) ? xo[t - 1 + (k & 1)] : 0.0f;
+            face_update(g, U, 2, idx3(i, j, k, ny, nz + 1), xc - zl, k == 0 && g.bt[4] == 2);
+            if (k == nz - 1) face_update(g, U, 2, idx3(i, j, nz, ny, nz + 1), 0.0f - xc, g.bt[5] == 2);
+        }
+    }
+}
+
+// red-black planes <-> lexicographic field of one level; `valid` (may be
+// NULL) gates the planes' content (x before the first update reads as 0)
+__global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p1, float* dst, const int* valid) {
     if (st) count_launch(st);
+    const bool ok = valid == nullptr || *valid != 0;
+    GRID_STRIDE(t, L.n0 * L.n1 * L.n2) {
+        int row = fdiv(t, L.d2);
+        int k = t - row * L.n2;
+        int i = fdiv(row, L.d1);
+        int j = row - i * L.n1;
+        const float* p = ((i + j + k) & 1) ? p1 : p0;
+        dst[t] = ok ? p[row * L.H + (k >> 1)] : 0.0f;
+    }
+}
+
+__global__ void k_to_rb(Lvl L, const float* src, float* p0, float* p1) {
+    GRID_STRIDE(t, L.n0 * L.n1 * L.n2) {
+        int row = fdiv(t, L.d2);
+        int k = t - row * L.n2;
+        int i = fdiv(row, L.d1);
+        int j = row - i * L.n1;
+        float* p = ((i + j + k) & 1) ? p1 : p0;
+        p[row * L.H + (k >> 1)] = src[t];
+    }
+}
+
+// num_fluid_neighbors from the lexicographic mask (edge_mgpcg_apply_A)
+EDGE_D float n_fluid_lex(const int* bt, const Lvl& L, int i, int j, int k) {
+    float num = 6.0f;
+    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (I[a] <= 0 && bt[2 * a] == 2) num -= 1.0f;
+        else if (L.bm && I[a] > 0) {
+            int e = idx3(i - (a == 0), j - (a == 1), k - (a == 2), L.n1, L.n2);
+            if (__ldg(L.bm + e) > 0) num -= 1.0f;
+        }
+        if (I[a] >= D[a] - 1 && bt[2 * a + 1] == 2) num -= 1.0f;
+        else if (L.bm && I[a] < D[a] - 1) {
+            int e = idx3(i + (a == 0), j + (a == 1), k + (a == 2), L.n1, L.n2);
+            if (__ldg(L.bm + e) > 0) num -= 1.0f;
+        }
+    }
+    return num;
+}
+
+EDGE_D bool is_fluid(const int* bm, int e) { return bm == nullptr || __ldg(bm + e) <= 0; }
+
+__global__ void k_apply_A(G g, Lvl L, const float* p, float* Ap) {
+    int n = L.n0 * L.n1 * L.n2;
     int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < n) b[e] = a[e];
+    if (e >= n) return;
+    if (!is_fluid(L.bm, e)) {
+        Ap[e] = 0.0f;
+        return;
+    }
+    int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+    int stride[3] = {L.n1 * L.n2, L.n2, 1};
+    float ns = 0.0f;
+    for (int a = 0; a < 3; a++) {
+        if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += p[e + stride[a]];
+        if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
+    }
+    Ap[e] = __fsub_rn(__fmul_rn(n_fluid_lex(g.bt, L, i, j, k), p[e]), ns);
 }
 
 // ---------------------------------------------------------------------------
@@ -743,6 +1293,25 @@ inline int cu(cudaError_t e) { return e == cudaSuccess ? EDGE_OK : (int)e; }
         int _r = cu(x);              \
         if (_r != EDGE_OK) return _r; \
     } while (0)
+
+// reduction and sweep kernels loop over their slots with at most this many
+// blocks (8 per SM), which bounds the last-block atomics
+constexpr int kMaxBlocks = 148 * 8;
+inline int rgrid(long long n) { return (int)std::max<long long>(1, std::min<long long>(grid_for(n), kMaxBlocks)); }
+
+// plane length rounded to 64 floats, so every plane starts 256-byte aligned
+inline size_t plane_alloc(long long P) { return (size_t)((P + 63) / 64 * 64); }
+
+void set_level_dims(Lvl& V, int n0, int n1, int n2) {
+    V.n0 = n0; V.n1 = n1; V.n2 = n2;
+    V.H = (n2 + 1) / 2;
+    V.P = n0 * n1 * V.H;
+    V.dH = make_fdiv((unsigned)V.H);
+    V.d1 = make_fdiv((unsigned)n1);
+    V.d2 = make_fdiv((unsigned)n2);
+    V.vec = V.H % 4 == 0;
+    V.dQ = make_fdiv((unsigned)std::max(1, V.H / 4));
+}
 
 struct GraphKey {
     const void* a[7];
@@ -764,7 +1333,6 @@ struct Solver {
     std::map<GraphKey, cudaGraphExec_t> graphs;
     std::vector<cudaGraph_t> graph_defs;
     SolveState* st_host;  // pinned
-    int max_blocks;
 };
 
 int alloc(Solver* s, void** p, size_t bytes) {
@@ -776,17 +1344,16 @@ int alloc(Solver* s, void** p, size_t bytes) {
 // The levels lc..L-1 that fit in kCoarseSmem of shared memory together go to
 // k_coarse; the finer ones run half-sweep kernels.
 void plan_coarse(Ctx& c, bool solid) {
-    for (int lc = 0; lc < c.L; lc++) {
-        size_t floats = 0, cells = 0;
-        for (int l = lc; l < c.L; l++) {
-            size_t n = (size_t)c.lv[l].n0 * c.lv[l].n1 * c.lv[l].n2;
-            floats += 2 * n;
-            cells += n;
+    Levels& V = c.lv;
+    for (int lc = 0; lc < V.L; lc++) {
+        size_t floats = 0, codes = 0;
+        for (int l = lc; l < V.L; l++) {
+            floats += 4 * (size_t)V.lv[l].P;
+            codes += 2 * (size_t)V.lv[l].P;
         }
-        size_t bytes = floats * sizeof(float) + (solid ? cells : 0) + 16;
-        if (bytes <= kCoarseSmem || lc == c.L - 1) {
-            c.lc = lc;
-            c.cmoff = (int)floats;
+        size_t bytes = floats * sizeof(float) + (solid ? codes * sizeof(unsigned short) : 0) + 16;
+        if (bytes <= kCoarseSmem || lc == V.L - 1) {
+            V.lc = lc;
             c.csmem = (int)bytes;
             return;
         }
@@ -796,57 +1363,139 @@ void plan_coarse(Ctx& c, bool solid) {
 int prepare_coarse_kernels(const Ctx& c) {
     if ((size_t)c.csmem > kCoarseSmem) return EDGE_EINVAL;  // the coarsest level alone must fit
     if (c.csmem > 48 * 1024) {
-        CK(cudaFuncSetAttribute(k_coarse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
     }
     return EDGE_OK;
 }
 
 // One V-cycle (mgpcg.py:177-195); with final_zr the last kernel also forms
 // z.r and the end-of-iteration bookkeeping (mgpcg.py:263-277).
-// reduction and sweep kernels loop over their cells with at most this many
-// blocks (8 per SM), which bounds the last-block atomics
-constexpr int kMaxBlocks = 148 * 8;
-inline int rgrid(long long n) { return (int)std::min<long long>(grid_for(n), kMaxBlocks); }
-
-void enqueue_vcycle_ctx(const Ctx& c, cudaStream_t stream, bool final_zr) {
-    const int lc = c.lc;
+template <bool S>
+void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
+    const Levels& V = c.lv;
+    const int lc = V.lc;
     for (int l = 0; l < lc; l++) {
-        const Lvl& L = c.lv[l];
-        int g = rgrid((long long)L.n0 * L.n1 * (L.n2 / 2));
-        k_hsweep<HS_FIRST><<<g, 256, 0, stream>>>(c, l, 0);
-        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 1);
-        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 0);
-        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 1);
-        const Lvl& C = c.lv[l + 1];
-        k_restrict<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c, l);
+        const Lvl& L = V.lv[l];
+        const Lvl& C = V.lv[l + 1];
+        const int l0 = l == 0, first = l + 1 < lc;
+        if (L.vec) {
+            const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
+            if (l == 0) k_hsweep4<HS_FIRST, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_restrict4<S><<<rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream>>>(c.g, L, C, l0, first);
+        } else {
+            const int g = rgrid(L.P);
+            if (l == 0) k_hsweep<HS_FIRST, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_restrict<S><<<rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c.g, L, C, l0, first);
+        }
     }
-    if (final_zr && lc == 0) k_coarse<true><<<1, 1024, c.csmem, stream>>>(c, lc, c.cmoff);
-    else k_coarse<false><<<1, 1024, c.csmem, stream>>>(c, lc, c.cmoff);
+    if (final_zr && lc == 0) k_coarse<true, S><<<1, 1024, c.csmem, stream>>>(c.g, V);
+    else k_coarse<false, S><<<1, 1024, c.csmem, stream>>>(c.g, V);
     for (int l = lc - 1; l >= 0; l--) {
-        const Lvl& L = c.lv[l];
-        int g = rgrid((long long)L.n0 * L.n1 * (L.n2 / 2));
-        k_hsweep<HS_PROLONG><<<g, 256, 0, stream>>>(c, l, 1);
-        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 0);
-        k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 1);
-        if (l == 0 && final_zr) k_hsweep<HS_ZR><<<g, 256, 0, stream>>>(c, l, 0);
-        else k_hsweep<HS_PLAIN><<<g, 256, 0, stream>>>(c, l, 0);
+        const Lvl& L = V.lv[l];
+        const Lvl& C = V.lv[l + 1];
+        const int l0 = l == 0;
+        const bool zr = l == 0 && final_zr;
+        if (L.vec) {
+            const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
+            k_hsweep4<HS_PROLONG, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            if (zr) k_hsweep4<HS_ZR, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            else k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+        } else {
+            const int g = rgrid(L.P);
+            k_hsweep<HS_PROLONG, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            if (zr) k_hsweep<HS_ZR, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            else k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+        }
     }
 }
 
-void enqueue_vcycle(Solver* s, cudaStream_t stream, bool final_zr) { enqueue_vcycle_ctx(s->ctx, stream, final_zr); }
+void enqueue_vcycle(const Ctx& c, bool solid, cudaStream_t stream, bool final_zr) {
+    if (solid) vcycle_t<true>(c, stream, final_zr);
+    else vcycle_t<false>(c, stream, final_zr);
+}
 
 // The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
-void enqueue_iteration(Solver* s, cudaStream_t stream) {
-    Ctx& c = s->ctx;
-    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
-    k_cg_ap<<<rgrid(n), 256, 0, stream>>>(c);
-    k_cg_xr<<<rgrid(n), 256, 0, stream>>>(c);
-    enqueue_vcycle(s, stream, true);
+void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
+    const Lvl& L = c.lv.lv[0];
+    if (L.vec) {
+        const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
+        if (solid) {
+            k_cg_ap4<true><<<g, 256, 0, stream>>>(c.g, L, c.f);
+            k_cg_xr4<true><<<g, 256, 0, stream>>>(c.g, L, c.f);
+        } else {
+            k_cg_ap4<false><<<g, 256, 0, stream>>>(c.g, L, c.f);
+            k_cg_xr4<false><<<g, 256, 0, stream>>>(c.g, L, c.f);
+        }
+    } else if (solid) {
+        k_cg_ap<true><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+        k_cg_xr<true><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+    } else {
+        k_cg_ap<false><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+        k_cg_xr<false><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+    }
+    enqueue_vcycle(c, solid, stream, true);
 }
 
-// set-up kernels of Poisson / solve, then the conditional while node, then
-// the gradient update; captured into a graph
+// set-up kernels of Poisson / solve (everything before the CG loop)
+void enqueue_setup(Solver* s, Faces U, const float* rhs, double abs_tol, double rel_tol, int max_iters,
+                   cudaStream_t cs) {
+    Ctx& c = s->ctx;
+    const Lvl& L0 = c.lv.lv[0];
+    int n = L0.n0 * L0.n1 * L0.n2;
+    int nx = s->nx, ny = s->ny, nz = s->nz;
+    if (!rhs) {
+        const int plane = std::max(ny * nz, std::max(nx * nz, nx * ny));
+        k_apply_walls<<<dim3(std::min(grid_for(plane), 1184), 6), 256, 0, cs>>>(c.g, nx, ny, nz, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.g.st, nx, ny, nz, L0.bm, s->bvel, U);
+    }
+    if (s->solid) {
+        for (int l = 1; l < c.lv.L; l++) {
+            const Lvl& F = c.lv.lv[l - 1];
+            const Lvl& C = c.lv.lv[l];
+            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(c.g.st, F.bm, C.bm, C.n0, C.n1,
+                                                                                    C.n2, F.n1, F.n2);
+        }
+        for (int l = 0; l < c.lv.L; l++) {
+            const Lvl& V = c.lv.lv[l];
+            k_codes<<<rgrid((long long)V.n0 * V.n1 * V.n2), 256, 0, cs>>>(c.g, V);
+        }
+    }
+    cudaMemsetAsync(c.g.st->counter, 0, sizeof(c.g.st->counter), cs);  // fresh reduction counters
+    if (s->solid) k_setup_rhs<true><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
+    else k_setup_rhs<false><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
+    if (s->solid && !rhs) k_solid_fix<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f);
+    enqueue_vcycle(c, s->solid, cs, true);  // first preconditioner application + z.r + tol
+}
+
+// gradient update (Poisson) or the solution copy (solve)
+void enqueue_finish(Solver* s, Faces U, const float* rhs, float* xout, cudaStream_t cs) {
+    Ctx& c = s->ctx;
+    const Lvl& L0 = c.lv.lv[0];
+    int n = L0.n0 * L0.n1 * L0.n2;
+    int nx = s->nx, ny = s->ny, nz = s->nz;
+    if (!rhs) {
+        k_grad_p<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U);
+        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.g.st, nx, ny, nz, L0.bm, s->bvel, U);
+    } else {
+        k_from_rb<<<rgrid(n), 256, 0, cs>>>(c.g.st, L0, c.f.x[0], c.f.x[1], xout, &c.g.st->x_valid);
+    }
+}
+
+// set-up, then the conditional while node, then the gradient update; captured
+// into a graph
 int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
                 cudaGraphExec_t* exec) {
     cudaStream_t cs;
@@ -855,29 +1504,11 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     CK(cudaGraphCreate(&graph, 0));
     cudaGraphConditionalHandle handle;
     CK(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
-    s->ctx.cond = handle;
-    s->ctx.use_cond = 1;
-    Ctx& c = s->ctx;
-    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
-    int nx = s->nx, ny = s->ny, nz = s->nz;
+    s->ctx.g.cond = handle;
+    s->ctx.g.use_cond = 1;
     // 1) set-up
     CK(cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    if (!rhs) {
-        k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
-    }
-    if (s->solid) {
-        for (int l = 1; l < c.L; l++) {
-            const Lvl& F = c.lv[l - 1];
-            const Lvl& C = c.lv[l];
-            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(c.st, F.bm, (int*)C.bm, C.n0, C.n1,
-                                                                                    C.n2, F.n1, F.n2);
-        }
-    }
-    CK(cudaMemsetAsync(c.st->counter, 0, sizeof(c.st->counter), cs));  // fresh reduction counters
-    k_setup_rhs<<<rgrid(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
-    if (s->solid && !rhs) k_solid_fix<<<rgrid(n), 256, 0, cs>>>(c);
-    enqueue_vcycle(s, cs, true);  // first preconditioner application + z.r + tol
+    enqueue_setup(s, U, rhs, abs_tol, rel_tol, max_iters, cs);
     cudaGraph_t g2;
     CK(cudaStreamEndCapture(cs, &g2));
     // leaf of the set-up chain
@@ -901,17 +1532,12 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     CK(cudaGraphAddNode(&cnode, graph, &leaf, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_iteration(s, cs);
+    enqueue_iteration(s->ctx, s->solid, cs);
     cudaGraph_t b2;
     CK(cudaStreamEndCapture(cs, &b2));
     // 3) finish
     CK(cudaStreamBeginCaptureToGraph(cs, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
-    if (!rhs) {
-        k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
-    } else {
-        k_copy<<<grid_for(n), 256, 0, cs>>>(c.st, c.x, xout, n);
-    }
+    enqueue_finish(s, U, rhs, xout, cs);
     CK(cudaStreamEndCapture(cs, &g2));
     int r = cu(cudaGraphInstantiate(exec, graph, 0));
     s->graph_defs.push_back(graph);
@@ -924,37 +1550,15 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
 // that replay kernels one by one.
 int run_solve_eager(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
                     cudaStream_t cs) {
-    s->ctx.use_cond = 0;
-    Ctx& c = s->ctx;
-    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
-    int nx = s->nx, ny = s->ny, nz = s->nz;
-    if (!rhs) {
-        k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
-    }
-    if (s->solid)
-        for (int l = 1; l < c.L; l++) {
-            const Lvl& F = c.lv[l - 1];
-            const Lvl& C = c.lv[l];
-            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, cs>>>(c.st, F.bm, (int*)C.bm, C.n0,
-                                                                                    C.n1, C.n2, F.n1, F.n2);
-        }
-    CK(cudaMemsetAsync(c.st->counter, 0, sizeof(c.st->counter), cs));
-    k_setup_rhs<<<rgrid(n), 256, 0, cs>>>(c, U, rhs, abs_tol, rel_tol, max_iters);
-    if (s->solid && !rhs) k_solid_fix<<<rgrid(n), 256, 0, cs>>>(c);
-    enqueue_vcycle(s, cs, true);
+    s->ctx.g.use_cond = 0;
+    enqueue_setup(s, U, rhs, abs_tol, rel_tol, max_iters, cs);
     for (int it = 0; it <= max_iters + 8; it++) {
-        CK(cudaMemcpyAsync(&s->st_host->status, &c.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
+        CK(cudaMemcpyAsync(&s->st_host->status, &s->ctx.g.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
         CK(cudaStreamSynchronize(cs));
         if (s->st_host->status != ST_RUNNING) break;
-        enqueue_iteration(s, cs);
+        enqueue_iteration(s->ctx, s->solid, cs);
     }
-    if (!rhs) {
-        k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-        if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.st, nx, ny, nz, c.lv[0].bm, s->bvel, U);
-    } else {
-        k_copy<<<grid_for(n), 256, 0, cs>>>(c.st, c.x, xout, n);
-    }
+    enqueue_finish(s, U, rhs, xout, cs);
     return cu(cudaPeekAtLastError());
 }
 
@@ -980,6 +1584,21 @@ int run_solve(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol,
     return cu(cudaGraphLaunch(exec, stream));
 }
 
+// levels of a grid (mgpcg.py:34); EDGE_EINVAL when a level would not halve
+int level_count(int nx, int ny, int nz, int base_level, int* L) {
+    int mn = std::min(nx, std::min(ny, nz));
+    int lg = 0;
+    while ((1 << (lg + 1)) <= mn) lg++;
+    *L = lg - base_level + 1;
+    if (*L < 1 || *L > 16) return EDGE_EINVAL;
+    for (int l = 1; l < *L; l++) {
+        int f = 1 << l;
+        // restrict writes r[l+1][I//2]: every level must halve exactly
+        if (nx % f || ny % f || nz % f) return EDGE_EINVAL;
+    }
+    return EDGE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -991,16 +1610,8 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     if (precision != 0) return EDGE_EINVAL;
     long long n = (long long)nx * ny * nz;
     if (n * 3 >= (1LL << 31)) return EDGE_EINVAL;
-    int mn = std::min(nx, std::min(ny, nz));
-    int lg = 0;
-    while ((1 << (lg + 1)) <= mn) lg++;
-    int L = lg - base_level + 1;  // mgpcg.py:34
-    if (L < 1 || L > 16) return EDGE_EINVAL;
-    for (int l = 1; l < L; l++) {
-        int f = 1 << l;
-        // restrict writes r[l+1][I//2]: every level must halve exactly
-        if (nx % f || ny % f || nz % f) return EDGE_EINVAL;
-    }
+    int L = 0;
+    if (level_count(nx, ny, nz, base_level, &L) != EDGE_OK) return EDGE_EINVAL;
     Solver* s = new Solver();
     s->nx = nx; s->ny = ny; s->nz = nz;
     s->solid = mask != nullptr;
@@ -1008,36 +1619,45 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     s->precision = precision;
     Ctx& c = s->ctx;
     memset(&c, 0, sizeof(c));
-    c.L = L;
-    for (int q = 0; q < 6; q++) c.bt[q] = bt[q];
+    c.lv.L = L;
+    for (int q = 0; q < 6; q++) c.g.bt[q] = bt[q];
     int r = EDGE_OK;
     for (int l = 0; l < L && r == EDGE_OK; l++) {
-        Lvl& V = c.lv[l];
-        V.n0 = nx >> l; V.n1 = ny >> l; V.n2 = nz >> l;
-        size_t m = (size_t)V.n0 * V.n1 * V.n2;
-        r = alloc(s, (void**)&V.r, m * sizeof(float));
-        if (r == EDGE_OK) r = alloc(s, (void**)&V.z, m * sizeof(float));
-        if (r == EDGE_OK) r = cu(cudaMemset(V.z, 0, m * sizeof(float)));
-        if (s->solid) {
-            if (l == 0) V.bm = mask;
-            else if (r == EDGE_OK) r = alloc(s, (void**)&V.bm, m * sizeof(int));
+        Lvl& V = c.lv.lv[l];
+        set_level_dims(V, nx >> l, ny >> l, nz >> l);
+        size_t pa = plane_alloc(V.P);
+        r = alloc(s, (void**)&V.r[0], 2 * pa * sizeof(float));
+        if (r == EDGE_OK) r = alloc(s, (void**)&V.z[0], 2 * pa * sizeof(float));
+        if (r == EDGE_OK) r = cu(cudaMemset(V.z[0], 0, 2 * pa * sizeof(float)));
+        V.r[1] = V.r[0] + pa;
+        V.z[1] = V.z[0] + pa;
+        if (s->solid && r == EDGE_OK) {
+            if (l == 0) V.bm = const_cast<int*>(mask);
+            else r = alloc(s, (void**)&V.bm, (size_t)V.n0 * V.n1 * V.n2 * sizeof(int));
+            if (r == EDGE_OK) r = alloc(s, (void**)&V.code[0], 2 * pa * sizeof(unsigned short));
+            V.code[1] = V.code[0] + pa;
         }
     }
     plan_coarse(c, s->solid);
     if (r == EDGE_OK) r = prepare_coarse_kernels(c);
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.x, n * sizeof(float));
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.p[0], n * sizeof(float));
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.p[1], n * sizeof(float));
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.Ap, n * sizeof(float));
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.div, n * sizeof(float));
-    long long maxblk = std::max<long long>(grid_for(n), grid_for(n_faces(nx, ny, nz))) + 1024;
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.partials, 3 * maxblk * sizeof(double));
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.st, sizeof(SolveState));
+    const size_t pa0 = plane_alloc(c.lv.lv[0].P);
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.f.x[0], 2 * pa0 * sizeof(float));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.f.p[0][0], 4 * pa0 * sizeof(float));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.f.div, n * sizeof(float));
+    if (r == EDGE_OK) r = cu(cudaMemset(c.f.div, 0, n * sizeof(float)));
+    if (r == EDGE_OK) {
+        c.f.x[1] = c.f.x[0] + pa0;
+        c.f.p[0][1] = c.f.p[0][0] + pa0;
+        c.f.p[1][0] = c.f.p[0][0] + 2 * pa0;
+        c.f.p[1][1] = c.f.p[0][0] + 3 * pa0;
+    }
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.g.partials, 3 * (size_t)(kMaxBlocks + 64) * sizeof(double));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.g.st, sizeof(SolveState));
     if (r == EDGE_OK) {
         SolveState st;
         memset(&st, 0, sizeof(st));
         st.all_neumann = (bt[0] + bt[1] + bt[2] + bt[3] + bt[4] + bt[5]) == 12;
-        r = cu(cudaMemcpy(c.st, &st, sizeof(st), cudaMemcpyHostToDevice));
+        r = cu(cudaMemcpy(c.g.st, &st, sizeof(st), cudaMemcpyHostToDevice));
     }
     if (r == EDGE_OK) r = cu(cudaMallocHost((void**)&s->st_host, sizeof(SolveState)));
     if (r != EDGE_OK) {
@@ -1061,12 +1681,12 @@ int edge_mgpcg_destroy(void* handle) {
     return EDGE_OK;
 }
 
-int edge_mgpcg_levels(void* handle) { return handle ? ((Solver*)handle)->ctx.L : EDGE_EINVAL; }
+int edge_mgpcg_levels(void* handle) { return handle ? ((Solver*)handle)->ctx.lv.L : EDGE_EINVAL; }
 
 int edge_mgpcg_kernel_count(void* handle, long long* count, void* stream) {
     if (!handle || !count) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    CK(cudaMemcpyAsync(s->st_host, s->ctx.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaMemcpyAsync(s->st_host, s->ctx.g.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(cudaStreamSynchronize((cudaStream_t)stream));
     *count = (long long)s->st_host->kernels;
     return EDGE_OK;
@@ -1094,7 +1714,7 @@ int edge_mgpcg_solve(void* handle, const float* b, float* x, double abs_tol, dou
 int edge_mgpcg_result(void* handle, int* iters, double* rTr, int* status, void* stream) {
     if (!handle) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    CK(cudaMemcpyAsync(s->st_host, s->ctx.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaMemcpyAsync(s->st_host, s->ctx.g.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(cudaStreamSynchronize((cudaStream_t)stream));
     const SolveState& st = *s->st_host;
     if (iters) *iters = st.it;
@@ -1109,10 +1729,11 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
     Solver* s = (Solver*)handle;
     cudaStream_t st = (cudaStream_t)stream;
     Ctx c = s->ctx;
-    int n = c.lv[0].n0 * c.lv[0].n1 * c.lv[0].n2;
-    // status = running, mean = 0, setup flag off so the z.r epilogue is inert
+    const Lvl& L0 = c.lv.lv[0];
+    int n = L0.n0 * L0.n1 * L0.n2;
+    // status = running, mean = 0, setup flag on so the z.r epilogue is inert
     SolveState* hs = s->st_host;
-    CK(cudaMemcpyAsync(hs, c.st, sizeof(SolveState), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hs, c.g.st, sizeof(SolveState), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     hs->status = ST_RUNNING;
     hs->mean = 0.0f;
@@ -1120,48 +1741,48 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
     hs->max_iters = 1;
     hs->abs_tol = 0.0;
     hs->rel_tol = 0.0;
-    CK(cudaMemcpyAsync(c.st, hs, sizeof(SolveState), cudaMemcpyHostToDevice, st));
-    k_copy<<<grid_for(n), 256, 0, st>>>(nullptr, r, c.lv[0].r, n);
-    // outside a graph there is no loop condition to set
-    c.use_cond = 0;
-    enqueue_vcycle_ctx(c, st, false);
-    k_copy<<<grid_for(n), 256, 0, st>>>(nullptr, c.lv[0].z, z, n);
-    return cu(cudaPeekAtLastError());
-}
-
-__global__ void k_apply_A(Ctx c, const float* p, float* Ap) {
-    const Lvl& L = c.lv[0];
-    int n = L.n0 * L.n1 * L.n2;
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    if (!is_fluid(L.bm, e)) { Ap[e] = 0.0f; return; }
-    int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
-    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
-    int stride[3] = {L.n1 * L.n2, L.n2, 1};
-    float ns = 0.0f;
-    for (int a = 0; a < 3; a++) {
-        if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += p[e + stride[a]];
-        if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
+    CK(cudaMemcpyAsync(c.g.st, hs, sizeof(SolveState), cudaMemcpyHostToDevice, st));
+    if (s->solid) {
+        for (int l = 1; l < c.lv.L; l++) {
+            const Lvl& F = c.lv.lv[l - 1];
+            const Lvl& C = c.lv.lv[l];
+            k_downsample_bm<<<grid_for((long long)C.n0 * C.n1 * C.n2), 256, 0, st>>>(c.g.st, F.bm, C.bm, C.n0, C.n1,
+                                                                                    C.n2, F.n1, F.n2);
+        }
+        for (int l = 0; l < c.lv.L; l++) {
+            const Lvl& V = c.lv.lv[l];
+            k_codes<<<rgrid((long long)V.n0 * V.n1 * V.n2), 256, 0, st>>>(c.g, V);
+        }
     }
-    Ap[e] = n_fluid(c, L, i, j, k) * p[e] - ns;
+    k_to_rb<<<rgrid(n), 256, 0, st>>>(L0, r, L0.r[0], L0.r[1]);
+    // outside a graph there is no loop condition to set
+    c.g.use_cond = 0;
+    enqueue_vcycle(c, s->solid, st, false);
+    k_from_rb<<<rgrid(n), 256, 0, st>>>(nullptr, L0, L0.z[0], L0.z[1], z, nullptr);
+    return cu(cudaPeekAtLastError());
 }
 
 int edge_mgpcg_apply_A(void* handle, const float* p, float* Ap, void* stream) {
     if (!handle || !p || !Ap) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    const Lvl& L = s->ctx.lv[0];
-    k_apply_A<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx, p, Ap);
+    const Lvl& L = s->ctx.lv.lv[0];
+    k_apply_A<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx.g, L, p, Ap);
     return cu(cudaPeekAtLastError());
 }
 
 int edge_mgpcg_get(void* handle, int which, float* dst, void* stream) {
     if (!handle || !dst) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    const Lvl& L = s->ctx.lv[0];
+    const Lvl& L = s->ctx.lv.lv[0];
     size_t n = (size_t)L.n0 * L.n1 * L.n2;
-    const float* src = which == 0 ? s->ctx.div : (which == 1 ? s->ctx.x : nullptr);
-    if (!src) return EDGE_EINVAL;
-    return cu(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (which == 0) return cu(cudaMemcpyAsync(dst, s->ctx.f.div, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (which == 1) {
+        k_from_rb<<<rgrid((long long)n), 256, 0, st>>>(nullptr, L, s->ctx.f.x[0], s->ctx.f.x[1], dst,
+                                                      &s->ctx.g.st->x_valid);
+        return cu(cudaPeekAtLastError());
+    }
+    return EDGE_EINVAL;
 }
 
 }  // extern "C"
@@ -1181,11 +1802,10 @@ int edge_mgpcg_get(void* handle, int which, float* dst, void* stream) {
 namespace {
 
 constexpr long long kNoAllocMaxCells = 262144;  // 64^3 cells
-constexpr long long kNoAllocFloats = 7 * kNoAllocMaxCells + kNoAllocMaxCells / 2 + 4096;
-constexpr int kNoAllocMaxBlocks = 4096;
+constexpr long long kNoAllocFloats = 8 * kNoAllocMaxCells + 4096;
 
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
-static __device__ __align__(256) double g_noalloc_partials[3 * kNoAllocMaxBlocks];
+static __device__ __align__(256) double g_noalloc_partials[3 * (kMaxBlocks + 64)];
 static __device__ __align__(256) SolveState g_noalloc_state;
 
 struct NoAllocAddrs {
@@ -1222,20 +1842,14 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     if (!bt || !ux || !uy || !uz || nx < 2 || ny < 2 || nz < 2) return EDGE_EINVAL;
     long long n = (long long)nx * ny * nz;
     if (n > kNoAllocMaxCells) return EDGE_EINVAL;  // beyond the static scratch
-    int mn = std::min(nx, std::min(ny, nz));
-    int lg = 0;
-    while ((1 << (lg + 1)) <= mn) lg++;
-    int L = lg - base_level + 1;  // mgpcg.py:34
-    if (L < 1 || L > 16) return EDGE_EINVAL;
-    for (int l = 1; l < L; l++)
-        if (nx % (1 << l) || ny % (1 << l) || nz % (1 << l)) return EDGE_EINVAL;
-    if ((n + 255) / 256 > kNoAllocMaxBlocks) return EDGE_EINVAL;
+    int L = 0;
+    if (level_count(nx, ny, nz, base_level, &L) != EDGE_OK) return EDGE_EINVAL;
     if (max_iters < 0) max_iters = 400;
     NoAllocAddrs* A = nullptr;
     int r = noalloc_addrs(&A);
     if (r != EDGE_OK) return r;
     cudaStream_t cs = (cudaStream_t)stream;
-    // carve the scratch: 256-byte aligned slices
+    // carve the scratch: 256-byte aligned planes
     Solver s;  // host-side description only; its containers stay empty
     s.nx = nx; s.ny = ny; s.nz = nz;
     s.solid = false;
@@ -1244,8 +1858,8 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     s.st_host = nullptr;
     Ctx& c = s.ctx;
     memset(&c, 0, sizeof(c));
-    c.L = L;
-    for (int q = 0; q < 6; q++) c.bt[q] = bt[q];
+    c.lv.L = L;
+    for (int q = 0; q < 6; q++) c.g.bt[q] = bt[q];
     long long off = 0;
     auto take = [&](long long count) {
         float* p = A->scratch + off;
@@ -1253,47 +1867,42 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
         return p;
     };
     for (int l = 0; l < L; l++) {
-        Lvl& V = c.lv[l];
-        V.n0 = nx >> l; V.n1 = ny >> l; V.n2 = nz >> l;
-        long long m = (long long)V.n0 * V.n1 * V.n2;
-        V.r = take(m);
-        V.z = take(m);
-        V.bm = nullptr;
+        Lvl& V = c.lv.lv[l];
+        set_level_dims(V, nx >> l, ny >> l, nz >> l);
+        for (int q = 0; q < 2; q++) V.r[q] = take(V.P);
+        for (int q = 0; q < 2; q++) V.z[q] = take(V.P);
     }
-    c.x = take(n);
-    c.p[0] = take(n);
-    c.p[1] = take(n);
-    c.Ap = take(n);
-    c.div = take(n);
+    const int P0 = c.lv.lv[0].P;
+    for (int q = 0; q < 2; q++) c.f.x[q] = take(P0);
+    for (int b = 0; b < 2; b++)
+        for (int q = 0; q < 2; q++) c.f.p[b][q] = take(P0);
+    c.f.div = take(n);
     if (off > kNoAllocFloats) return EDGE_EINVAL;
-    c.partials = A->partials;
-    c.st = A->state;
-    c.use_cond = 0;
+    c.g.partials = A->partials;
+    c.g.st = A->state;
+    c.g.use_cond = 0;
     plan_coarse(c, false);
     r = prepare_coarse_kernels(c);
     if (r != EDGE_OK) return r;
     // the loop state starts clean on every call (the arrays keep the last
-    // call's contents); x and p are zeroed by the set-up kernel
+    // call's contents; the set-up and the first iteration overwrite what is read)
     SolveState init;
     memset(&init, 0, sizeof(init));
     init.all_neumann = (bt[0] + bt[1] + bt[2] + bt[3] + bt[4] + bt[5]) == 12;
-    CK(cudaMemcpyAsync(c.st, &init, sizeof(init), cudaMemcpyHostToDevice, cs));
+    CK(cudaMemcpyAsync(c.g.st, &init, sizeof(init), cudaMemcpyHostToDevice, cs));
     Faces U = {{ux, uy, uz}, {nullptr, nullptr, nullptr}};
-    int N = (int)n;
-    k_apply_walls<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
-    k_setup_rhs<<<rgrid(N), 256, 0, cs>>>(c, U, nullptr, abs_tol, rel_tol, max_iters);
-    enqueue_vcycle(&s, cs, true);
+    enqueue_setup(&s, U, nullptr, abs_tol, rel_tol, max_iters, cs);
     int st_status = ST_RUNNING;
     for (int it = 0; it <= max_iters + 8; it++) {
-        CK(cudaMemcpyAsync(&st_status, &c.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
+        CK(cudaMemcpyAsync(&st_status, &c.g.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
         CK(cudaStreamSynchronize(cs));
         if (st_status != ST_RUNNING) break;
-        enqueue_iteration(&s, cs);
+        enqueue_iteration(c, false, cs);
     }
-    k_grad_p<<<grid_for(n_faces(nx, ny, nz)), 256, 0, cs>>>(c, nx, ny, nz, U);
+    enqueue_finish(&s, U, nullptr, nullptr, cs);
     CK(cudaPeekAtLastError());
     SolveState fin;
-    CK(cudaMemcpyAsync(&fin, c.st, sizeof(fin), cudaMemcpyDeviceToHost, cs));
+    CK(cudaMemcpyAsync(&fin, c.g.st, sizeof(fin), cudaMemcpyDeviceToHost, cs));
     CK(cudaStreamSynchronize(cs));
     if (iters) *iters = fin.it;
     if (rTr) *rTr = fin.rTr;

@@ -78,14 +78,21 @@ def test_solid_golden():
     assert rel_l2(N_(s.u_div), d["div"]) < 1e-5
 
 
-@pytest.mark.parametrize("res,base_level", [((64, 32, 32), 2), ((64, 32, 32), 3), ((32, 32, 16), 1)])
-def test_poisson_vs_oracle(res, base_level):
+# (128, 64, 64) runs two levels outside the shared-memory coarse group (the
+# restriction then also applies the coarse level's first half sweep);
+# (48, 24, 24) ends on a 6x3x3 level (an odd row length); the open x
+# boundaries take the path without recentering.
+@pytest.mark.parametrize("res,base_level,bt", [((64, 32, 32), 2, None), ((64, 32, 32), 3, None),
+                                               ((32, 32, 16), 1, None), ((128, 64, 64), 2, None),
+                                               ((48, 24, 24), 1, None), ((64, 32, 32), 2, ((1, 1), (2, 2), (2, 2)))])
+def test_poisson_vs_oracle(res, base_level, bt):
     from edgeb200.projection import Projection
+    bt = bt or ((2, 2), (2, 2), (2, 2))
     rng = np.random.default_rng(sum(res) + base_level)
     u = [rng.normal(size=s).astype(np.float32) for s in O.face_shapes(res)]
     uo = [a.copy() for a in u]
-    it_o, div_o, p_o, rtr_o = O.poisson(uo, base_level=base_level)
-    P = Projection(res, base_level=base_level)
+    it_o, div_o, p_o, rtr_o = O.poisson(uo, base_level=base_level, boundary_types=bt)
+    P = Projection(res, base_level=base_level, boundary_types=bt)
     ug = [T_(a) for a in u]
     P.poisson(*ug)
     it, rtr, st = P.result()
@@ -97,6 +104,46 @@ def test_poisson_vs_oracle(res, base_level):
     # absolute tolerance the reference uses (r.r < 1e-12 on the recursion)
     d = div_of([N_(t).astype(np.float64) for t in ug])
     assert np.sqrt((d ** 2).sum()) < 1e-3 * np.sqrt((div_of([a.astype(np.float64) for a in u]) ** 2).sum())
+
+
+@pytest.mark.parametrize("res,base_level", [((128, 64, 64), 2), ((48, 24, 24), 1)])
+def test_vcycle_vs_oracle(res, base_level):
+    """One preconditioner application against the oracle's V-cycle."""
+    from edgeb200.projection import Projection
+    rng = np.random.default_rng(11)
+    r = rng.normal(size=res).astype(np.float32)
+    z_o, ap_o, L = O.vcycle(r, base_level)
+    P = Projection(res, base_level=base_level)
+    assert P.levels == L
+    z = torch.empty(res, device="cuda")
+    P.vcycle(T_(r), z)
+    assert rel_l2(N_(z), z_o) < 1e-5
+
+
+def test_solid_vs_oracle():
+    """Solid solver with two levels outside the shared-memory coarse group: a
+    wedge-shaped obstacle moving with a constant velocity."""
+    from edgeb200.projection import Projection
+    res = (128, 64, 64)
+    rng = np.random.default_rng(11)
+    i, j, k = np.meshgrid(*(np.arange(n) for n in res), indexing="ij")
+    mask = ((np.abs(j - 32) < (i - 20) * 0.6) & (i > 20) & (i < 60)).astype(np.int32)
+    bvel = np.zeros(res + (3,), np.float32)
+    bvel[..., 0] = 0.25
+    u = [rng.normal(size=s).astype(np.float32) for s in O.face_shapes(res)]
+    uo = [a.copy() for a in u]
+    # r.r < 1e-6: the reference's 1e-12 on this grid is below float32
+    # resolution of the initial residual, where iteration counts depend on
+    # rounding
+    it_o, div_o, p_o, bm1, bm2, dsum = O.poisson_solid(uo, mask, bvel, base_level=2, tol=1e-6)
+    P = Projection(res, base_level=2, mask=T_(mask, np.int32), bvel=T_(bvel))
+    ug = [T_(a) for a in u]
+    P.poisson(*ug, abs_tol=1e-6, rel_tol=0.0, max_iters=100)
+    it, rtr, st = P.result()
+    assert it_o > 0 and st == 0
+    assert abs(it - it_o) <= 1
+    for a in range(3):
+        assert rel_l2(N_(ug[a]), uo[a]) < 1e-4
 
 
 def test_graph_reuse_and_repeat():
