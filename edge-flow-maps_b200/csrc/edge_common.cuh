@@ -574,23 +574,28 @@ EDGE_D void rk4_pos(const Mac& mac, float psi[3], float dt) {
     for (int c = 0; c < 3; c++) psi[c] = psi[c] + w6 * (u1[c] + 2.0f * u2[c] + 2.0f * u3[c] + u4[c]);
 }
 
-// RK4 of a point with NC Jacobian columns C[a] (dC/dt = grad u . C).
+// RK4 of a point with NC Jacobian columns C[a] (dC/dt = grad u . C).  The
+// four stages run as a loop (not unrolled): one copy of the 81-tap sampler
+// keeps the kernels inside the instruction cache.
 template <int NC>
 EDGE_D void rk4_jac(const Mac& mac, float psi[3], float C[NC][3], float dt) {
     float u[3], G[3][3], q[3], Cs[NC][3], d[NC][3], su[3], sd[NC][3];
     float h = 0.5f * dt;
 #pragma unroll
+    for (int c = 0; c < 3; c++) q[c] = psi[c];
+#pragma unroll
+    for (int a = 0; a < NC; a++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) Cs[a][c] = C[a][c];
+#pragma unroll 1
     for (int stage = 0; stage < 4; stage++) {
-        const float* pin = stage == 0 ? psi : q;
-        mac_sample<true>(mac, pin, u, G);
+        mac_sample<true>(mac, q, u, G);
         // derivative of the columns at this stage
 #pragma unroll
-        for (int a = 0; a < NC; a++) {
-            const float* cin = stage == 0 ? C[a] : Cs[a];
+        for (int a = 0; a < NC; a++)
 #pragma unroll
-            for (int r = 0; r < 3; r++) d[a][r] = G[r][0] * cin[0] + G[r][1] * cin[1] + G[r][2] * cin[2];
-        }
-        float wt = (stage == 0 || stage == 3) ? 1.0f : 2.0f;
+            for (int r = 0; r < 3; r++) d[a][r] = G[r][0] * Cs[a][0] + G[r][1] * Cs[a][1] + G[r][2] * Cs[a][2];
+        const float wt = (stage == 0 || stage == 3) ? 1.0f : 2.0f;
 #pragma unroll
         for (int c = 0; c < 3; c++) su[c] = stage == 0 ? u[c] : su[c] + wt * u[c];
 #pragma unroll
@@ -598,7 +603,7 @@ EDGE_D void rk4_jac(const Mac& mac, float psi[3], float C[NC][3], float dt) {
 #pragma unroll
             for (int c = 0; c < 3; c++) sd[a][c] = stage == 0 ? d[a][c] : sd[a][c] + wt * d[a][c];
         if (stage < 3) {
-            float hh = stage < 2 ? h : dt;
+            const float hh = stage < 2 ? h : dt;
 #pragma unroll
             for (int c = 0; c < 3; c++) q[c] = psi[c] + hh * u[c];
 #pragma unroll

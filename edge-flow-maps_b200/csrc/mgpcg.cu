@@ -688,6 +688,91 @@ __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Four slots per thread (levels with H % 4 == 0): one float4 per plane row
+// segment instead of four scalar loads, same arithmetic in the same order.
+// ---------------------------------------------------------------------------
+EDGE_D void ld4(const float* p, float (&v)[4]) {
+    float4 t = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+// coherent load (the thread itself rewrites these words in the same kernel)
+EDGE_D void ld4c(const float* p, float (&v)[4]) {
+    float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+EDGE_D void st4(float* p, const float (&v)[4]) { *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]); }
+
+// slots kk0..kk0+3 of row (i, j); t0 = the first slot's index in a plane
+struct Quad {
+    int i, j, kk0, t0;
+};
+template <class LV>
+EDGE_D Quad quad_of(const LV& L, int t) {
+    int row = fdiv(t, L.dQ);
+    int i = fdiv(row, L.d1);
+    int kk0 = (t - row * (L.H >> 2)) << 2;
+    return Quad{i, row - i * L.n1, kk0, row * L.H + kk0};
+}
+
+// codes of the four cells of plane `plane` (parity p: k = 2 kk + p)
+template <bool SOLID>
+EDGE_D void quad_codes(const Lvl& L, int plane, const Quad& q, int p, unsigned (&code)[4]) {
+    if (SOLID) {
+        ushort4 c = *reinterpret_cast<const ushort4*>(L.code[plane] + q.t0);
+        code[0] = c.x; code[1] = c.y; code[2] = c.z; code[3] = c.w;
+    } else {
+#pragma unroll
+        for (int m = 0; m < 4; m++) code[m] = range_code(L, q.i, q.j, 2 * (q.kk0 + m) + p);
+    }
+}
+
+// neighbour sums of the four cells over the other plane, in the reference's
+// order; v4(slot, out[4]) loads four consecutive other-plane values, v1(slot)
+// one.  With PRO each neighbour also takes pz(i, j, k), the coarse level's z
+// at its parent (the prolongation, added before the neighbour enters the sum).
+template <bool PRO, class LV, class V4, class V1, class PZ>
+EDGE_D void quad_nbr_sum(const LV& L, const Quad& q, int p, const unsigned (&code)[4], V4 v4, V1 v1, PZ pz,
+                         float (&ns)[4]) {
+    const int sx = L.n1 * L.H;
+    float xp[4] = {0, 0, 0, 0}, xm[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0}, ym[4] = {0, 0, 0, 0};
+    float ov[4], o[6];
+    if (q.i < L.n0 - 1) v4(q.t0 + sx, xp);
+    if (q.i > 0) v4(q.t0 - sx, xm);
+    if (q.j < L.n1 - 1) v4(q.t0 + L.H, yp);
+    if (q.j > 0) v4(q.t0 - L.H, ym);
+    v4(q.t0, ov);
+    o[0] = (p == 0 && q.kk0 > 0) ? v1(q.t0 - 1) : 0.0f;  // slot kk0-1
+    o[1] = ov[0]; o[2] = ov[1]; o[3] = ov[2]; o[4] = ov[3];
+    o[5] = (p == 1 && q.kk0 + 4 < L.H) ? v1(q.t0 + 4) : 0.0f;  // slot kk0+4
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const unsigned c = code[m];
+        const int k = 2 * (q.kk0 + m) + p;
+        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = o[m + 1 + p], vzm = o[m + p];
+        if (PRO) {
+            if (c & NB_XP) vxp = vxp + pz(q.i + 1, q.j, k);
+            if (c & NB_XM) vxm = vxm + pz(q.i - 1, q.j, k);
+            if (c & NB_YP) vyp = vyp + pz(q.i, q.j + 1, k);
+            if (c & NB_YM) vym = vym + pz(q.i, q.j - 1, k);
+            if (c & NB_ZP) vzp = vzp + pz(q.i, q.j, k + 1);
+            if (c & NB_ZM) vzm = vzm + pz(q.i, q.j, k - 1);
+        }
+        float r = 0.0f;
+        if (c & NB_XP) r += vxp;
+        if (c & NB_XM) r += vxm;
+        if (c & NB_YP) r += vyp;
+        if (c & NB_YM) r += vym;
+        if (c & NB_ZP) r += vzp;
+        if (c & NB_ZM) r += vzm;
+        ns[m] = r;
+    }
+}
+
+struct NoParent {
+    EDGE_D float operator()(int, int, int) const { return 0.0f; }
+};
+
 // The coarse levels lc..L-1 of a V-cycle in one thread block out of shared
 // memory (same red-black layout): down sweeps + restriction, 20 bottom
 // sweeps, prolongation + up sweeps (mgpcg.py:177-195); z[lc] is written back
@@ -696,7 +781,8 @@ __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0,
 // and runs the end-of-iteration bookkeeping.
 struct CLvl {
     int n0, n1, n2, H, P;
-    FDiv dH, d1, d2;
+    FDiv dH, d1, d2, dQ;
+    int vec;
     int roff, zoff, coff;  // float offsets of the r and z planes, ushort offset of the codes
 };
 
@@ -718,7 +804,8 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
             const Lvl& V = a.lv[l];
             CLvl q;
             q.n0 = V.n0; q.n1 = V.n1; q.n2 = V.n2; q.H = V.H; q.P = V.P;
-            q.dH = V.dH; q.d1 = V.d1; q.d2 = V.d2;
+            q.dH = V.dH; q.d1 = V.d1; q.d2 = V.d2; q.dQ = V.dQ;
+            q.vec = V.vec;
             q.roff = off;
             q.zoff = off + 2 * V.P;
             off += 4 * V.P;
@@ -747,36 +834,72 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
             }
     }
     __syncthreads();
-    // one half sweep; mode 0: from zero, 1: plain, 2: with the prolongation of l+1
+    // one half sweep; mode 0: from zero, 1: plain, 2: with the prolongation of
+    // l+1.  Levels of at most 64 slots per plane run on warp 0 alone; levels
+    // with H % 4 == 0 take four slots per thread (float4 shared-memory loads;
+    // plane offsets are multiples of four floats).
     auto half = [&](int l, int color, int mode) {
         const CLvl& q = cl[l];
-        const bool small = q.P <= 32;
+        const bool small = q.P <= 64;
         if (!small || threadIdx.x < 32) {
             const int step = small ? 32 : blockDim.x;
             const float* r = sh + q.roff + color * q.P;
             float* z = sh + q.zoff + color * q.P;
             const float* zo = sh + q.zoff + (color ^ 1) * q.P;
             const unsigned short* cd = codes + q.coff + color * q.P;
-            for (int t = threadIdx.x; t < q.P; t += step) {
-                Slot s = slot_of(q, t);
-                const int k = 2 * s.kk + ((s.i + s.j + color) & 1);
-                if (k >= q.n2) continue;
-                const unsigned code = SOLID ? (unsigned)cd[t] : range_code(q, s.i, s.j, k);
-                if (!(code & CELL_FLUID)) continue;
-                float ns = 0.0f;
-                if (mode == 1) {
-                    ns = nbr_sum(q, code, t, k, [&](int e, int) { return zo[e]; });
-                } else if (mode == 2) {
-                    const CLvl& u = cl[l + 1];
-                    const float* zc0 = sh + u.zoff;
-                    const float* zc1 = zc0 + u.P;
-                    ns = nbr_sum(q, code, t, k, [&](int e, int d) {
-                        int di, dj, dk;
-                        dir_offset(d, di, dj, dk);
-                        return zo[e] + parent_z(u, zc0, zc1, s.i + di, s.j + dj, k + dk);
-                    });
+            const CLvl& u = cl[mode == 2 ? l + 1 : l];
+            const float* zc0 = sh + u.zoff;
+            const float* zc1 = zc0 + u.P;
+            auto pz = [&](int i, int j, int k) { return parent_z(u, zc0, zc1, i, j, k); };
+            if (q.vec) {
+                const int nq = q.P >> 2;
+                for (int t = threadIdx.x; t < nq; t += step) {
+                    const Quad qd = quad_of(q, t);
+                    const int p = (qd.i + qd.j + color) & 1;
+                    unsigned code[4];
+                    if (SOLID) {
+                        ushort4 c4 = *reinterpret_cast<const ushort4*>(cd + qd.t0);
+                        code[0] = c4.x; code[1] = c4.y; code[2] = c4.z; code[3] = c4.w;
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < 4; m++) code[m] = range_code(q, qd.i, qd.j, 2 * (qd.kk0 + m) + p);
+                    }
+                    float ns[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                    auto v4 = [&](int e, float(&o)[4]) {
+                        float4 w = *reinterpret_cast<const float4*>(zo + e);
+                        o[0] = w.x; o[1] = w.y; o[2] = w.z; o[3] = w.w;
+                    };
+                    auto v1 = [&](int e) { return zo[e]; };
+                    if (mode == 1) quad_nbr_sum<false>(q, qd, p, code, v4, v1, NoParent(), ns);
+                    else if (mode == 2) quad_nbr_sum<true>(q, qd, p, code, v4, v1, pz, ns);
+                    float4 rv = *reinterpret_cast<const float4*>(r + qd.t0);
+                    float4 zv = *reinterpret_cast<const float4*>(z + qd.t0);
+                    float rr[4] = {rv.x, rv.y, rv.z, rv.w}, zz[4] = {zv.x, zv.y, zv.z, zv.w};
+#pragma unroll
+                    for (int m = 0; m < 4; m++)
+                        if (code[m] & CELL_FLUID)
+                            zz[m] = (rr[m] + ns[m]) / nf_of<SOLID>(g.bt, q, code[m], qd.i, qd.j, 2 * (qd.kk0 + m) + p);
+                    *reinterpret_cast<float4*>(z + qd.t0) = make_float4(zz[0], zz[1], zz[2], zz[3]);
                 }
-                z[t] = (r[t] + ns) / nf_of<SOLID>(g.bt, q, code, s.i, s.j, k);
+            } else {
+                for (int t = threadIdx.x; t < q.P; t += step) {
+                    Slot s = slot_of(q, t);
+                    const int k = 2 * s.kk + ((s.i + s.j + color) & 1);
+                    if (k >= q.n2) continue;
+                    const unsigned code = SOLID ? (unsigned)cd[t] : range_code(q, s.i, s.j, k);
+                    if (!(code & CELL_FLUID)) continue;
+                    float ns = 0.0f;
+                    if (mode == 1) {
+                        ns = nbr_sum(q, code, t, k, [&](int e, int) { return zo[e]; });
+                    } else if (mode == 2) {
+                        ns = nbr_sum(q, code, t, k, [&](int e, int d) {
+                            int di, dj, dk;
+                            dir_offset(d, di, dj, dk);
+                            return zo[e] + pz(s.i + di, s.j + dj, k + dk);
+                        });
+                    }
+                    z[t] = (r[t] + ns) / nf_of<SOLID>(g.bt, q, code, s.i, s.j, k);
+                }
             }
         }
         if (small) __syncwarp();
@@ -859,88 +982,6 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// Four slots per thread (levels with H % 4 == 0): one float4 per plane row
-// segment instead of four scalar loads, same arithmetic in the same order.
-// ---------------------------------------------------------------------------
-EDGE_D void ld4(const float* p, float (&v)[4]) {
-    float4 t = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-}
-// coherent load (the thread itself rewrites these words in the same kernel)
-EDGE_D void ld4c(const float* p, float (&v)[4]) {
-    float4 t = *reinterpret_cast<const float4*>(p);
-    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-}
-EDGE_D void st4(float* p, const float (&v)[4]) { *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]); }
-
-// slots kk0..kk0+3 of row (i, j); t0 = the first slot's index in a plane
-struct Quad {
-    int i, j, kk0, t0;
-};
-EDGE_D Quad quad_of(const Lvl& L, int t) {
-    int row = fdiv(t, L.dQ);
-    int i = fdiv(row, L.d1);
-    int kk0 = (t - row * (L.H >> 2)) << 2;
-    return Quad{i, row - i * L.n1, kk0, row * L.H + kk0};
-}
-
-// codes of the four cells of plane `plane` (parity p: k = 2 kk + p)
-template <bool SOLID>
-EDGE_D void quad_codes(const Lvl& L, int plane, const Quad& q, int p, unsigned (&code)[4]) {
-    if (SOLID) {
-        ushort4 c = *reinterpret_cast<const ushort4*>(L.code[plane] + q.t0);
-        code[0] = c.x; code[1] = c.y; code[2] = c.z; code[3] = c.w;
-    } else {
-#pragma unroll
-        for (int m = 0; m < 4; m++) code[m] = range_code(L, q.i, q.j, 2 * (q.kk0 + m) + p);
-    }
-}
-
-// neighbour sums of the four cells over the other plane, in the reference's
-// order; v4(slot, out[4]) loads four consecutive other-plane values, v1(slot)
-// one.  With PRO each neighbour also takes the coarse level's z at its parent
-// (the prolongation, added before the neighbour enters the sum).
-template <bool PRO, class V4, class V1>
-EDGE_D void quad_nbr_sum(const Lvl& L, const Lvl& C, const Quad& q, int p, const unsigned (&code)[4], V4 v4, V1 v1,
-                         float (&ns)[4]) {
-    const int sx = L.n1 * L.H;
-    float xp[4] = {0, 0, 0, 0}, xm[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0}, ym[4] = {0, 0, 0, 0};
-    float ov[4], o[6];
-    if (q.i < L.n0 - 1) v4(q.t0 + sx, xp);
-    if (q.i > 0) v4(q.t0 - sx, xm);
-    if (q.j < L.n1 - 1) v4(q.t0 + L.H, yp);
-    if (q.j > 0) v4(q.t0 - L.H, ym);
-    v4(q.t0, ov);
-    o[0] = (p == 0 && q.kk0 > 0) ? v1(q.t0 - 1) : 0.0f;  // slot kk0-1
-    o[1] = ov[0]; o[2] = ov[1]; o[3] = ov[2]; o[4] = ov[3];
-    o[5] = (p == 1 && q.kk0 + 4 < L.H) ? v1(q.t0 + 4) : 0.0f;  // slot kk0+4
-#pragma unroll
-    for (int m = 0; m < 4; m++) {
-        const unsigned c = code[m];
-        const int k = 2 * (q.kk0 + m) + p;
-        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = o[m + 1 + p], vzm = o[m + p];
-        if (PRO) {
-            const float* z0 = C.z[0];
-            const float* z1 = C.z[1];
-            if (c & NB_XP) vxp = vxp + parent_z(C, z0, z1, q.i + 1, q.j, k);
-            if (c & NB_XM) vxm = vxm + parent_z(C, z0, z1, q.i - 1, q.j, k);
-            if (c & NB_YP) vyp = vyp + parent_z(C, z0, z1, q.i, q.j + 1, k);
-            if (c & NB_YM) vym = vym + parent_z(C, z0, z1, q.i, q.j - 1, k);
-            if (c & NB_ZP) vzp = vzp + parent_z(C, z0, z1, q.i, q.j, k + 1);
-            if (c & NB_ZM) vzm = vzm + parent_z(C, z0, z1, q.i, q.j, k - 1);
-        }
-        float r = 0.0f;
-        if (c & NB_XP) r += vxp;
-        if (c & NB_XM) r += vxm;
-        if (c & NB_YP) r += vyp;
-        if (c & NB_YM) r += vym;
-        if (c & NB_ZP) r += vzp;
-        if (c & NB_ZM) r += vzm;
-        ns[m] = r;
-    }
-}
-
 template <int MODE, bool SOLID>
 __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, int color) {
     count_launch(g.st);
@@ -964,7 +1005,11 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
         if (MODE != HS_FIRST) {
             auto v4 = [&](int e, float(&o)[4]) { ld4(zo + e, o); };
             auto v1 = [&](int e) { return __ldg(zo + e); };
-            quad_nbr_sum<MODE == HS_PROLONG>(L, C, q, p, code, v4, v1, ns);
+            if (MODE == HS_PROLONG)
+                quad_nbr_sum<true>(L, q, p, code, v4, v1,
+                                   [&](int i, int j, int k) { return parent_z(C, C.z[0], C.z[1], i, j, k); }, ns);
+            else
+                quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
         }
 #pragma unroll
         for (int m = 0; m < 4; m++) {
@@ -1030,9 +1075,9 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
             float pe[4], ns[4];
             pn4(L.z[pl], f.p[pc][pl], q.t0, pe);
             quad_nbr_sum<false>(
-                L, L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
+                L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
                 [&](int e) { return first ? __ldg(zo + e) : __fadd_rn(__ldg(zo + e), __fmul_rn(beta, __ldg(po + e))); },
-                ns);
+                NoParent(), ns);
 #pragma unroll
             for (int m = 0; m < 4; m++) {
                 if (code[m] & CELL_FLUID) {
@@ -1081,8 +1126,8 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
             ld4c(L.r[pl] + q.t0, r);
             if (!first) ld4c(f.x[pl] + q.t0, x);
             quad_nbr_sum<false>(
-                L, L, q, h, code, [&](int e, float(&o)[4]) { ld4(po + e, o); }, [&](int e) { return __ldg(po + e); },
-                ns);
+                L, q, h, code, [&](int e, float(&o)[4]) { ld4(po + e, o); }, [&](int e) { return __ldg(po + e); },
+                NoParent(), ns);
 #pragma unroll
             for (int m = 0; m < 4; m++) {
                 r[m] = r[m] - mean;
@@ -1143,8 +1188,8 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
                     const float* __restrict__ zo = F.z[pl ^ 1];
                     float ns[4], zc[4], rc[4];
                     quad_nbr_sum<false>(
-                        F, F, q, h, code, [&](int e, float(&o)[4]) { ld4(zo + e, o); },
-                        [&](int e) { return __ldg(zo + e); }, ns);
+                        F, q, h, code, [&](int e, float(&o)[4]) { ld4(zo + e, o); },
+                        [&](int e) { return __ldg(zo + e); }, NoParent(), ns);
                     ld4(F.z[pl] + q.t0, zc);
                     ld4(F.r[pl] + q.t0, rc);
 #pragma unroll
