@@ -301,6 +301,75 @@ def run_reference(args, rank, world):
     return 0
 
 
+# "PCG time to 1e-6": the plain MGPCG solve of A x = b (6 levels, all walls)
+# for a seeded N(0,1) mean-removed right-hand side, run until the CG residual
+# satisfies ||r|| <= 1e-6 ||b|| (r.r <= 1e-12 b.b)
+PCG_REL = 1e-6
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) summed over the
+# launches of that solve (4 CG iterations), one ncu capture of
+# `bench.py --pcg-only` with the host-driven solver loop (EDGE_MGPCG_EAGER=1);
+# ncu flushes the caches before every launch, so this is the cold-L2 figure
+PCG_TRAFFIC = 1498300672
+
+
+def pcg_measure(res, reps=5):
+    import torch
+    from edgeb200.projection import Projection
+    g = torch.Generator().manual_seed(1)
+    b = torch.randn(res, generator=g, dtype=torch.float64)
+    b -= b.mean()
+    bb = float((b * b).sum())
+    b = b.float().cuda()
+    x = torch.zeros(res, device="cuda")
+    P = Projection(res, base_level=BASE_LEVEL)
+    tol = PCG_REL * PCG_REL * bb
+    P.solve(b, x, abs_tol=tol, rel_tol=0.0)  # captures the solve graph
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.solve(b, x, abs_tol=tol, rel_tol=0.0)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    it, rtr, st = P.result()
+    Ax = torch.empty_like(x)
+    P.apply_A(x, Ax)
+    true_rel = float((Ax.double() - b.double()).norm() / b.double().norm())
+    nc = res[0] * res[1] * res[2]
+    nbytes = 100 * nc + (it + 1) * 117 * nc  # set-up + one preconditioned CG iteration per iteration (+1: set-up V-cycle)
+    ms = statistics.median(times)
+    P.close()
+    return {"ms": ms, "iters": it, "status": st, "rel_residual": math.sqrt(rtr / bb), "true_rel_residual": true_rel,
+            "algorithmic_bytes": nbytes, "res": list(res), "rhs": "N(0,1) seed 1, mean removed"}
+
+
+# FLOPs per cell of the marches, counted from the reference's arithmetic
+# (EDGE: 5 trajectories x (RK4 with Jacobian + Hermite value/gradient))
+MARCH_FLOP_PER_CELL = {"edge": 27400, "ed4": 8400, "ed8": 16800}
+
+
+def march_roofline(stages, variant, peak_tflops, ncells):
+    ms = stages.get("march_edge", 0.0)
+    if ms <= 0 or not peak_tflops:
+        return None
+    flops = MARCH_FLOP_PER_CELL[variant] * ncells
+    ach = flops / (ms * 1e-3) / 1e12
+    return {"kernel": f"k_march_{variant}_p", "bound": "fp32", "achieved": ach, "peak": peak_tflops,
+            "unit": "TFLOP/s", "frac": ach / peak_tflops, "flop_per_cell": MARCH_FLOP_PER_CELL[variant],
+            "peak_source": "measured here (edge_fma_peak, FP32 FMA chains)"}
+
+
+def run_pcg_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    res = tuple(args.res) if args.res else RES
+    print(json.dumps({"pcg": pcg_measure(res, reps=1)}), flush=True)
+    return 0
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -310,7 +379,7 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     from edgeb200 import ops
-    sim = make_sim(args.variant, args.res, packed=args.packed)
+    sim = make_sim(args.variant, args.res, packed=not args.unpacked)
     if args.res and tuple(args.res) != RES:
         args.no_cpu_baseline = True  # profiling runs on a smaller grid
     for _ in range(args.warmup):
@@ -371,14 +440,45 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "1 full substep of the same workload (first step after reinit), C/OpenMP restatement "
                          "of the reference kernels"}
+    # ED4 / ED8 steps of the same workload (a few steps each, outside the
+    # timed region of the EDGE line)
+    variants = {}
+    if not args.no_variants and args.variant == "edge" and not args.res:
+        del sim
+        torch.cuda.empty_cache()
+        for v in ("ed4", "ed8"):
+            vs = make_sim(v, args.res, packed=not args.unpacked)
+            for _ in range(3):
+                vs.step()
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record()
+            for _ in range(6):
+                vs.step()
+            a1.record()
+            torch.cuda.synchronize()
+            vst, _ = instrumented_step(vs)
+            variants[v] = {"ms_per_step": a0.elapsed_time(a1) / 6, "steps_per_s": 6e3 / a0.elapsed_time(a1),
+                           "march_ms": round(vst.get("march_edge", 0.0), 4)}
+            del vs
+            torch.cuda.empty_cache()
+    pcg = pcg_measure(RES) if not args.res else None
+    fp32_peak = ops.fma_peak_tflops()
     if world > 1:
         dist.barrier()
     if rank == 0:
         hbm, src = peaks()
-        # dominant HBM-bound stage: one MGPCG solve (graph of the CG loop)
-        solve_ms = stages.get("mgpcg_solve_2", 0.0)
-        it2 = max(iters[1], 0) + 1
-        mg_bytes = MG_SETUP_BYTES + it2 * MG_ITER_BYTES
+        # HBM-bound roofline: the plain MGPCG solve to 1e-6 (one CUDA graph:
+        # set-up, CG loop, solution copy); else the step's second projection
+        if pcg:
+            roof_kernel = "mgpcg_solve to 1e-6 relative residual (CG loop graph)"
+            mg_bytes, solve_ms, it2 = pcg["algorithmic_bytes"], pcg["ms"], pcg["iters"]
+        else:
+            roof_kernel = "mgpcg_solve (CG loop graph, second projection of the step)"
+            solve_ms = stages.get("mgpcg_solve_2", 0.0)
+            it2 = max(iters[1], 0) + 1
+            mg_bytes = MG_SETUP_BYTES + it2 * MG_ITER_BYTES
         achieved = mg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -387,11 +487,15 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": "four-vortex collision 256x128x128, EDGE, CFL 0.5, reinit 12, 6-level MGPCG, "
                                    "BFECC clamp", "res": list(RES), "variant": args.variant,
                        "parallelism": f"replicas x{world}", "l2": "step working set ~1.7 GB > L2 (no flush needed)"},
-            "roofline": {"kernel": "mgpcg_solve (CG loop graph, second projection of the step)", "bound": "hbm",
+            "roofline": {"kernel": roof_kernel, "bound": "hbm",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "frac": (achieved / hbm) if achieved else None,
+                         "traffic": PCG_TRAFFIC if pcg else None,
                          "algorithmic_bytes": mg_bytes, "iterations": it2, "peak_source": src},
             "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+            "roofline_fp32": march_roofline(stages, args.variant, fp32_peak, NC),
+            "pcg": pcg,
+            "variants": variants or None,
             "mgpcg_iters": list(iters),
             "clocks": clk.summary(),
             "gpu_launches": launches,
@@ -416,7 +520,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=2)
-    ap.add_argument("--packed", action="store_true", help="float4-plane map layout in the device driver")
+    ap.add_argument("--unpacked", action="store_true", help="separate-field map layout in the device driver "
+                    "(default: float4 planes)")
+    ap.add_argument("--pcg-only", action="store_true", help="only the PCG-to-1e-6 measurement (profiling)")
+    ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8 step timings")
     ap.add_argument("--res", type=int, nargs=3, default=None,
                     help="grid override for profiling a smaller case (not a bench line)")
     args = ap.parse_args()
@@ -425,6 +532,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.pcg_only:
+        return run_pcg_only(args)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -234,3 +234,24 @@ def lp_position(vel, pos, dt, num, L):
 def lp_viscous(u, dx, Re, vis):
     nx, ny, nz = dims_from_faces(*u)
     _call("edge_lp_viscous", nx, ny, nz, F(dx), F(Re), *_p3(u), *_p3(vis), stream())
+
+
+# ---- measurement ------------------------------------------------------------------
+def fma_peak_tflops(iters=2048, reps=3):
+    """FP32 FMA throughput of the current GPU in TFLOP/s (best of `reps`
+    launches of 8 resident blocks per SM, timed with CUDA events)."""
+    dev = torch.cuda.current_device()
+    blocks = 8 * torch.cuda.get_device_properties(dev).multi_processor_count
+    out = torch.zeros(1, device="cuda")
+    flops = ctypes.c_double()
+    _call("edge_fma_peak", blocks, iters, ptr(out), ctypes.byref(flops), stream())  # warm-up
+    best = 0.0
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _call("edge_fma_peak", blocks, iters, ptr(out), ctypes.byref(flops), stream())
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best

@@ -245,6 +245,13 @@ int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level, const int
                                float *uz, double abs_tol, double rel_tol, int max_iters, int *iters, double *rTr,
                                int *status, void *stream);
 
+/* ---- measurement ---------------------------------------------------------- */
+/* FP32 FMA throughput probe (no reference counterpart): `blocks` blocks of
+ * 256 threads run `iters` x 128 dependent-chain FMAs each; *flops receives
+ * the floating-point operations enqueued.  Time it with events on `stream`.
+ * `out` is a device float that is never written for these inputs. */
+int edge_fma_peak(int blocks, int iters, float *out, double *flops, void *stream);
+
 /* ---- laden particles (sim/lp.py) ---------------------------------------- */
 /* update_particles_acc, lp.py:6-29 (acc zeroed for all nmax particles) */
 int edge_lp_acc(int nx, int ny, int nz, float dx, const float *ux, const float *uy, const float *uz,
