@@ -31,6 +31,16 @@ def ptr(t, name="field"):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def ptr_any(t, dtypes, name="tensor"):
+    """Device pointer of a contiguous CUDA tensor of one of `dtypes` (the
+    network's bf16 / int32 / float32 / float64 buffers)."""
+    if t is None:
+        return NULL
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or not t.is_contiguous() or t.dtype not in dtypes:
+        raise ValueError(f"{name} must be a contiguous CUDA tensor of {dtypes}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
 def stream(device=None):
     return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 

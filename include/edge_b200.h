@@ -252,6 +252,70 @@ int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level, const int
  * `out` is a device float that is never written for these inputs. */
 int edge_fma_peak(int blocks, int iters, float *out, double *flops, void *stream);
 
+/* ---- learned preconditioner (no reference counterpart) ------------------------
+ * A 3-D U-Net whose 16-64 channel 3x3x3 convolutions run on the tensor cores
+ * (tcgen05, BF16 operands, FP32 accumulation in TMEM).  Activation tensors
+ * are "padded chunked" bf16: interior grid X x Y x Z with a zero voxel of
+ * padding on each side, channels in chunks of 8, each chunk *chunk_voxels
+ * voxels long (guards included); a tensor of C channels holds
+ * C/8 * chunk_voxels * 8 bf16 values and starts zeroed.  Calls that can give
+ * up a bounded wait set the device int *err to 1. */
+/* One-CTA tcgen05 GEMM D = A B^T (layout self-test).  mode 0: M = 128, A is
+ * 128 x K, B is N x K; mode 1: M = 64, A is K x 64, B is K x N.  D is M x N
+ * row-major FP32; 16 <= N, K <= 256, multiples of 16. */
+int edge_tc_selftest(int mode, int N, int K, const void *A, const void *B, float *D, int *err, void *stream);
+int edge_unet_geometry(int X, int Y, int Z, long long *chunk_voxels);
+/* y = act(conv3(x0; w0) [+ conv3(x1; w1)] + bias): 3x3x3 zero-padded
+ * cross-correlation, tap t = 9(dx+1) + 3(dy+1) + (dz+1) reading x[v+(dx,dy,dz)].
+ * cin0, cin1, cout in {16, 32, 64}; w packed by edge_unet_pack_weights;
+ * flags bit 0: ReLU, bit 1: add the result to y; x1 and bias may be NULL. */
+int edge_unet_conv(int X, int Y, int Z, const void *x0, const void *w0, int cin0, const void *x1, const void *w1,
+                   int cin1, int cout, const float *bias, int flags, void *y, int *err, void *stream);
+/* dw[co][ci][27] (float32) = sum over voxels of d[v][co] x[v+off(t)][ci] on
+ * the tensor cores; partial holds nsplit * 27 * cout * cin floats. */
+int edge_unet_wgrad(int X, int Y, int Z, const void *d, int cout, const void *x, int cin, float *partial,
+                    int nsplit, float *dw, int *err, void *stream);
+/* First layer (1 -> 16, ReLU) of r (float32 X x Y x Z) times *scale, and last
+ * layer (16 -> 1, divided by *scale), on the SIMT cores; w [16][27] float
+ * (bf16-rounded values). */
+int edge_unet_conv_first(int X, int Y, int Z, const float *r, const float *scale, const float *w, const float *bias,
+                         void *y, void *stream);
+int edge_unet_conv_last(int X, int Y, int Z, const void *f, const float *w, const float *bias, const float *scale,
+                        float *z, void *stream);
+/* Backward of the first layer (weight gradient dw [16][27] from its
+ * pre-activation gradient d) and of the last (data gradient df and weight
+ * gradient dw [16][27] from dzn, the gradient of the output times *scale);
+ * partial holds 27 * nblk * 16 floats. */
+int edge_unet_first_bwd(int X, int Y, int Z, const void *d, const float *r, const float *scale, float *partial,
+                        int nblk, float *dw, void *stream);
+int edge_unet_last_bwd(int X, int Y, int Z, const float *dzn, const float *w, const void *f, void *df,
+                       float *partial, int nblk, float *dw, void *stream);
+/* out[c] = sum over voxels of d[v][c] (bias gradients); partial holds
+ * channels * nblk floats. */
+int edge_unet_chan_sum(int X, int Y, int Z, int channels, const void *d, float *partial, int nblk, float *out,
+                       void *stream);
+/* out = dy where y > 0, else 0 (whole tensors). */
+int edge_unet_relu_bwd(int X, int Y, int Z, int channels, const void *dy, const void *y, void *out, void *stream);
+/* 2x2x2 mean pooling fine -> coarse and its backward (dfine = dcoarse/8,
+ * added when accum); nearest 2x upsampling coarse -> fine and its backward
+ * (sum of the 8 children).  X, Y, Z: the fine grid. */
+int edge_unet_pool(int X, int Y, int Z, int channels, const void *fine, void *coarse, void *stream);
+int edge_unet_pool_bwd(int X, int Y, int Z, int channels, const void *dcoarse, void *dfine, int accum, void *stream);
+int edge_unet_upsample(int X, int Y, int Z, int channels, const void *coarse, void *fine, void *stream);
+int edge_unet_up_bwd(int X, int Y, int Z, int channels, const void *dfine, void *dcoarse, void *stream);
+/* float32 weights [cout][cin][27] -> packed bf16 [27][cin/8][cout][8]; with
+ * transpose != 0 the data-gradient form [27][cout/8][cin][8] of w[co][ci][26-t]. */
+int edge_unet_pack_weights(const float *w, int cout, int cin, int transpose, void *out, void *stream);
+/* *scale = 1 / rms(r) over n values (the network's input normalisation). */
+int edge_unet_input_scale(const float *r, long long n, float *scale, void *stream);
+/* Training loss on the scaled problem, d = (z - target) * scale:
+ * stats[0] = mean(d), stats[1] = mean((d - mean d)^2); dzn = 2 (d - mean d) / n. */
+int edge_unet_loss(const float *z, const float *target, const float *scale, long long n, double *stats, float *dzn,
+                   void *stream);
+/* One Adam step on n float32 parameters (step counts from 1). */
+int edge_unet_adam(long long n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps,
+                   int step, void *stream);
+
 /* ---- laden particles (sim/lp.py) ---------------------------------------- */
 /* update_particles_acc, lp.py:6-29 (acc zeroed for all nmax particles) */
 int edge_lp_acc(int nx, int ny, int nz, float dx, const float *ux, const float *uy, const float *uz,
