@@ -341,8 +341,30 @@ def pcg_measure(res, reps=5):
     nc = res[0] * res[1] * res[2]
     nbytes = 100 * nc + (it + 1) * 117 * nc  # set-up + one preconditioned CG iteration per iteration (+1: set-up V-cycle)
     ms = statistics.median(times)
+    # errors against an FP64 solve of the same system, and the mixed-precision
+    # solver (BF16 V-cycle storage, FP32 residual, FP64 dots) on it
+    from edgeb200.precision import fp64_solve, rel_error
+    ref = fp64_solve(P, b)
+    err32 = rel_error(x, ref)
+    P16 = Projection(res, base_level=BASE_LEVEL, precision=1)
+    x16 = torch.zeros(res, device="cuda")
+    P16.solve(b, x16, abs_tol=tol, rel_tol=0.0)
+    t16 = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P16.solve(b, x16, abs_tol=tol, rel_tol=0.0)
+        e1.record()
+        torch.cuda.synchronize()
+        t16.append(e0.elapsed_time(e1))
+    it16, rtr16, st16 = P16.result()
+    mixed = {"ms": statistics.median(t16), "iters": it16, "status": st16, "rel_residual": math.sqrt(rtr16 / bb),
+             "fp64_rel_error": rel_error(x16, ref), "speedup_vs_fp32": ms / statistics.median(t16)}
+    P16.close()
     P.close()
     return {"ms": ms, "iters": it, "status": st, "rel_residual": math.sqrt(rtr / bb), "true_rel_residual": true_rel,
+            "fp64_rel_error": err32, "mixed": mixed,
             "algorithmic_bytes": nbytes, "res": list(res), "rhs": "N(0,1) seed 1, mean removed"}
 
 
@@ -360,6 +382,62 @@ def march_roofline(stages, variant, peak_tflops, ncells):
     return {"kernel": f"k_march_{variant}_p", "bound": "fp32", "achieved": ach, "peak": peak_tflops,
             "unit": "TFLOP/s", "frac": ach / peak_tflops, "flop_per_cell": MARCH_FLOP_PER_CELL[variant],
             "peak_source": "measured here (edge_fma_peak, FP32 FMA chains)"}
+
+
+WEIGHTS = os.path.join(PKG, "edgeb200", "weights", "unet_pcg.npz")
+
+
+def learned_measure(res, reps=3):
+    """Flexible CG to 1e-6 on the same right-hand side as the plain solve,
+    preconditioned by the trained U-Net warm-starting the V-cycle, next to
+    the same flexible CG with the plain V-cycle; plus one network forward."""
+    import torch
+    from edgeb200.projection import Projection
+    from edgeb200.train_unet import load_params
+    from edgeb200.unet import LearnedPCG, UNet
+    if not os.path.exists(WEIGHTS):
+        return None
+    g = torch.Generator().manual_seed(1)
+    b = torch.randn(res, generator=g, dtype=torch.float64)
+    b = (b - b.mean()).float().cuda()
+    P = Projection(res, base_level=BASE_LEVEL)
+    net = UNet(res, params=load_params(WEIGHTS))
+    pcg = LearnedPCG(P, net)
+    x = torch.zeros(res, device="cuda")
+    out = {}
+    for mode in ("vcycle", "warm"):
+        pcg.solve(b, x, rel_tol=PCG_REL, mode=mode)
+        times = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            it, rel, fb = pcg.solve(b, x, rel_tol=PCG_REL, mode=mode)
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+        out[mode] = {"iters": it, "ms_wall": statistics.median(times), "rel_residual": rel, "fell_back": fb}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    z = torch.empty_like(b)
+    net.forward(b, z)
+    e0.record()
+    for _ in range(reps):
+        net.forward(b, z)
+    e1.record()
+    torch.cuda.synchronize()
+    out["unet_forward_ms"] = e0.elapsed_time(e1) / reps
+    out["unet_timed_out"] = net.timed_out()
+    out["note"] = ("flexible CG driven from Python (host-synchronised scalars) in both modes; "
+                   "time ratio vs the graph-captured plain solve is in pcg.ms")
+    P.close()
+    return out
+
+
+def run_learned_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    res = tuple(args.res) if args.res else RES
+    print(json.dumps({"learned": learned_measure(res, reps=1)}), flush=True)
+    return 0
 
 
 def run_pcg_only(args):
@@ -443,6 +521,8 @@ def run_ours(args, rank, world, local_rank):
     # ED4 / ED8 steps of the same workload (a few steps each, outside the
     # timed region of the EDGE line)
     variants = {}
+    if args.no_extras:
+        args.no_variants = True
     if not args.no_variants and args.variant == "edge" and not args.res:
         del sim
         torch.cuda.empty_cache()
@@ -463,8 +543,10 @@ def run_ours(args, rank, world, local_rank):
                            "march_ms": round(vst.get("march_edge", 0.0), 4)}
             del vs
             torch.cuda.empty_cache()
-    pcg = pcg_measure(RES) if not args.res else None
-    fp32_peak = ops.fma_peak_tflops()
+    pcg = pcg_measure(RES) if not (args.res or args.no_extras) else None
+    if pcg is not None:
+        pcg["learned"] = learned_measure(RES)
+    fp32_peak = ops.fma_peak_tflops() if not args.no_extras else None
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -523,7 +605,10 @@ def main():
     ap.add_argument("--unpacked", action="store_true", help="separate-field map layout in the device driver "
                     "(default: float4 planes)")
     ap.add_argument("--pcg-only", action="store_true", help="only the PCG-to-1e-6 measurement (profiling)")
+    ap.add_argument("--learned-only", action="store_true", help="only the learned-preconditioner measurement")
     ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8 step timings")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="only the EDGE steps (no ED4/ED8, PCG or FP32-peak measurements; profiling)")
     ap.add_argument("--res", type=int, nargs=3, default=None,
                     help="grid override for profiling a smaller case (not a bench line)")
     args = ap.parse_args()
@@ -534,6 +619,8 @@ def main():
         return run_reference(args, rank, world)
     if args.pcg_only:
         return run_pcg_only(args)
+    if args.learned_only:
+        return run_learned_only(args)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -19,6 +19,7 @@
 // The all-Neumann recentering (mgpcg.py:169-175) is kept as a pending scalar
 // `mean` that every reader of r[0] subtracts and that the r update folds into
 // the stored residual.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -106,6 +107,7 @@ struct Ctx {
     G g;
     Fine f;
     int csmem;  // dynamic shared memory of k_coarse (bytes)
+    int zbf16;  // 1: the V-cycle's level arrays are BF16 (mixed-precision solver)
 };
 
 EDGE_D void set_cond(const G& g, unsigned v) {
@@ -184,6 +186,64 @@ EDGE_D float parent_z(const LV& C, const float* zc0, const float* zc1, int i, in
     int I = i >> 1, J = j >> 1, K = k >> 1;
     int e = (I * C.n1 + J) * C.H + (K >> 1);
     return ((I + J + K) & 1) ? zc1[e] : zc0[e];
+}
+
+// Storage of the V-cycle's level arrays: FP32, or BF16 in the mixed-precision
+// solver (the arithmetic stays FP32).  Level 0's r is the CG residual and is
+// FP32 in both; pointers are carried as float* and reinterpreted.
+template <class ZT>
+struct Zs;
+template <>
+struct Zs<float> {
+    static EDGE_D float ld(const float* b, int e) { return __ldg(b + e); }
+    static EDGE_D void st(float* b, int e, float v) { b[e] = v; }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        float4 t = __ldg(reinterpret_cast<const float4*>(b + e));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+    static EDGE_D void st4(float* b, int e, const float (&v)[4]) {
+        *reinterpret_cast<float4*>(b + e) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    static EDGE_D void st2(float* b, int e, float x, float y) { *reinterpret_cast<float2*>(b + e) = make_float2(x, y); }
+};
+template <>
+struct Zs<__nv_bfloat16> {
+    static EDGE_D const __nv_bfloat16* h(const float* b) { return reinterpret_cast<const __nv_bfloat16*>(b); }
+    static EDGE_D __nv_bfloat16* h(float* b) { return reinterpret_cast<__nv_bfloat16*>(b); }
+    static EDGE_D float ld(const float* b, int e) { return __bfloat162float(h(b)[e]); }
+    static EDGE_D void st(float* b, int e, float v) { h(b)[e] = __float2bfloat16_rn(v); }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        const uint2 u = *reinterpret_cast<const uint2*>(h(b) + e);
+        const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&u.x);
+        const __nv_bfloat162 c = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
+        v[0] = __low2float(a); v[1] = __high2float(a); v[2] = __low2float(c); v[3] = __high2float(c);
+    }
+    static EDGE_D void st4(float* b, int e, const float (&v)[4]) {
+        __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), c = __floats2bfloat162_rn(v[2], v[3]);
+        uint2 u;
+        u.x = *reinterpret_cast<unsigned*>(&a);
+        u.y = *reinterpret_cast<unsigned*>(&c);
+        *reinterpret_cast<uint2*>(h(b) + e) = u;
+    }
+    static EDGE_D void st2(float* b, int e, float x, float y) {
+        *reinterpret_cast<__nv_bfloat162*>(h(b) + e) = __floats2bfloat162_rn(x, y);
+    }
+};
+// r of a level: FP32 at level 0, else the level storage type
+template <class ZT>
+EDGE_D float rld(const float* b, int e, int level0) { return level0 ? __ldg(b + e) : Zs<ZT>::ld(b, e); }
+template <class ZT>
+EDGE_D void rld4(const float* b, int e, int level0, float (&v)[4]) {
+    if (level0) Zs<float>::ld4(b, e, v);
+    else Zs<ZT>::ld4(b, e, v);
+}
+
+// z of the coarse level (global storage) at the parent of fine cell (i, j, k)
+template <class ZT, class LV>
+EDGE_D float parent_zg(const LV& C, int i, int j, int k) {
+    int I = i >> 1, J = j >> 1, K = k >> 1;
+    int e = (I * C.n1 + J) * C.H + (K >> 1);
+    return Zs<ZT>::ld(C.z[(I + J + K) & 1], e);
 }
 
 // ---------------------------------------------------------------------------
@@ -476,7 +536,7 @@ EDGE_D unsigned code_at(const Lvl& L, int plane, int e, int i, int j, int k) {
 // and the p.Ap partials; the last block forms alpha (mgpcg.py:237-240).
 // Products are rounded before the sums (no fused multiply-add), as the
 // reference's separate kernels round them.
-template <bool SOLID>
+template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
     count_launch(g.st);
     // The loop stops unless the iteration's last kernel completes its
@@ -503,9 +563,11 @@ __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
             if (code & CELL_FLUID) {
                 const float* __restrict__ zo = L.z[pl ^ 1];
                 const float* __restrict__ po = f.p[pc][pl ^ 1];
-                pe = first ? __ldg(L.z[pl] + t) : __fadd_rn(__ldg(L.z[pl] + t), __fmul_rn(beta, __ldg(f.p[pc][pl] + t)));
+                const float zt = Zs<ZT>::ld(L.z[pl], t);
+                pe = first ? zt : __fadd_rn(zt, __fmul_rn(beta, __ldg(f.p[pc][pl] + t)));
                 float ns = nbr_sum(L, code, t, k, [&](int e, int) {
-                    return first ? __ldg(zo + e) : __fadd_rn(__ldg(zo + e), __fmul_rn(beta, __ldg(po + e)));
+                    const float ze = Zs<ZT>::ld(zo, e);
+                    return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e)));
                 });
                 float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, L, code, s.i, s.j, k), pe), ns);
                 v[0] += (double)pe * (double)ape;
@@ -593,7 +655,7 @@ __global__ void __launch_bounds__(256) k_cg_xr(G g, Lvl L, Fine f) {
 //     before its own value is read again, and solid cells are never read.
 enum { HS_FIRST = 0, HS_PLAIN = 1, HS_PROLONG = 2, HS_ZR = 3 };
 
-template <int MODE, bool SOLID>
+template <int MODE, bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, int color) {
     count_launch(g.st);
     if (!running(g)) {
@@ -612,19 +674,19 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
         if (k < L.n2) {
             const unsigned code = code_at<SOLID>(L, color, t, s.i, s.j, k);
             if (code & CELL_FLUID) {
-                const float rv = __ldg(rs + t) - mean;
+                const float rv = rld<ZT>(rs, t, level0) - mean;
                 float ns = 0.0f;
                 if (MODE == HS_PROLONG) {
                     ns = nbr_sum(L, code, t, k, [&](int e, int d) {
                         int di, dj, dk;
                         dir_offset(d, di, dj, dk);
-                        return __ldg(zo + e) + parent_z(C, C.z[0], C.z[1], s.i + di, s.j + dj, k + dk);
+                        return Zs<ZT>::ld(zo, e) + parent_zg<ZT>(C, s.i + di, s.j + dj, k + dk);
                     });
                 } else if (MODE != HS_FIRST) {
-                    ns = nbr_sum(L, code, t, k, [&](int e, int) { return __ldg(zo + e); });
+                    ns = nbr_sum(L, code, t, k, [&](int e, int) { return Zs<ZT>::ld(zo, e); });
                 }
                 const float zn = (rv + ns) / nf_of<SOLID>(g.bt, L, code, s.i, s.j, k);
-                zs[t] = zn;
+                Zs<ZT>::st(zs, t, zn);
                 if (MODE == HS_ZR) v[0] += (double)zn * (double)rv;
             }
         }
@@ -632,7 +694,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
             // the other cell of the slot (final from the previous half sweep)
             const int ko = 2 * s.kk + ((s.i + s.j + oc) & 1);
             if (ko < L.n2 && (code_at<SOLID>(L, oc, t, s.i, s.j, ko) & CELL_FLUID))
-                v[0] += (double)__ldg(zo + t) * (double)(__ldg(L.r[oc] + t) - mean);
+                v[0] += (double)Zs<ZT>::ld(zo, t) * (double)(rld<ZT>(L.r[oc], t, level0) - mean);
         }
     }
     if (MODE == HS_ZR) {
@@ -650,7 +712,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
 // One thread per coarse cell; the children of (I,J,K) all sit at slot
 // (i*n1 + j)*H + K of their planes.  With `first` it also applies the first
 // half sweep of the coarse level (z = r / n_fluid on colour 0).
-template <bool SOLID>
+template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0, int first) {
     count_launch(g.st);
     if (!running(g)) return;
@@ -673,17 +735,17 @@ __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0,
                     const unsigned code = code_at<SOLID>(F, pl, e, i, j, k);
                     if (!(code & CELL_FLUID)) continue;
                     const float* __restrict__ zo = F.z[pl ^ 1];
-                    float ns = nbr_sum(F, code, e, k, [&](int ee, int) { return __ldg(zo + ee); });
-                    float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, F, code, i, j, k), __ldg(F.z[pl] + e)), ns);
-                    float res = (__ldg(F.r[pl] + e) - mean) - az;
+                    float ns = nbr_sum(F, code, e, k, [&](int ee, int) { return Zs<ZT>::ld(zo, ee); });
+                    float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, F, code, i, j, k), Zs<ZT>::ld(F.z[pl], e)), ns);
+                    float res = (rld<ZT>(F.r[pl], e, level0) - mean) - az;
                     acc += res * 0.5f;
                 }
         const int pc = (I + J + K) & 1;
         const int ec = (I * C.n1 + J) * C.H + (K >> 1);
-        C.r[pc][ec] = acc;
+        Zs<ZT>::st(C.r[pc], ec, acc);
         if (first && pc == 0) {
             const unsigned cc = code_at<SOLID>(C, 0, ec, I, J, K);
-            if (cc & CELL_FLUID) C.z[0][ec] = (acc + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K);
+            if (cc & CELL_FLUID) Zs<ZT>::st(C.z[0], ec, (acc + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K));
         }
     }
 }
@@ -786,7 +848,7 @@ struct CLvl {
     int roff, zoff, coff;  // float offsets of the r and z planes, ushort offset of the codes
 };
 
-template <bool ZR, bool SOLID>
+template <bool ZR, bool SOLID, class ZT>
 __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     extern __shared__ float sh[];
     __shared__ CLvl cl[16];
@@ -823,8 +885,8 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     {
         const CLvl& q = cl[lc];
         for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
-            const float* src = e < q.P ? a.lv[lc].r[0] + e : a.lv[lc].r[1] + (e - q.P);
-            sh[q.roff + e] = __ldg(src) - mean;
+            const float* src = e < q.P ? a.lv[lc].r[0] : a.lv[lc].r[1];
+            sh[q.roff + e] = rld<ZT>(src, e < q.P ? e : e - q.P, lc == 0) - mean;
         }
         if (SOLID)
             for (int l = lc; l < L; l++) {
@@ -962,8 +1024,8 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     {
         const CLvl& q = cl[lc];
         for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
-            float* dst = e < q.P ? a.lv[lc].z[0] + e : a.lv[lc].z[1] + (e - q.P);
-            *dst = sh[q.zoff + e];
+            float* dst = e < q.P ? a.lv[lc].z[0] : a.lv[lc].z[1];
+            Zs<ZT>::st(dst, e < q.P ? e : e - q.P, sh[q.zoff + e]);
         }
     }
     if (ZR) {
@@ -982,7 +1044,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     }
 }
 
-template <int MODE, bool SOLID>
+template <int MODE, bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, int color) {
     count_launch(g.st);
     if (!running(g)) {
@@ -1001,13 +1063,13 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
         unsigned code[4];
         quad_codes<SOLID>(L, color, q, p, code);
         float rv[4], ns[4] = {0.0f, 0.0f, 0.0f, 0.0f}, zn[4];
-        ld4(rs + q.t0, rv);
+        rld4<ZT>(rs, q.t0, level0, rv);
         if (MODE != HS_FIRST) {
-            auto v4 = [&](int e, float(&o)[4]) { ld4(zo + e, o); };
-            auto v1 = [&](int e) { return __ldg(zo + e); };
+            auto v4 = [&](int e, float(&o)[4]) { Zs<ZT>::ld4(zo, e, o); };
+            auto v1 = [&](int e) { return Zs<ZT>::ld(zo, e); };
             if (MODE == HS_PROLONG)
                 quad_nbr_sum<true>(L, q, p, code, v4, v1,
-                                   [&](int i, int j, int k) { return parent_z(C, C.z[0], C.z[1], i, j, k); }, ns);
+                                   [&](int i, int j, int k) { return parent_zg<ZT>(C, i, j, k); }, ns);
             else
                 quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
         }
@@ -1018,14 +1080,14 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
                                            : 0.0f;
             if (MODE == HS_ZR && (code[m] & CELL_FLUID)) v[0] += (double)zn[m] * (double)rv[m];
         }
-        st4(zs + q.t0, zn);
+        Zs<ZT>::st4(zs, q.t0, zn);
         if (MODE == HS_ZR) {
             // the other cells of the slots (final from the previous half sweep)
             unsigned co[4];
             quad_codes<SOLID>(L, oc, q, p ^ 1, co);
             float ro[4], zz[4];
-            ld4(L.r[oc] + q.t0, ro);
-            ld4(zo + q.t0, zz);
+            rld4<ZT>(L.r[oc], q.t0, level0, ro);
+            Zs<ZT>::ld4(zo, q.t0, zz);
 #pragma unroll
             for (int m = 0; m < 4; m++)
                 if (co[m] & CELL_FLUID) v[0] += (double)zz[m] * (double)(ro[m] - mean);
@@ -1040,7 +1102,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
     }
 }
 
-template <bool SOLID>
+template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
     count_launch(g.st);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1064,7 +1126,7 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
             const float* __restrict__ zo = L.z[pl ^ 1];
             const float* __restrict__ po = f.p[pc][pl ^ 1];
             auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
-                ld4(zz + e, o);
+                Zs<ZT>::ld4(zz, e, o);
                 if (!first) {
                     float b[4];
                     ld4(pp + e, b);
@@ -1076,7 +1138,7 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
             pn4(L.z[pl], f.p[pc][pl], q.t0, pe);
             quad_nbr_sum<false>(
                 L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
-                [&](int e) { return first ? __ldg(zo + e) : __fadd_rn(__ldg(zo + e), __fmul_rn(beta, __ldg(po + e))); },
+                [&](int e) { const float ze = Zs<ZT>::ld(zo, e); return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e))); },
                 NoParent(), ns);
 #pragma unroll
             for (int m = 0; m < 4; m++) {
@@ -1161,7 +1223,7 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
 
 // restriction, four coarse cells (I, J, K0..K0+3) per thread: their children
 // are slots K0..K0+3 of both planes in the four fine rows (2I+a, 2J+b)
-template <bool SOLID>
+template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0, int first) {
     count_launch(g.st);
     if (!running(g)) return;
@@ -1188,10 +1250,10 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
                     const float* __restrict__ zo = F.z[pl ^ 1];
                     float ns[4], zc[4], rc[4];
                     quad_nbr_sum<false>(
-                        F, q, h, code, [&](int e, float(&o)[4]) { ld4(zo + e, o); },
-                        [&](int e) { return __ldg(zo + e); }, NoParent(), ns);
-                    ld4(F.z[pl] + q.t0, zc);
-                    ld4(F.r[pl] + q.t0, rc);
+                        F, q, h, code, [&](int e, float(&o)[4]) { Zs<ZT>::ld4(zo, e, o); },
+                        [&](int e) { return Zs<ZT>::ld(zo, e); }, NoParent(), ns);
+                    Zs<ZT>::ld4(F.z[pl], q.t0, zc);
+                    rld4<ZT>(F.r[pl], q.t0, level0, rc);
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         if (!(code[m] & CELL_FLUID)) continue;
@@ -1206,8 +1268,8 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
         // at slots ecb, ecb+1
         const int ecb = (I * C.n1 + J) * C.H + (K0 >> 1);
         const int pa = (I + J) & 1;
-        *reinterpret_cast<float2*>(C.r[pa] + ecb) = make_float2(acc[0], acc[2]);
-        *reinterpret_cast<float2*>(C.r[pa ^ 1] + ecb) = make_float2(acc[1], acc[3]);
+        Zs<ZT>::st2(C.r[pa], ecb, acc[0], acc[2]);
+        Zs<ZT>::st2(C.r[pa ^ 1], ecb, acc[1], acc[3]);
         if (first) {
             // first half sweep of the coarse level: z = r / n_fluid on colour 0
             const int m0 = pa;  // the colour-0 cells are m0 and m0 + 2
@@ -1218,7 +1280,7 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
                 const unsigned cc = SOLID ? (unsigned)C.code[0][ecb + u] : range_code(C, I, J, K);
                 zz[u] = (cc & CELL_FLUID) ? (acc[m] + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K) : 0.0f;
             }
-            *reinterpret_cast<float2*>(C.z[0] + ecb) = make_float2(zz[0], zz[1]);
+            Zs<ZT>::st2(C.z[0], ecb, zz[0], zz[1]);
         }
     }
 }
@@ -1262,7 +1324,8 @@ __global__ void __launch_bounds__(256) k_grad_p(G g, Lvl L, Fine f, Faces U) {
 
 // red-black planes <-> lexicographic field of one level; `valid` (may be
 // NULL) gates the planes' content (x before the first update reads as 0)
-__global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p1, float* dst, const int* valid) {
+__global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p1, float* dst, const int* valid,
+                          int bf16) {
     if (st) count_launch(st);
     const bool ok = valid == nullptr || *valid != 0;
     GRID_STRIDE(t, L.n0 * L.n1 * L.n2) {
@@ -1271,7 +1334,8 @@ __global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p
         int i = fdiv(row, L.d1);
         int j = row - i * L.n1;
         const float* p = ((i + j + k) & 1) ? p1 : p0;
-        dst[t] = ok ? p[row * L.H + (k >> 1)] : 0.0f;
+        const int e = row * L.H + (k >> 1);
+        dst[t] = ok ? (bf16 ? Zs<__nv_bfloat16>::ld(p, e) : p[e]) : 0.0f;
     }
 }
 
@@ -1325,6 +1389,26 @@ __global__ void k_apply_A(G g, Lvl L, const float* p, float* Ap) {
         if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
     }
     Ap[e] = __fsub_rn(__fmul_rn(n_fluid_lex(g.bt, L, i, j, k), p[e]), ns);
+}
+
+// the same operator in float64 (the FP64 reference solve of the precision study)
+__global__ void k_apply_A64(G g, Lvl L, const double* p, double* Ap) {
+    int n = L.n0 * L.n1 * L.n2;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    if (!is_fluid(L.bm, e)) {
+        Ap[e] = 0.0;
+        return;
+    }
+    int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+    int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+    int stride[3] = {L.n1 * L.n2, L.n2, 1};
+    double ns = 0.0;
+    for (int a = 0; a < 3; a++) {
+        if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += p[e + stride[a]];
+        if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
+    }
+    Ap[e] = (double)n_fluid_lex(g.bt, L, i, j, k) * p[e] - ns;
 }
 
 // ---------------------------------------------------------------------------
@@ -1408,17 +1492,25 @@ void plan_coarse(Ctx& c, bool solid) {
 int prepare_coarse_kernels(const Ctx& c) {
     if ((size_t)c.csmem > kCoarseSmem) return EDGE_EINVAL;  // the coarsest level alone must fit
     if (c.csmem > 48 * 1024) {
-        CK(cudaFuncSetAttribute(k_coarse<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<true, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<true, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<true, false, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false, false, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<true, true, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                c.csmem));
+        CK(cudaFuncSetAttribute(k_coarse<false, true, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                c.csmem));
     }
     return EDGE_OK;
 }
 
 // One V-cycle (mgpcg.py:177-195); with final_zr the last kernel also forms
 // z.r and the end-of-iteration bookkeeping (mgpcg.py:263-277).
-template <bool S>
+template <bool S, class ZT>
 void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
     const Levels& V = c.lv;
     const int lc = V.lc;
@@ -1428,22 +1520,22 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
         const int l0 = l == 0, first = l + 1 < lc;
         if (L.vec) {
             const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-            if (l == 0) k_hsweep4<HS_FIRST, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_restrict4<S><<<rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream>>>(c.g, L, C, l0, first);
+            if (l == 0) k_hsweep4<HS_FIRST, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_restrict4<S, ZT><<<rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream>>>(c.g, L, C, l0, first);
         } else {
             const int g = rgrid(L.P);
-            if (l == 0) k_hsweep<HS_FIRST, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_restrict<S><<<rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c.g, L, C, l0, first);
+            if (l == 0) k_hsweep<HS_FIRST, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_restrict<S, ZT><<<rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c.g, L, C, l0, first);
         }
     }
-    if (final_zr && lc == 0) k_coarse<true, S><<<1, 1024, c.csmem, stream>>>(c.g, V);
-    else k_coarse<false, S><<<1, 1024, c.csmem, stream>>>(c.g, V);
+    if (final_zr && lc == 0) k_coarse<true, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
+    else k_coarse<false, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
     for (int l = lc - 1; l >= 0; l--) {
         const Lvl& L = V.lv[l];
         const Lvl& C = V.lv[l + 1];
@@ -1451,45 +1543,53 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
         const bool zr = l == 0 && final_zr;
         if (L.vec) {
             const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-            k_hsweep4<HS_PROLONG, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            if (zr) k_hsweep4<HS_ZR, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            else k_hsweep4<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PROLONG, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            if (zr) k_hsweep4<HS_ZR, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            else k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
         } else {
             const int g = rgrid(L.P);
-            k_hsweep<HS_PROLONG, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            if (zr) k_hsweep<HS_ZR, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            else k_hsweep<HS_PLAIN, S><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PROLONG, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
+            if (zr) k_hsweep<HS_ZR, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            else k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
         }
     }
 }
 
 void enqueue_vcycle(const Ctx& c, bool solid, cudaStream_t stream, bool final_zr) {
-    if (solid) vcycle_t<true>(c, stream, final_zr);
-    else vcycle_t<false>(c, stream, final_zr);
+    if (c.zbf16) {
+        if (solid) vcycle_t<true, __nv_bfloat16>(c, stream, final_zr);
+        else vcycle_t<false, __nv_bfloat16>(c, stream, final_zr);
+    } else {
+        if (solid) vcycle_t<true, float>(c, stream, final_zr);
+        else vcycle_t<false, float>(c, stream, final_zr);
+    }
+}
+
+template <bool S, class ZT>
+void cg_kernels(const Ctx& c, cudaStream_t stream) {
+    const Lvl& L = c.lv.lv[0];
+    if (L.vec) {
+        const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
+        k_cg_ap4<S, ZT><<<g, 256, 0, stream>>>(c.g, L, c.f);
+        k_cg_xr4<S><<<g, 256, 0, stream>>>(c.g, L, c.f);
+    } else {
+        k_cg_ap<S, ZT><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+        k_cg_xr<S><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+    }
 }
 
 // The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
 void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
-    const Lvl& L = c.lv.lv[0];
-    if (L.vec) {
-        const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-        if (solid) {
-            k_cg_ap4<true><<<g, 256, 0, stream>>>(c.g, L, c.f);
-            k_cg_xr4<true><<<g, 256, 0, stream>>>(c.g, L, c.f);
-        } else {
-            k_cg_ap4<false><<<g, 256, 0, stream>>>(c.g, L, c.f);
-            k_cg_xr4<false><<<g, 256, 0, stream>>>(c.g, L, c.f);
-        }
-    } else if (solid) {
-        k_cg_ap<true><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
-        k_cg_xr<true><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+    if (c.zbf16) {
+        if (solid) cg_kernels<true, __nv_bfloat16>(c, stream);
+        else cg_kernels<false, __nv_bfloat16>(c, stream);
     } else {
-        k_cg_ap<false><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
-        k_cg_xr<false><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+        if (solid) cg_kernels<true, float>(c, stream);
+        else cg_kernels<false, float>(c, stream);
     }
     enqueue_vcycle(c, solid, stream, true);
 }
@@ -1535,7 +1635,7 @@ void enqueue_finish(Solver* s, Faces U, const float* rhs, float* xout, cudaStrea
         k_grad_p<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U);
         if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.g.st, nx, ny, nz, L0.bm, s->bvel, U);
     } else {
-        k_from_rb<<<rgrid(n), 256, 0, cs>>>(c.g.st, L0, c.f.x[0], c.f.x[1], xout, &c.g.st->x_valid);
+        k_from_rb<<<rgrid(n), 256, 0, cs>>>(c.g.st, L0, c.f.x[0], c.f.x[1], xout, &c.g.st->x_valid, 0);
     }
 }
 
@@ -1652,7 +1752,7 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
                       const float* bvel, int precision) {
     if (!handle || !bt || nx < 2 || ny < 2 || nz < 2) return EDGE_EINVAL;
     if ((mask == nullptr) != (bvel == nullptr)) return EDGE_EINVAL;
-    if (precision != 0) return EDGE_EINVAL;
+    if (precision != 0 && precision != 1) return EDGE_EINVAL;
     long long n = (long long)nx * ny * nz;
     if (n * 3 >= (1LL << 31)) return EDGE_EINVAL;
     int L = 0;
@@ -1665,17 +1765,21 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     Ctx& c = s->ctx;
     memset(&c, 0, sizeof(c));
     c.lv.L = L;
+    c.zbf16 = precision == 1;
     for (int q = 0; q < 6; q++) c.g.bt[q] = bt[q];
     int r = EDGE_OK;
     for (int l = 0; l < L && r == EDGE_OK; l++) {
         Lvl& V = c.lv.lv[l];
         set_level_dims(V, nx >> l, ny >> l, nz >> l);
         size_t pa = plane_alloc(V.P);
-        r = alloc(s, (void**)&V.r[0], 2 * pa * sizeof(float));
-        if (r == EDGE_OK) r = alloc(s, (void**)&V.z[0], 2 * pa * sizeof(float));
-        if (r == EDGE_OK) r = cu(cudaMemset(V.z[0], 0, 2 * pa * sizeof(float)));
-        V.r[1] = V.r[0] + pa;
-        V.z[1] = V.z[0] + pa;
+        // level 0's r is the FP32 CG residual; the other level arrays are
+        // BF16 in the mixed-precision solver
+        const size_t esz = precision == 1 ? 2 : 4, esr = l == 0 ? 4 : esz;
+        r = alloc(s, (void**)&V.r[0], 2 * pa * esr);
+        if (r == EDGE_OK) r = alloc(s, (void**)&V.z[0], 2 * pa * esz);
+        if (r == EDGE_OK) r = cu(cudaMemset(V.z[0], 0, 2 * pa * esz));
+        V.r[1] = reinterpret_cast<float*>(reinterpret_cast<char*>(V.r[0]) + pa * esr);
+        V.z[1] = reinterpret_cast<float*>(reinterpret_cast<char*>(V.z[0]) + pa * esz);
         if (s->solid && r == EDGE_OK) {
             if (l == 0) V.bm = const_cast<int*>(mask);
             else r = alloc(s, (void**)&V.bm, (size_t)V.n0 * V.n1 * V.n2 * sizeof(int));
@@ -1803,7 +1907,15 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
     // outside a graph there is no loop condition to set
     c.g.use_cond = 0;
     enqueue_vcycle(c, s->solid, st, false);
-    k_from_rb<<<rgrid(n), 256, 0, st>>>(nullptr, L0, L0.z[0], L0.z[1], z, nullptr);
+    k_from_rb<<<rgrid(n), 256, 0, st>>>(nullptr, L0, L0.z[0], L0.z[1], z, nullptr, c.zbf16);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_apply_A_f64(void* handle, const double* p, double* Ap, void* stream) {
+    if (!handle || !p || !Ap) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& L = s->ctx.lv.lv[0];
+    k_apply_A64<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx.g, L, p, Ap);
     return cu(cudaPeekAtLastError());
 }
 
@@ -1824,7 +1936,7 @@ int edge_mgpcg_get(void* handle, int which, float* dst, void* stream) {
     if (which == 0) return cu(cudaMemcpyAsync(dst, s->ctx.f.div, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     if (which == 1) {
         k_from_rb<<<rgrid((long long)n), 256, 0, st>>>(nullptr, L, s->ctx.f.x[0], s->ctx.f.x[1], dst,
-                                                      &s->ctx.g.st->x_valid);
+                                                      &s->ctx.g.st->x_valid, 0);
         return cu(cudaPeekAtLastError());
     }
     return EDGE_EINVAL;

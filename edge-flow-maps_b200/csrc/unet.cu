@@ -729,18 +729,31 @@ __global__ void k_pack_weights(const float* __restrict__ w, int co, int ci, int 
     }
 }
 
-// the scale 1/rms(r) of the network input (one block, float64 sum)
-__global__ void __launch_bounds__(1024) k_input_scale(const float* __restrict__ r, long long n, float* scale) {
-    __shared__ double sm[32];
+// the scale 1/rms(r) of the network input: per-block float64 partial sums,
+// the last block to finish (arrival counter) adds them in block order
+__global__ void __launch_bounds__(256) k_input_scale(const float* __restrict__ r, long long n, double* partial,
+                                                     unsigned* counter, float* scale) {
+    __shared__ double sm[8];
+    __shared__ bool last;
     double s = 0.0;
-    for (long long e = threadIdx.x; e < n; e += blockDim.x) s += (double)r[e] * (double)r[e];
+    GSTRIDE(e, n) s += (double)r[e] * (double)r[e];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        double t = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if (threadIdx.x == 0) *scale = (float)(1.0 / sqrt(t / (double)n));
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += sm[w];
+        partial[blockIdx.x] = t;
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double t = 0.0;
+        for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(partial + b);
+        *scale = (float)(1.0 / sqrt(t / (double)n));
+        *counter = 0;
     }
 }
 
@@ -1001,9 +1014,13 @@ int edge_unet_pack_weights(const float* w, int cout, int cin, int transpose, voi
     return rc_last();
 }
 
-int edge_unet_input_scale(const float* r, long long n, float* scale, void* stream) {
-    if (!r || !scale || n <= 0) return EDGE_EINVAL;
-    k_input_scale<<<1, 1024, 0, (cudaStream_t)stream>>>(r, n, scale);
+int edge_unet_input_scale(const float* r, long long n, void* work, float* scale, void* stream) {
+    if (!r || !scale || !work || n <= 0) return EDGE_EINVAL;
+    // work: 1024 doubles of partial sums, then the arrival counter (zero on entry, reset on exit)
+    double* partial = (double*)work;
+    unsigned* counter = (unsigned*)(partial + 1024);
+    const int grid = (int)std::min<long long>(1024, std::max<long long>(1, (n + 255) / 256));
+    k_input_scale<<<grid, 256, 0, (cudaStream_t)stream>>>(r, n, partial, counter, scale);
     return rc_last();
 }
 

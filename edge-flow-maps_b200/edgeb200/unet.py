@@ -110,6 +110,7 @@ class UNet:
         self.a = {k: Act(self.lv[l], c) for k, (l, c) in FWD.items()}
         self.g = None
         self.scale = torch.zeros(1, device="cuda")
+        self.scale_work = torch.zeros(1026, dtype=torch.float64, device="cuda")
         self.err = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.z = torch.zeros(r0, device="cuda")
         self.packed = {}
@@ -146,7 +147,8 @@ class UNet:
         z = self.z if z is None else z
         a, p = self.a, self.params
         r0, r1, r2 = self.lv
-        N.call("edge_unet_input_scale", ptr(r), ctypes.c_longlong(r.numel()), ptr(self.scale), stream())
+        N.call("edge_unet_input_scale", ptr(r), ctypes.c_longlong(r.numel()), ptr_any(self.scale_work, F64),
+               ptr(self.scale), stream())
         N.call("edge_unet_conv_first", *r0, ptr(r), ptr(self.scale), ptr(self.packed["W0a"]), ptr(p["b0a"]),
                a["h0"].p, stream())
         self._conv(r0, a["h0"], "W0b", None, None, 16, p["b0b"], 1, a["e0"])
@@ -350,9 +352,11 @@ class LearnedPCG:
             torch.add(self.z0, self.v, out=z)
         z -= z.mean()
 
-    def solve(self, b, x, rel_tol=1e-6, max_iters=200, mode="warm"):
+    def solve(self, b, x, rel_tol=1e-6, max_iters=200, mode="warm", record=None):
         """x (zeroed here) solves A x = b - mean(b) to ||r|| <= rel_tol ||b||.
-        Returns (iterations, final relative residual, fell_back)."""
+        Returns (iterations, final relative residual, fell_back).  With a
+        list `record`, (r_k, x_k) of every iterate is appended to it (training
+        pairs: the correction of r_k is x_final - x_k)."""
         r = b - b.mean()
         x.zero_()
         bn = float(torch.linalg.vector_norm(r.double()))
@@ -367,6 +371,8 @@ class LearnedPCG:
         rn = bn
         it = 0
         while it < max_iters:
+            if record is not None:
+                record.append((r.clone(), x.clone()))
             self.P.apply_A(p, Ap)
             pAp = float(torch.dot(p.double().view(-1), Ap.double().view(-1)))
             if pAp <= 0.0:

@@ -219,6 +219,9 @@ int edge_mgpcg_result(void *handle, int *iters, double *rTr, int *status, void *
  * Ap = A p (compute_Ap, mgpcg.py:112-117), for testing. */
 int edge_mgpcg_vcycle(void *handle, const float *r, float *z, void *stream);
 int edge_mgpcg_apply_A(void *handle, const float *p, float *Ap, void *stream);
+/* The same operator in float64 (no reference counterpart): the FP64
+ * reference solve that the precision study measures errors against. */
+int edge_mgpcg_apply_A_f64(void *handle, const double *p, double *Ap, void *stream);
 /* Copy the divergence (u_div) or pressure (p) of the last Poisson call. */
 int edge_mgpcg_get(void *handle, int which, float *dst, void *stream);
 /* Number of multigrid levels (mgpcg.py:34). */
@@ -306,8 +309,10 @@ int edge_unet_up_bwd(int X, int Y, int Z, int channels, const void *dfine, void 
 /* float32 weights [cout][cin][27] -> packed bf16 [27][cin/8][cout][8]; with
  * transpose != 0 the data-gradient form [27][cout/8][cin][8] of w[co][ci][26-t]. */
 int edge_unet_pack_weights(const float *w, int cout, int cin, int transpose, void *out, void *stream);
-/* *scale = 1 / rms(r) over n values (the network's input normalisation). */
-int edge_unet_input_scale(const float *r, long long n, float *scale, void *stream);
+/* *scale = 1 / rms(r) over n values (the network's input normalisation).
+ * work: device scratch of 1024 doubles + 8 bytes, zeroed before its first use
+ * (the call leaves it ready for the next). */
+int edge_unet_input_scale(const float *r, long long n, void *work, float *scale, void *stream);
 /* Training loss on the scaled problem, d = (z - target) * scale:
  * stats[0] = mean(d), stats[1] = mean((d - mean d)^2); dzn = 2 (d - mean d) / n. */
 int edge_unet_loss(const float *z, const float *target, const float *scale, long long n, double *stats, float *dzn,

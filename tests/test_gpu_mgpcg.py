@@ -214,3 +214,33 @@ def test_poisson_with_buffer():
     for i in range(3):
         assert rel_l2(N_(f[i]), fo[i]) < 1e-4
         assert rel_l2(N_(u[i]), uo[i]) < 1e-4
+
+
+def test_mixed_precision_vs_fp64():
+    """BF16 V-cycle storage (precision=1): one V-cycle within bf16 rounding of
+    the float32 one, and solves to 1e-6 whose error against an FP64 solve is
+    of the float32 solver's size."""
+    from edgeb200.precision import fp64_solve, rel_error
+    from edgeb200.projection import Projection
+    res = (128, 64, 64)
+    g = torch.Generator().manual_seed(21)
+    b = torch.randn(res, generator=g)
+    b = (b - b.mean()).cuda()
+    P32 = Projection(res, base_level=1)
+    P16 = Projection(res, base_level=1, precision=1)
+    z32, z16 = torch.empty_like(b), torch.empty_like(b)
+    P32.vcycle(b, z32)
+    P16.vcycle(b, z16)
+    assert rel_l2(N_(z16), N_(z32)) < 3e-2
+    ref = fp64_solve(P32, b)
+    bb = float((b.double() ** 2).sum())
+    errs, its = [], []
+    for P in (P32, P16):
+        x = torch.zeros(res, device="cuda")
+        P.solve(b, x, abs_tol=1e-12 * bb, rel_tol=0.0)
+        it, rtr, st = P.result()
+        assert st == 0
+        its.append(it)
+        errs.append(rel_error(x, ref))
+    assert its[1] <= its[0] + 2
+    assert errs[0] < 1e-3 and errs[1] < 3 * errs[0] + 1e-6, errs

@@ -187,3 +187,17 @@ def test_training_reduces_loss():
     losses = [net.train_step(r, x, lr=3e-3).item() for _ in range(30)]
     assert not net.timed_out()
     assert losses[-1] < 0.8 * losses[0]
+
+
+def test_learned_preconditioner_gain():
+    """The shipped weights (trained on the GPU by edgeb200.train_unet from
+    plain-MGPCG solves at 128x64x64) warm-start the V-cycle well enough that
+    flexible CG needs fewer iterations to 1e-6 than with the plain V-cycle, on
+    right-hand sides it was not trained on."""
+    import os
+    from edgeb200 import unet as UN
+    from edgeb200.projection import Projection
+    from edgeb200.train_unet import evaluate, load_params
+    w = os.path.join(os.path.dirname(UN.__file__), "weights", "unet_pcg.npz")
+    out = evaluate(load_params(w), sizes=((128, 64, 64),), seeds=(1, 2, 3))["128x64x64"]
+    assert all(a < b for a, b in zip(out["warm"], out["vcycle"])), out
