@@ -309,7 +309,7 @@ PCG_REL = 1e-6
 # launches of that solve (4 CG iterations), one ncu capture of
 # `bench.py --pcg-only` with the host-driven solver loop (EDGE_MGPCG_EAGER=1);
 # ncu flushes the caches before every launch, so this is the cold-L2 figure
-PCG_TRAFFIC = 1498300672
+PCG_TRAFFIC = 1509646080
 
 
 def pcg_measure(res, reps=5):
@@ -440,6 +440,57 @@ def run_learned_only(args):
     return 0
 
 
+def c2_measure(steps=5, warm=3, per_cell=8):
+    """Configuration 2: solid wedge (chord 0.3, span 0.4, 20 degrees angle of
+    attack) in a uniform inflow u = (1, 0, 0) carried by the solid outer
+    shell, MGPCG_Solid_3 projection, dye emitters, and laden particles at
+    `per_cell` per fluid cell (jittered per octant, seed 0) two-way coupled
+    through the lp.py G2P/P2G kernels; EDGE at 256x128x128."""
+    import torch
+    from edgeb200.sim import EdgeSim, delta_emitters, uniform_flow, wedge_mask
+    res, dx = RES, DX
+    half = math.degrees(math.atan2(0.2, 0.3))
+    mask, bvel = wedge_mask(res, dx, apex=(0.5, 0.5, 0.45), chord=0.3, half_angle_deg=half, aoa_deg=20.0,
+                            thickness_cells=4, shell_vel=(1.0, 0.0, 0.0))
+    sim = EdgeSim(res, dx, variant="edge", cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * dx, base_level=BASE_LEVEL,
+                  bfecc_clamp=True, visualize_dt=1e9, solid=(mask, bvel),
+                  emitters=delta_emitters(offset=(0.5, 0.5, 0.47), half_angle_deg=half, radius=0.02), packed=True)
+    sim.set_velocity(*uniform_flow(res, (1.0, 0.0, 0.0)))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    fluid = torch.nonzero(mask.reshape(-1) <= 0).squeeze(1)
+    nf = fluid.numel()
+    cell = fluid.repeat_interleave(per_cell)
+    octant = torch.arange(per_cell, device="cuda").repeat(nf)
+    i = cell // (res[1] * res[2])
+    j = (cell // res[2]) % res[1]
+    k = cell % res[2]
+    base = torch.stack([i, j, k], 1).float()
+    sub = torch.stack([(octant >> 2) & 1, (octant >> 1) & 1, octant & 1], 1).float() * 0.5
+    pos = ((base + sub + torch.rand(base.shape, generator=g, device="cuda") * 0.5) * dx).contiguous()
+    vel = torch.zeros_like(pos)
+    rad = (0.001 + 0.002 * torch.rand(pos.shape[0], generator=g, device="cuda")).contiguous()
+    sim.add_particles(pos, vel, rad, tuple(n * dx for n in res), St=6.6e-2, gravity=0.0, density_ratio=2.0 / 3,
+                      epiral_radius_ratio=35.0, Re=5.5, laden_radius=0.01)
+    for _ in range(warm):
+        sim.step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sim.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    it, rtr, st = sim.proj.result()
+    out = {"workload": "solid wedge + laden particles 256x128x128, EDGE, MGPCG_Solid_3", "ms_per_step": ms,
+           "steps_per_s": 1e3 / ms, "particles": int(pos.shape[0]), "solid_cells": int((mask > 0).sum()),
+           "last_solve_iters": it, "last_solve_status": st}
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_pcg_only(args):
     import torch
     torch.cuda.set_device(0)
@@ -543,6 +594,7 @@ def run_ours(args, rank, world, local_rank):
                            "march_ms": round(vst.get("march_edge", 0.0), 4)}
             del vs
             torch.cuda.empty_cache()
+    c2 = c2_measure() if not (args.res or args.no_extras) else None
     pcg = pcg_measure(RES) if not (args.res or args.no_extras) else None
     if pcg is not None:
         pcg["learned"] = learned_measure(RES)
@@ -578,6 +630,7 @@ def run_ours(args, rank, world, local_rank):
             "roofline_fp32": march_roofline(stages, args.variant, fp32_peak, NC),
             "pcg": pcg,
             "variants": variants or None,
+            "c2_solid_particles": c2,
             "mgpcg_iters": list(iters),
             "clocks": clk.summary(),
             "gpu_launches": launches,
@@ -606,6 +659,7 @@ def main():
                     "(default: float4 planes)")
     ap.add_argument("--pcg-only", action="store_true", help="only the PCG-to-1e-6 measurement (profiling)")
     ap.add_argument("--learned-only", action="store_true", help="only the learned-preconditioner measurement")
+    ap.add_argument("--c2-only", action="store_true", help="only the solid + particle configuration")
     ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8 step timings")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the EDGE steps (no ED4/ED8, PCG or FP32-peak measurements; profiling)")
@@ -621,6 +675,11 @@ def main():
         return run_pcg_only(args)
     if args.learned_only:
         return run_learned_only(args)
+    if args.c2_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"c2_solid_particles": c2_measure()}), flush=True)
+        return 0
     return run_ours(args, rank, world, local_rank)
 
 

@@ -82,6 +82,7 @@ class EdgeSim:
             self.proj = Projection(r, base_level=base_level)
             self.max_iters = 400  # mgpcg.py:434-438
         self.emitters = emitters
+        self.side_stream = torch.cuda.Stream(device=device)
         self.particles = None
         self.i = -1
         self.sub_t = 0.0
@@ -183,8 +184,21 @@ class EdgeSim:
         tm.stop("pre-advect")
         self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
         tm.start("advect")
+        # The backward-map march and the forward-map march both read only the
+        # projected u: the forward map runs on a side stream next to the march
+        # (the march's register footprint leaves most warp slots free), and
+        # later the dye chain runs there next to the velocity chain.
+        main = torch.cuda.current_stream()
+        side = self.side_stream
+        ev = torch.cuda.Event()
+        ev.record(main)
+        with torch.cuda.stream(side):
+            side.wait_event(ev)
+            ops.advance_map(self.u, dx, curr_dt, self.phi, self.F)          # run_edge.py:660
+            ev_fwd = torch.cuda.Event()
+            ev_fwd.record(side)
         self._march(curr_dt, reinit)
-        ops.advance_map(self.u, dx, curr_dt, self.phi, self.F)          # run_edge.py:660
+        main.wait_event(ev_fwd)
         if self.particles is not None:
             # the forcing integrated into the map's origin velocity through the
             # forward map (run_edge.py:662-667)
@@ -197,15 +211,24 @@ class EdgeSim:
         else:
             m = self.maps[self.cur]
             ops.face_map(self.hv, dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"), self.fpsi, self.fcol)
-        # u = (grad psi)^T u_init(psi), smoke = smoke_init(psi)        run_edge.py:669-670
+        ev_map = torch.cuda.Event()
+        ev_map.record(main)
+        with torch.cuda.stream(side):
+            # dye: smoke = smoke_init(psi); err = 0.5*(smoke(phi) - smoke_init);
+            # smoke - err(psi), clamped                     run_edge.py:670, 677-689
+            side.wait_event(ev_map)
+            ops.pullback_dye(self.init_smoke, dx, self.fpsi, self.smoke)
+            ops.pullback_dye(self.smoke, dx, self.phi, self.err_smoke, init=self.init_smoke, scale=0.5)
+            ops.pullback_dye(self.err_smoke, dx, self.fpsi, self.smoke, sub=self.smoke, clampsrc=self.init_smoke)
+            ev_dye = torch.cuda.Event()
+            ev_dye.record(side)
+        # u = (grad psi)^T u_init(psi)                                 run_edge.py:669
         ops.pullback_u(self.init_u, dx, self.fpsi, self.fcol, self.u)
-        ops.pullback_dye(self.init_smoke, dx, self.fpsi, self.smoke)
-        # err = 0.5*(F^T u(phi) - u_init)                             run_edge.py:671-682
+        # err = 0.5*(F^T u(phi) - u_init)                             run_edge.py:671-676
         ops.pullback_u(self.u, dx, self.phi, self.F, self.err_u, init=self.init_u, scale=0.5)
-        ops.pullback_dye(self.smoke, dx, self.phi, self.err_smoke, init=self.init_smoke, scale=0.5)
-        # u - (grad psi)^T err(psi); smoke - err(psi), clamped           run_edge.py:683-689
+        # u - (grad psi)^T err(psi)                                    run_edge.py:683-686
         ops.pullback_u(self.err_u, dx, self.fpsi, self.fcol, self.tmp_u, sub=self.u)
-        ops.pullback_dye(self.err_smoke, dx, self.fpsi, self.smoke, sub=self.smoke, clampsrc=self.init_smoke)
+        main.wait_event(ev_dye)
         if self.bfecc_clamp:
             ops.clamp_u(self.tmp_u, self.u, self.tmp_u)                  # run_edge.py:690-696
         self.u, self.tmp_u = self.tmp_u, self.u
