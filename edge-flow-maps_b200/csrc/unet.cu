@@ -180,18 +180,12 @@ EDGE_D uint4 pack8(const float (&f)[8]) {
 // connection is a second input of the same convolution, not a concatenated
 // copy).  Weights are packed per input as [tap][Cin/8][Cout][8] bf16 (a
 // K-major B operand per tap).  One tile = 128 consecutive padded voxels (the
-// M rows), N = Cout, K = 16 channels per MMA; the A operand of tap (dx, dy,
-// dz) is the staged row of (dx, dy) shifted by dz voxels (16 bytes), so no
-// im2col copy exists.
-//
-// Pipeline: a CTA walks its tiles as a sequence of steps (input, dx, dy
-// group); each step stages its rows (and, when the weights do not stay
-// resident in shared memory, its taps' weights) into one of two buffers
-// while the tensor cores work on the previous step, one thread issues the
-// step's MMAs and commits them to that buffer's mbarrier.  Tiles alternate
-// between two TMEM accumulators, so the epilogue of tile t (TMEM -> bias,
-// ReLU -> bf16) overlaps the MMAs of tile t+1.  The data gradient is the same
-// kernel with transposed, tap-flipped weights.
+// M rows); for each input and each x-offset dx the CTA stages the three
+// dy-rows of 130 voxels (all channel chunks) and the nine taps' weights, and
+// one thread issues 9 taps x Cin/16 MMAs into the FP32 TMEM accumulator
+// (M = 128, N = Cout, K = 16 each); the A operand of tap (dy, dz) is the
+// staged row of dy shifted by dz voxels (16 bytes).  The data gradient is the
+// same kernel with transposed, tap-flipped weights.
 struct ConvIn {
     const __nv_bfloat16* x;
     const __nv_bfloat16* w;
@@ -201,80 +195,86 @@ struct ConvIn {
 constexpr int kSeg = 130;  // voxels staged per row (tile + 1 on each side)
 constexpr uint32_t kSegBytes = kSeg * 16;
 
-struct ConvPlan {
-    int resident;  // all weights stay in shared memory
-    int G;         // dy rows per step (3 or 1)
-    uint32_t wbytes;  // resident weight bytes (all inputs)
-    uint32_t bufbytes;  // one step buffer
-};
-
-inline ConvPlan plan_conv(int cin0, int cin1, int nin, int cout) {
-    ConvPlan p;
-    const int nchmax = std::max(cin0, nin > 1 ? cin1 : 0) / 8;
-    const uint32_t w = (uint32_t)(27 * cout * 16) * (uint32_t)(cin0 / 8 + (nin > 1 ? cin1 / 8 : 0));
-    const uint32_t seg3 = 3u * nchmax * kSegBytes;
-    if (w + 2 * seg3 <= 200 * 1024) {
-        p.resident = 1; p.G = 3; p.wbytes = w; p.bufbytes = seg3;
-    } else {
-        p.resident = 0; p.G = 1; p.wbytes = 0;
-        p.bufbytes = (uint32_t)nchmax * kSegBytes + 3u * nchmax * cout * 16;
-    }
-    return p;
-}
-
 template <int COUT>
-__global__ void __launch_bounds__(128) k_conv_tc(Geo g, ConvIn in0, ConvIn in1, int nin, ConvPlan plan,
-                                                 const float* __restrict__ bias, int flags,
-                                                 __nv_bfloat16* __restrict__ y, int* err) {
+__global__ void __launch_bounds__(128) k_conv_tc(Geo g, ConvIn in0, ConvIn in1, int nin, const float* __restrict__ bias,
+                                                 int flags, __nv_bfloat16* __restrict__ y, int* err) {
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tslot;
-    constexpr uint32_t NCOLS = 2 * COUT < 32 ? 32 : 2 * COUT;
+    constexpr uint32_t NCOLS = COUT < 32 ? 32 : COUT;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nchmax = max(in0.cin, nin > 1 ? in1.cin : 0) / 8;
-    const int G = plan.G, groups = 3 / G, spi = 3 * groups;  // steps per input
-    const int nphase = nin * spi;
-    uint8_t* sW = smem;                   // resident weights (input 0, then input 1)
-    uint8_t* sbuf = smem + plan.wbytes;   // two step buffers
-    const uint32_t segarea = (uint32_t)G * nchmax * kSegBytes;  // rows of a step; its weights follow
+    uint8_t* sseg = smem;
+    uint8_t* sw = smem + (size_t)3 * nchmax * kSegBytes;
     if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), NCOLS);
-    if (tid == 0) {
-        tc::mbar_init(tc::smem_u32(&mbar[0]), 1);
-        tc::mbar_init(tc::smem_u32(&mbar[1]), 1);
-    }
-    if (plan.resident) {
-        const uint32_t n0 = 27u * (in0.cin / 8) * COUT;  // uint4 per input
-        for (uint32_t e = tid; e < n0; e += blockDim.x)
-            reinterpret_cast<uint4*>(sW)[e] = reinterpret_cast<const uint4*>(in0.w)[e];
-        if (nin > 1) {
-            const uint32_t n1 = 27u * (in1.cin / 8) * COUT;
-            for (uint32_t e = tid; e < n1; e += blockDim.x)
-                reinterpret_cast<uint4*>(sW)[n0 + e] = reinterpret_cast<const uint4*>(in1.w)[e];
-        }
-    }
-    tc::fence_smem_to_async();
+    if (tid == 0) tc::mbar_init(tc::smem_u32(&mbar), 1);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = tslot;
     const uint32_t idesc = tc::idesc_bf16(128, COUT, false, false);
-    const int my_tiles = blockIdx.x < g.ntiles ? (g.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    const long long nsteps = (long long)my_tiles * nphase;
+    uint32_t parity = 0;
     bool bad = false;
-    long long last_issued = -1;
-    auto wait_step = [&](long long st) -> bool {
-        return tc::mbar_wait(tc::smem_u32(&mbar[st & 1]), (uint32_t)((st >> 1) & 1), kMaxPolls);
-    };
-    auto epilogue = [&](int tl) {
-        const int tile = blockIdx.x + tl * gridDim.x;
-        const int v = tile * 128 + 32 * warp + lane;
+    for (int tile = blockIdx.x; tile < g.ntiles && !bad; tile += gridDim.x) {
+        const int v0 = tile * 128;
+        int nmma = 0;
+        bool pending = false;
+        for (int i = 0; i < nin && !bad; i++) {
+            const ConvIn in = i ? in1 : in0;
+            const int nch = in.cin / 8;
+            for (int dxi = 0; dxi < 3 && !bad; dxi++) {
+                if (pending) {  // the previous phase's MMAs still read shared memory
+                    bool ok = tc::mbar_wait(tc::smem_u32(&mbar), parity, kMaxPolls);
+                    parity ^= 1;
+                    pending = false;
+                    if (__syncthreads_or(!ok)) { bad = true; break; }
+                }
+                const long long base = (long long)v0 + (dxi - 1) * (long long)g.Sx - g.Sy - 1;
+                for (int e = tid; e < 3 * nch * kSeg; e += blockDim.x) {
+                    const int dyi = e / (nch * kSeg), rem = e - dyi * nch * kSeg;
+                    const int q = rem / kSeg, s = rem - q * kSeg;
+                    const long long v = base + (long long)dyi * g.Sy + s;
+                    const uint4 val = *reinterpret_cast<const uint4*>(in.x + act_off(g, q, v));
+                    *reinterpret_cast<uint4*>(sseg + ((size_t)(dyi * nch + q) * kSeg + s) * 16) = val;
+                }
+                const uint4* wsrc = reinterpret_cast<const uint4*>(in.w) + (size_t)dxi * 9 * nch * COUT;
+                for (int e = tid; e < 9 * nch * COUT; e += blockDim.x) reinterpret_cast<uint4*>(sw)[e] = wsrc[e];
+                tc::fence_smem_to_async();
+                tc::fence_before_sync();
+                __syncthreads();
+                tc::fence_after_sync();
+                if (tid == 0) {
+                    const uint32_t a0 = tc::smem_u32(sseg), b0 = tc::smem_u32(sw);
+                    for (int dyi = 0; dyi < 3; dyi++)
+                        for (int dzi = 0; dzi < 3; dzi++)
+                            for (int ks = 0; ks < nch / 2; ks++) {
+                                const uint64_t da = tc::sdesc(
+                                    a0 + (uint32_t)((dyi * nch + 2 * ks) * kSegBytes + dzi * 16), kSegBytes, 128);
+                                const uint64_t db = tc::sdesc(
+                                    b0 + (uint32_t)(((dyi * 3 + dzi) * nch + 2 * ks) * COUT * 16), COUT * 16, 128);
+                                tc::mma_bf16(tbase, da, db, idesc, nmma > 0 ? 1u : 0u);
+                                nmma++;
+                            }
+                    tc::commit(tc::smem_u32(&mbar));
+                }
+                pending = true;
+            }
+        }
+        if (bad) break;
+        {
+            bool ok = tc::mbar_wait(tc::smem_u32(&mbar), parity, kMaxPolls);
+            parity ^= 1;
+            if (__syncthreads_or(!ok)) { bad = true; break; }
+        }
+        tc::fence_after_sync();
+        // epilogue: this thread's voxel, all output channels
+        const int v = v0 + 32 * warp + lane;
         int x, yy, z;
         const bool in_dom = interior(g, v, x, yy, z);
-        const uint32_t acc_col = (uint32_t)((tl & 1) * COUT);
 #pragma unroll
         for (int c0 = 0; c0 < COUT; c0 += 16) {
             float acc[16];
-            tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + acc_col + (uint32_t)c0, acc);
+            tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 uint4* dst = reinterpret_cast<uint4*>(y + act_off(g, (c0 >> 3) + h, v));
@@ -291,73 +291,12 @@ __global__ void __launch_bounds__(128) k_conv_tc(Geo g, ConvIn in0, ConvIn in1, 
             }
         }
         tc::fence_before_sync();
-    };
-    for (long long st = 0; st < nsteps && !bad; st++) {
-        const int tl = (int)(st / nphase), ph = (int)(st % nphase);
-        const int i = ph / spi, rem = ph % spi, dxi = rem / groups, dyg = rem % groups;
-        const ConvIn in = i ? in1 : in0;
-        const int nch = in.cin / 8;
-        const int v0 = (blockIdx.x + tl * gridDim.x) * 128;
-        uint8_t* buf = sbuf + (size_t)(st & 1) * plan.bufbytes;
-        if (st >= 2) {  // the MMAs of step st-2 read this buffer
-            const bool ok = wait_step(st - 2);
-            if (__syncthreads_or(!ok)) { bad = true; break; }
-        }
-        for (int e = tid; e < G * nch * kSeg; e += blockDim.x) {
-            const int dyl = e / (nch * kSeg), r2 = e - dyl * nch * kSeg;
-            const int q = r2 / kSeg, s = r2 - q * kSeg;
-            const int dyi = dyg * G + dyl;
-            const long long v = (long long)v0 + (dxi - 1) * (long long)g.Sx + (dyi - 1) * (long long)g.Sy - 1 + s;
-            *reinterpret_cast<uint4*>(buf + ((size_t)(dyl * nch + q) * kSeg + s) * 16) =
-                *reinterpret_cast<const uint4*>(in.x + act_off(g, q, v));
-        }
-        if (!plan.resident) {
-            const uint4* wsrc = reinterpret_cast<const uint4*>(in.w) + (size_t)(dxi * 9 + dyg * G * 3) * nch * COUT;
-            for (int e = tid; e < G * 3 * nch * COUT; e += blockDim.x)
-                reinterpret_cast<uint4*>(buf + segarea)[e] = wsrc[e];
-        }
-        tc::fence_smem_to_async();
-        tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
-        if (tid == 0) {
-            const uint32_t a0 = tc::smem_u32(buf);
-            const uint32_t wres = tc::smem_u32(sW) + (i ? 27u * (in0.cin / 8) * COUT * 16 : 0u);
-            const uint32_t wbuf = tc::smem_u32(buf + segarea);
-            const uint32_t acc = tbase + (uint32_t)((tl & 1) * COUT);
-            for (int dyl = 0; dyl < G; dyl++)
-                for (int dzi = 0; dzi < 3; dzi++)
-                    for (int ks = 0; ks < nch / 2; ks++) {
-                        const int dyi = dyg * G + dyl;
-                        const uint64_t da = tc::sdesc(
-                            a0 + (uint32_t)((dyl * nch + 2 * ks) * kSegBytes + dzi * 16), kSegBytes, 128);
-                        const uint32_t bw = plan.resident
-                                                ? wres + (uint32_t)(((dxi * 9 + dyi * 3 + dzi) * nch + 2 * ks) * COUT * 16)
-                                                : wbuf + (uint32_t)(((dyl * 3 + dzi) * nch + 2 * ks) * COUT * 16);
-                        const uint64_t db = tc::sdesc(bw, COUT * 16, 128);
-                        tc::mma_bf16(acc, da, db, idesc, (ph > 0 || dyl > 0 || dzi > 0 || ks > 0) ? 1u : 0u);
-                    }
-            tc::commit(tc::smem_u32(&mbar[st & 1]));
-        }
-        last_issued = st;
-        if (ph == 0 && tl >= 1) {  // the previous tile's last step: its MMAs done -> its epilogue
-            const bool ok = wait_step(st - 1);
-            if (__syncthreads_or(!ok)) { bad = true; break; }
-            tc::fence_after_sync();
-            epilogue(tl - 1);
-        }
-    }
-    if (!bad && nsteps > 0) {
-        const bool ok = wait_step(nsteps - 1);
-        if (__syncthreads_or(!ok)) bad = true;
-        else {
-            tc::fence_after_sync();
-            epilogue(my_tiles - 1);
-        }
     }
     if (bad) {
         if (tid == 0) atomicExch(err, 1);
-        if (last_issued >= 0) wait_step(last_issued);  // outstanding MMAs finish before TMEM is freed
+        tc::mbar_wait(tc::smem_u32(&mbar), parity, kMaxPolls);  // outstanding MMAs finish before TMEM is freed
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -894,15 +833,14 @@ inline int rc_last() {
 template <int COUT>
 int launch_conv(const Geo& g, ConvIn a, ConvIn b, int nin, const float* bias, int flags, __nv_bfloat16* y, int* err,
                 cudaStream_t st) {
-    const ConvPlan plan = plan_conv(a.cin, b.cin, nin, COUT);
-    const size_t smem = (size_t)plan.wbytes + 2 * (size_t)plan.bufbytes;
-    if (smem > 210 * 1024) return EDGE_EINVAL;
+    const int nchmax = std::max(a.cin, nin > 1 ? b.cin : 0) / 8;
+    const size_t smem = (size_t)3 * nchmax * kSegBytes + (size_t)9 * nchmax * COUT * 16;
+    if (smem > 200 * 1024) return EDGE_EINVAL;
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    const int ncols = 2 * COUT < 32 ? 32 : 2 * COUT;
-    int per_sm = (int)std::max<size_t>(1, std::min<size_t>(220 * 1024 / (smem + 1024), 512 / ncols));
+    int per_sm = (int)std::max<size_t>(1, std::min<size_t>(200 * 1024 / smem, 512 / (COUT < 32 ? 32 : COUT)));
     int grid = std::min(g.ntiles, g_sms() * per_sm);
-    k_conv_tc<COUT><<<grid, 128, smem, st>>>(g, a, b, nin, plan, bias, flags, y, err);
+    k_conv_tc<COUT><<<grid, 128, smem, st>>>(g, a, b, nin, bias, flags, y, err);
     return rc_last();
 }
 
