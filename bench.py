@@ -369,8 +369,10 @@ def pcg_measure(res, reps=5):
 
 
 # FLOPs per cell of the marches, counted from the reference's arithmetic
-# (EDGE: 5 trajectories x (RK4 with Jacobian + Hermite value/gradient))
-MARCH_FLOP_PER_CELL = {"edge": 27400, "ed4": 8400, "ed8": 16800}
+# (EDGE: 5 trajectories x (RK4 with Jacobian + Hermite value/gradient); GE: one
+# trajectory with Jacobian, 3 full Hermite value/gradient, 3x3 compose and the
+# grid differences of calc_fd_3_from_grad)
+MARCH_FLOP_PER_CELL = {"edge": 27400, "ed4": 8400, "ed8": 16800, "ge": 5500}
 
 
 def march_roofline(stages, variant, peak_tflops, ncells):
@@ -509,6 +511,7 @@ def run_ours(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     from edgeb200 import ops
     sim = make_sim(args.variant, args.res, packed=not args.unpacked)
+    mg_levels = sim.proj.levels
     if args.res and tuple(args.res) != RES:
         args.no_cpu_baseline = True  # profiling runs on a smaller grid
     for _ in range(args.warmup):
@@ -569,15 +572,16 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "1 full substep of the same workload (first step after reinit), C/OpenMP restatement "
                          "of the reference kernels"}
-    # ED4 / ED8 steps of the same workload (a few steps each, outside the
+    # ED4 / ED8 / GE steps of the same workload (a few steps each, outside the
     # timed region of the EDGE line)
     variants = {}
+    fp32_peak = ops.fma_peak_tflops() if not args.no_extras else None
     if args.no_extras:
         args.no_variants = True
     if not args.no_variants and args.variant == "edge" and not args.res:
         del sim
         torch.cuda.empty_cache()
-        for v in ("ed4", "ed8"):
+        for v in ("ed4", "ed8", "ge"):
             vs = make_sim(v, args.res, packed=not args.unpacked)
             for _ in range(3):
                 vs.step()
@@ -591,14 +595,14 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.synchronize()
             vst, _ = instrumented_step(vs)
             variants[v] = {"ms_per_step": a0.elapsed_time(a1) / 6, "steps_per_s": 6e3 / a0.elapsed_time(a1),
-                           "march_ms": round(vst.get("march_edge", 0.0), 4)}
+                           "march_ms": round(vst.get("march_edge", 0.0), 4),
+                           "march_roofline_fp32": march_roofline(vst, v, fp32_peak, NC)}
             del vs
             torch.cuda.empty_cache()
     c2 = c2_measure() if not (args.res or args.no_extras) else None
     pcg = pcg_measure(RES) if not (args.res or args.no_extras) else None
     if pcg is not None:
         pcg["learned"] = learned_measure(RES)
-    fp32_peak = ops.fma_peak_tflops() if not args.no_extras else None
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -614,12 +618,18 @@ def run_ours(args, rank, world, local_rank):
             it2 = max(iters[1], 0) + 1
             mg_bytes = MG_SETUP_BYTES + it2 * MG_ITER_BYTES
         achieved = mg_bytes / (solve_ms * 1e-3) / 1e9 if solve_ms > 0 else None
+        # the headline workload unless --res / --variant ask for another one
+        run_res = tuple(args.res) if args.res else RES
+        grid = "x".join(map(str, run_res))
+        metric = METRIC if (run_res == RES and args.variant == "edge") else \
+            f"{args.variant.upper()} steps/s at {grid}"
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded four-vortex rings, init_four_vorts geometry)",
-            "config": {"workload": "four-vortex collision 256x128x128, EDGE, CFL 0.5, reinit 12, 6-level MGPCG, "
-                                   "BFECC clamp", "res": list(RES), "variant": args.variant,
+            "config": {"workload": f"four-vortex collision {grid}, {args.variant.upper()}, CFL 0.5, reinit 12, "
+                                   f"{mg_levels}-level MGPCG, BFECC clamp", "res": list(run_res),
+                       "variant": args.variant,
                        "parallelism": f"replicas x{world}", "l2": "step working set ~1.7 GB > L2 (no flush needed)"},
             "roofline": {"kernel": roof_kernel, "bound": "hbm",
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -627,7 +637,7 @@ def run_ours(args, rank, world, local_rank):
                          "traffic": PCG_TRAFFIC if pcg else None,
                          "algorithmic_bytes": mg_bytes, "iterations": it2, "peak_source": src},
             "stages_ms": {k: round(v, 4) for k, v in stages.items()},
-            "roofline_fp32": march_roofline(stages, args.variant, fp32_peak, NC),
+            "roofline_fp32": march_roofline(stages, args.variant, fp32_peak, math.prod(run_res)),
             "pcg": pcg,
             "variants": variants or None,
             "c2_solid_particles": c2,
@@ -651,7 +661,7 @@ def main():
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="edge", choices=["edge", "ed4", "ed8"])
+    ap.add_argument("--variant", default="edge", choices=["edge", "ed4", "ed8", "ge"])
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=2)
@@ -660,7 +670,7 @@ def main():
     ap.add_argument("--pcg-only", action="store_true", help="only the PCG-to-1e-6 measurement (profiling)")
     ap.add_argument("--learned-only", action="store_true", help="only the learned-preconditioner measurement")
     ap.add_argument("--c2-only", action="store_true", help="only the solid + particle configuration")
-    ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8 step timings")
+    ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8/GE step timings")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the EDGE steps (no ED4/ED8, PCG or FP32-peak measurements; profiling)")
     ap.add_argument("--res", type=int, nargs=3, default=None,

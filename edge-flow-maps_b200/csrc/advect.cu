@@ -317,6 +317,146 @@ __global__ void __launch_bounds__(128) k_march_ed8_p(Mac mac, MapP m, float dt, 
     for (int q = 0; q < 8; q++) out[(size_t)q * n + e] = make_float4(o[q][0], o[q][1], o[q][2], 0.f);
 }
 
+// GE march (hermite.py:1398-1424 advect_ps_garm up to its copies): the cell
+// centre is marched back by RK4 with its Jacobian from the identity
+// (hermite.py:643-654, 864-918 with -dt) and composed with the accumulated
+// map through the full stored-derivative Hermite (hermite.py:1024-1046).
+// dT and d2T of the new map come from calc_fd_3_from_grad afterwards.
+EDGE_D void herm_full(const MapF& m, const float p[3], float v[3], float g[3][3]) { hermite3<HV_FULL, true>(m, p, v, g); }
+EDGE_D void herm_full(const MapP& m, const float p[3], float v[3], float g[3][3]) { hermite3p<HV_FULL, true>(m, p, v, g); }
+
+template <class M>
+EDGE_D void ge_center(const Mac& mac, const M& m, int e, float dt, float P[3], float T[3][3]) {
+    int k = e % m.nz, j = (e / m.nz) % m.ny, i = e / (m.ny * m.nz);
+    cell_pos(i, j, k, m.dx, P);
+    float C[3][3];
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) C[c][d] = c == d ? 1.0f : 0.0f;
+    rk4_jac<3>(mac, P, C, -dt);
+    float val[3], G[3][3];
+    herm_full(m, P, val, G);
+    // T = T_old @ T_step with T_step[a][d] = C[d][a]
+    for (int r = 0; r < 3; r++)
+        for (int d = 0; d < 3; d++) T[r][d] = G[r][0] * C[d][0] + G[r][1] * C[d][1] + G[r][2] * C[d][2];
+    for (int c = 0; c < 3; c++) P[c] = val[c];
+}
+
+__global__ void __launch_bounds__(128) k_march_ge(Mac mac, MapF m, float dt, float* __restrict__ opsi,
+                                                  float* __restrict__ oTx, float* __restrict__ oTy,
+                                                  float* __restrict__ oTz) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.nx * m.ny * m.nz) return;
+    float P[3], T[3][3];
+    ge_center(mac, m, e, dt, P, T);
+    float* oT[3] = {oTx, oTy, oTz};
+    for (int c = 0; c < 3; c++) {
+        opsi[3 * e + c] = P[c];
+        for (int d = 0; d < 3; d++) oT[c][3 * e + d] = T[c][d];
+    }
+}
+
+// packed layout: planes 0-3 of `out`
+__global__ void __launch_bounds__(128) k_march_ge_p(Mac mac, MapP m, float dt, float4* __restrict__ out) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = m.n;
+    if (e >= n) return;
+    float P[3], T[3][3];
+    ge_center(mac, m, e, dt, P, T);
+    out[e] = make_float4(P[0], P[1], P[2], 0.f);
+#pragma unroll
+    for (int d = 0; d < 3; d++) out[(size_t)(1 + d) * n + e] = make_float4(T[0][d], T[1][d], T[2][d], 0.f);
+}
+
+// calc_fd_3_from_grad (hermite.py:1180-1256), first loops: dT_c from central
+// differences of the gradient row T_c, neighbour index clamped to the grid.
+// One thread per cell and component.
+__global__ void k_fd3_dT(int nx, int ny, int nz, float dx, const float* __restrict__ Tx,
+                         const float* __restrict__ Ty, const float* __restrict__ Tz, float* dTx, float* dTy,
+                         float* dTz) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = nx * ny * nz;
+    if (t >= 3LL * n) return;
+    const int c = (int)(t / n), e = (int)(t - (long long)c * n);
+    const float* T = c == 0 ? Tx : (c == 1 ? Ty : Tz);
+    float* o = c == 0 ? dTx : (c == 1 ? dTy : dTz);
+    const int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
+    const int ip = min(i + 1, nx - 1), im = max(i - 1, 0), jp = min(j + 1, ny - 1), jm = max(j - 1, 0);
+    const int kp = min(k + 1, nz - 1), km = max(k - 1, 0);
+    const float* Tkp = T + 3 * idx3(i, j, kp, ny, nz);
+    const float* Tkm = T + 3 * idx3(i, j, km, ny, nz);
+    const float* Tjp = T + 3 * idx3(i, jp, k, ny, nz);
+    const float* Tjm = T + 3 * idx3(i, jm, k, ny, nz);
+    const float* Tip = T + 3 * idx3(ip, j, k, ny, nz);
+    const float* Tim = T + 3 * idx3(im, j, k, ny, nz);
+    o[3 * e + 0] = ((__ldg(Tkp + 1) - __ldg(Tkm + 1)) + (__ldg(Tjp + 2) - __ldg(Tjm + 2))) / 4.0f / dx;
+    o[3 * e + 1] = ((__ldg(Tkp + 0) - __ldg(Tkm + 0)) + (__ldg(Tip + 2) - __ldg(Tim + 2))) / 4.0f / dx;
+    o[3 * e + 2] = ((__ldg(Tjp + 0) - __ldg(Tjm + 0)) + (__ldg(Tip + 1) - __ldg(Tim + 1))) / 4.0f / dx;
+}
+
+// calc_fd_3_from_grad, last loops: d2T_c from central differences of dT_c.
+__global__ void k_fd3_d2T(int nx, int ny, int nz, float dx, const float* __restrict__ dTx,
+                          const float* __restrict__ dTy, const float* __restrict__ dTz, float* d2Tx, float* d2Ty,
+                          float* d2Tz) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = nx * ny * nz;
+    if (t >= 3LL * n) return;
+    const int c = (int)(t / n), e = (int)(t - (long long)c * n);
+    const float* D = c == 0 ? dTx : (c == 1 ? dTy : dTz);
+    float* o = c == 0 ? d2Tx : (c == 1 ? d2Ty : d2Tz);
+    const int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
+    const int ip = min(i + 1, nx - 1), im = max(i - 1, 0), jp = min(j + 1, ny - 1), jm = max(j - 1, 0);
+    const int kp = min(k + 1, nz - 1), km = max(k - 1, 0);
+    o[e] = ((__ldg(D + 3 * idx3(ip, j, k, ny, nz)) - __ldg(D + 3 * idx3(im, j, k, ny, nz))) +
+            (__ldg(D + 3 * idx3(i, jp, k, ny, nz) + 1) - __ldg(D + 3 * idx3(i, jm, k, ny, nz) + 1)) +
+            (__ldg(D + 3 * idx3(i, j, kp, ny, nz) + 2) - __ldg(D + 3 * idx3(i, j, km, ny, nz) + 2))) /
+           6.0f / dx;
+}
+
+// The same two passes on the packed planes: plane 1+d holds column d of the
+// gradient (component c = psi_c,d), plane 4+d the mixed derivative dT_c[d]
+// and plane 7 d2T_c, so every difference runs on the three components at once.
+EDGE_D float4 f4sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, 0.f); }
+EDGE_D float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, 0.f); }
+EDGE_D float4 f4div(float4 a, float s, float dx) {
+    return make_float4(a.x / s / dx, a.y / s / dx, a.z / s / dx, 0.f);
+}
+
+__global__ void k_fd3_dT_p(int nx, int ny, int nz, float dx, float4* __restrict__ g) {
+    const int n = nx * ny * nz;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
+    const int ekp = idx3(i, j, min(k + 1, nz - 1), ny, nz), ekm = idx3(i, j, max(k - 1, 0), ny, nz);
+    const int ejp = idx3(i, min(j + 1, ny - 1), k, ny, nz), ejm = idx3(i, max(j - 1, 0), k, ny, nz);
+    const int eip = idx3(min(i + 1, nx - 1), j, k, ny, nz), eim = idx3(max(i - 1, 0), j, k, ny, nz);
+    const float4* P1 = g + (size_t)1 * n;
+    const float4* P2 = g + (size_t)2 * n;
+    const float4* P3 = g + (size_t)3 * n;
+    float4 yz = f4add(f4sub(__ldg(P2 + ekp), __ldg(P2 + ekm)), f4sub(__ldg(P3 + ejp), __ldg(P3 + ejm)));
+    float4 xz = f4add(f4sub(__ldg(P1 + ekp), __ldg(P1 + ekm)), f4sub(__ldg(P3 + eip), __ldg(P3 + eim)));
+    float4 xy = f4add(f4sub(__ldg(P1 + ejp), __ldg(P1 + ejm)), f4sub(__ldg(P2 + eip), __ldg(P2 + eim)));
+    g[(size_t)4 * n + e] = f4div(yz, 4.0f, dx);
+    g[(size_t)5 * n + e] = f4div(xz, 4.0f, dx);
+    g[(size_t)6 * n + e] = f4div(xy, 4.0f, dx);
+}
+
+__global__ void k_fd3_d2T_p(int nx, int ny, int nz, float dx, float4* __restrict__ g) {
+    const int n = nx * ny * nz;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int k = e % nz, j = (e / nz) % ny, i = e / (ny * nz);
+    const float4* P4 = g + (size_t)4 * n;
+    const float4* P5 = g + (size_t)5 * n;
+    const float4* P6 = g + (size_t)6 * n;
+    float4 s = f4add(f4add(f4sub(__ldg(P4 + idx3(min(i + 1, nx - 1), j, k, ny, nz)),
+                                 __ldg(P4 + idx3(max(i - 1, 0), j, k, ny, nz))),
+                           f4sub(__ldg(P5 + idx3(i, min(j + 1, ny - 1), k, ny, nz)),
+                                 __ldg(P5 + idx3(i, max(j - 1, 0), k, ny, nz)))),
+                     f4sub(__ldg(P6 + idx3(i, j, min(k + 1, nz - 1), ny, nz)),
+                           __ldg(P6 + idx3(i, j, max(k - 1, 0), ny, nz))));
+    g[(size_t)7 * n + e] = f4div(s, 6.0f, dx);
+}
+
 // face map on the packed layout
 template <int V>
 __global__ void __launch_bounds__(128) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
@@ -901,6 +1041,52 @@ int edge_march_ed8(int nx, int ny, int nz, float dx, float dt, float epsilon, co
     int n = nx * ny * nz;
     k_march_ed8<<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, epsilon, opsi,
                                                         oTx, oTy, oTz, odTx, odTy, odTz, od2Tx, od2Ty, od2Tz);
+    return launch_status();
+}
+
+int edge_calc_fd_3_from_grad(int nx, int ny, int nz, float dx, const float* Tx, const float* Ty, const float* Tz,
+                             float* dTx, float* dTy, float* dTz, float* d2Tx, float* d2Ty, float* d2Tz, void* stream) {
+    if (!dims_ok(nx, ny, nz) || !Tx || !Ty || !Tz || !dTx || !dTy || !dTz || !d2Tx || !d2Ty || !d2Tz)
+        return EDGE_EINVAL;
+    if (dTx == Tx || dTy == Ty || dTz == Tz) return EDGE_EINVAL;
+    long long n3 = 3LL * nx * ny * nz;
+    k_fd3_dT<<<grid_for(n3), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, Tx, Ty, Tz, dTx, dTy, dTz);
+    k_fd3_d2T<<<grid_for(n3), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, dTx, dTy, dTz, d2Tx, d2Ty, d2Tz);
+    return launch_status();
+}
+
+int edge_march_ge(int nx, int ny, int nz, float dx, float dt, const float* ux, const float* uy, const float* uz,
+                  const float* psi, const float* Tx, const float* Ty, const float* Tz, const float* dTx,
+                  const float* dTy, const float* dTz, const float* d2Tx, const float* d2Ty, const float* d2Tz,
+                  float* opsi, float* oTx, float* oTy, float* oTz, float* odTx, float* odTy, float* odTz,
+                  float* od2Tx, float* od2Ty, float* od2Tz, void* stream) {
+    if (!dims_ok(nx, ny, nz) || !ux || !uy || !uz || !psi || !Tx || !Ty || !Tz || !dTx || !dTy || !dTz || !d2Tx ||
+        !d2Ty || !d2Tz || !opsi || !oTx || !oTy || !oTz || !odTx || !odTy || !odTz || !od2Tx || !od2Ty || !od2Tz)
+        return EDGE_EINVAL;
+    if (opsi == psi || oTx == Tx || odTx == dTx || od2Tx == d2Tx) return EDGE_EINVAL;
+    const float* T[3] = {Tx, Ty, Tz};
+    const float* dT[3] = {dTx, dTy, dTz};
+    const float* d2T[3] = {d2Tx, d2Ty, d2Tz};
+    MapF m = make_map(psi, T, dT, d2T, nx, ny, nz, dx);
+    int n = nx * ny * nz;
+    k_march_ge<<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, opsi, oTx, oTy,
+                                                       oTz);
+    int rc = launch_status();
+    if (rc) return rc;
+    return edge_calc_fd_3_from_grad(nx, ny, nz, dx, oTx, oTy, oTz, odTx, odTy, odTz, od2Tx, od2Ty, od2Tz, stream);
+}
+
+int edge_march_ge_packed(int nx, int ny, int nz, float dx, float dt, const float* ux, const float* uy,
+                         const float* uz, const float* in_packed, float* out_packed, void* stream) {
+    if (!dims_ok(nx, ny, nz) || !ux || !uy || !uz || !in_packed || !out_packed) return EDGE_EINVAL;
+    if (in_packed == out_packed) return EDGE_EINVAL;
+    if (!al16(in_packed) || !al16(out_packed)) return EDGE_EALIGN;
+    MapP m = make_mapp(in_packed, nx, ny, nz, dx);
+    int n = nx * ny * nz;
+    float4* o = (float4*)out_packed;
+    k_march_ge_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, o);
+    k_fd3_dT_p<<<grid_for(n), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, o);
+    k_fd3_d2T_p<<<grid_for(n), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, o);
     return launch_status();
 }
 

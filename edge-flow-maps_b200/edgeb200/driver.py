@@ -1,4 +1,4 @@
-"""Shared body of the run_edge.py / run_ed4.py / run_ed8.py drop-in drivers:
+"""Shared body of the run_edge.py / run_ed4.py / run_ed8.py / run_ge.py drop-in drivers:
 the reference's per-case configuration and its frame loop (run_edge.py:17-145,
 522-746) around the device substep ``EdgeSim.step``.
 

@@ -15,7 +15,8 @@ from .fields import NULL, cell_dims, dims_from_faces, ptr, stream
 F = ctypes.c_float
 
 # kernels each entry point launches (memcpy/memset nodes are not counted)
-_KERNELS = {"edge_max_speed": 2, "edge_copy": 0, "edge_lp_max_speed": 2}
+_KERNELS = {"edge_max_speed": 2, "edge_copy": 0, "edge_lp_max_speed": 2, "edge_march_ge": 3,
+            "edge_march_ge_packed": 3, "edge_calc_fd_3_from_grad": 2}
 _launched = [0]
 
 
@@ -94,6 +95,17 @@ def march_ed8(u, dx, dt, eps, psi, T, dT, d2T, opsi, oT, odT, od2T):
            ptr(opsi), *_p3(oT), *_p3(odT), *_p3(od2T), stream())
 
 
+def march_ge(u, dx, dt, psi, T, dT, d2T, opsi, oT, odT, od2T):
+    nx, ny, nz = cell_dims(opsi)
+    _call("edge_march_ge", nx, ny, nz, F(dx), F(dt), *_p3(u), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), ptr(opsi),
+          *_p3(oT), *_p3(odT), *_p3(od2T), stream())
+
+
+def calc_fd_3_from_grad(dx, T, dT, d2T):
+    nx, ny, nz = cell_dims(T[0])
+    _call("edge_calc_fd_3_from_grad", nx, ny, nz, F(dx), *_p3(T), *_p3(dT), *_p3(d2T), stream())
+
+
 PLANES = {0: 4, 1: 7, 2: 8}  # packed float4 planes per Hermite variant
 
 
@@ -110,6 +122,10 @@ def map_unpack(variant, packed, psi, T, dT, d2T):
 def march_packed(variant, u, dx, dt, eps, packed_in, packed_out, res, identity=False):
     _call("edge_march_packed", variant, *res, F(dx), F(dt), F(eps), *_p3(u), ptr(packed_in), ptr(packed_out),
           int(bool(identity)), stream())
+
+
+def march_ge_packed(u, dx, dt, packed_in, packed_out, res):
+    _call("edge_march_ge_packed", *res, F(dx), F(dt), *_p3(u), ptr(packed_in), ptr(packed_out), stream())
 
 
 def face_map_packed(variant, dx, packed, res, fpsi, fcol):

@@ -1,5 +1,6 @@
-"""The EDGE / ED4 / ED8 substep on one B200 (run_edge.py:588-712,
-run_ed4.py:402-484, run_ed8.py:365-451), on device-resident state.
+"""The EDGE / ED4 / ED8 / GE substep on one B200 (run_edge.py:588-712,
+run_ed4.py:402-484, run_ed8.py:365-451, run_ge.py:363-448), on
+device-resident state.
 
 Differences from the reference's orchestration that do not change results:
   * the flow-map state is ping-ponged between two buffer sets instead of being
@@ -23,7 +24,9 @@ from . import ops
 from .fields import face_shapes, zeros_cells, zeros_faces
 from .projection import Projection
 
-VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL}
+# GE (run_ge.py) keeps the ED8 map (psi, T, dT, d2T, full Hermite) and differs
+# from ED8 only in the march
+VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL, "ge": N.HERMITE_FULL}
 
 
 class EdgeSim:
@@ -93,9 +96,9 @@ class EdgeSim:
     def _map_set(self):
         r = self.res
         m = {"psi": zeros_cells(r, 3), "T": [zeros_cells(r, 3) for _ in range(3)]}
-        if self.variant in ("edge", "ed8"):
+        if self.variant in ("edge", "ed8", "ge"):
             m["dT"] = [zeros_cells(r, 3) for _ in range(3)]
-        if self.variant == "ed8":
+        if self.variant in ("ed8", "ge"):
             m["d2T"] = [zeros_cells(r) for _ in range(3)]
         return m
 
@@ -266,8 +269,11 @@ class EdgeSim:
                 m = self._map_set()
                 ops.reset_cells(dx, m["psi"], m["T"], m.get("dT"), m.get("d2T"))
                 ops.map_pack(self.hv, m["psi"], m["T"], m.get("dT"), m.get("d2T"), src)
-            ops.march_packed(self.hv, self.u, dx, dt, eps, src, dst, self.res,
-                             identity=reinit and self.variant == "edge")
+            if self.variant == "ge":
+                ops.march_ge_packed(self.u, dx, dt, src, dst, self.res)
+            else:
+                ops.march_packed(self.hv, self.u, dx, dt, eps, src, dst, self.res,
+                                 identity=reinit and self.variant == "edge")
             self.cur ^= 1
             return
         src, dst = self.maps[self.cur], self.maps[self.cur ^ 1]
@@ -279,6 +285,9 @@ class EdgeSim:
                 ops.reset_cells(dx, src["psi"], src["T"], src.get("dT"), src.get("d2T"))
             if self.variant == "ed4":
                 ops.march_ed4(self.u, dx, dt, eps, src["psi"], src["T"], dst["psi"], dst["T"])
+            elif self.variant == "ge":
+                ops.march_ge(self.u, dx, dt, src["psi"], src["T"], src["dT"], src["d2T"], dst["psi"], dst["T"],
+                             dst["dT"], dst["d2T"])
             else:
                 ops.march_ed8(self.u, dx, dt, eps, src["psi"], src["T"], src["dT"], src["d2T"], dst["psi"],
                               dst["T"], dst["dT"], dst["d2T"])

@@ -20,7 +20,7 @@ from edgeb200.fields import require
 
 __all__ = [
     "advect_psi_garm_ed4_fusion_unroll", "advect_ps_hermite_ed4_fd_unroll", "advect_ps_hermite_ed8",
-    "advect_u_semi_lagrangian", "reset_to_identity_1", "reset_to_identity_2", "reset_to_identity_3",
+    "advect_ps_garm", "calc_fd_3_from_grad", "advect_u_semi_lagrangian", "reset_to_identity_1", "reset_to_identity_2", "reset_to_identity_3",
     "reset_to_identity_ed4", "reset_to_identity_ed8", "interp_hermite_points",
 ]
 
@@ -59,6 +59,24 @@ def advect_ps_hermite_ed8(psi_000, psi_001, psi_010, psi_011, psi_100, psi_101, 
     for d, s in ((psi, psi_000), (T_x, psi_001), (T_y, psi_010), (T_z, psi_011), (dT_x, psi_100),
                  (dT_y, psi_101), (dT_z, psi_110), (d2T_x, d2[0]), (d2T_y, d2[1]), (d2T_z, d2[2])):
         ops.copy(s, d)
+
+
+def advect_ps_garm(psi_tmp, T_x_tmp, T_y_tmp, T_z_tmp, psi, T_x, T_y, T_z, dT_x, dT_y, dT_z, d2T_x, d2T_y, d2T_z,
+                   u_x, u_y, u_z, X, dx, dt):
+    """hermite.py:1398-1424: GE march.  As in the reference, the new psi and T
+    are left in the _tmp fields as well as in psi, T."""
+    dn = [torch.empty_like(dT_x) for _ in range(3)]
+    d2n = [torch.empty_like(d2T_x) for _ in range(3)]
+    ops.march_ge((u_x, u_y, u_z), dx, dt, psi, (T_x, T_y, T_z), (dT_x, dT_y, dT_z), (d2T_x, d2T_y, d2T_z),
+                 psi_tmp, (T_x_tmp, T_y_tmp, T_z_tmp), dn, d2n)
+    for d, s in ((psi, psi_tmp), (T_x, T_x_tmp), (T_y, T_y_tmp), (T_z, T_z_tmp), (dT_x, dn[0]), (dT_y, dn[1]),
+                 (dT_z, dn[2]), (d2T_x, d2n[0]), (d2T_y, d2n[1]), (d2T_z, d2n[2])):
+        ops.copy(s, d)
+
+
+def calc_fd_3_from_grad(T_x, T_y, T_z, dT_x, dT_y, dT_z, d2T_x, d2T_y, d2T_z, dx):
+    """hermite.py:1180-1256."""
+    ops.calc_fd_3_from_grad(dx, (T_x, T_y, T_z), (dT_x, dT_y, dT_z), (d2T_x, d2T_y, d2T_z))
 
 
 def advect_u_semi_lagrangian(u_x0, u_y0, u_z0, u_x1, u_y1, u_z1, dx, dt, X_x, X_y, X_z):

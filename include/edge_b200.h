@@ -95,6 +95,23 @@ int edge_march_ed8(int nx, int ny, int nz, float dx, float dt, float epsilon, co
                    const float *dTx, const float *dTy, const float *dTz, const float *d2Tx, const float *d2Ty,
                    const float *d2Tz, float *opsi, float *oTx, float *oTy, float *oTz, float *odTx, float *odTy,
                    float *odTz, float *od2Tx, float *od2Ty, float *od2Tz, void *stream);
+/* advect_ps_garm, hermite.py:1398-1424 (GE, run_ge.py:220-230): each cell
+ * centre marched back by RK4 with its Jacobian from the identity, composed
+ * with the accumulated map (psi, T, dT, d2T) by the full stored-derivative
+ * Hermite; dT and d2T of the new map by edge_calc_fd_3_from_grad.  Outputs
+ * must not alias the inputs. */
+int edge_march_ge(int nx, int ny, int nz, float dx, float dt, const float *ux, const float *uy, const float *uz,
+                  const float *psi, const float *Tx, const float *Ty, const float *Tz, const float *dTx,
+                  const float *dTy, const float *dTz, const float *d2Tx, const float *d2Ty, const float *d2Tz,
+                  float *opsi, float *oTx, float *oTy, float *oTz, float *odTx, float *odTy, float *odTz,
+                  float *od2Tx, float *od2Ty, float *od2Tz, void *stream);
+/* calc_fd_3_from_grad, hermite.py:1180-1256: dT_c = (psi_c,yz, psi_c,xz,
+ * psi_c,xy) from central differences of the gradient rows T_c and d2T_c =
+ * psi_c,xyz from central differences of dT_c, neighbour indices clamped to
+ * the grid.  dT must not alias T. */
+int edge_calc_fd_3_from_grad(int nx, int ny, int nz, float dx, const float *Tx, const float *Ty, const float *Tz,
+                             float *dTx, float *dTy, float *dTz, float *d2Tx, float *d2Ty, float *d2Tz,
+                             void *stream);
 /* Hermite psi and Jacobian column a at every face of grid a:
  *  - EDGE_HERMITE_FULL: split_psi_hermite, run_ed8.py:191-224
  *  - EDGE_HERMITE_GARM / _FD: the face evaluations shared by map_u_psi
@@ -124,6 +141,10 @@ int edge_map_unpack(int variant, int nx, int ny, int nz, const float *packed, fl
 int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, float epsilon, const float *ux,
                       const float *uy, const float *uz, const float *in_packed, float *out_packed, int identity,
                       void *stream);
+/* edge_march_ge on packed maps (the ED8 planes 0-7); out_packed must not
+ * alias in_packed. */
+int edge_march_ge_packed(int nx, int ny, int nz, float dx, float dt, const float *ux, const float *uy,
+                         const float *uz, const float *in_packed, float *out_packed, void *stream);
 /* edge_face_map on a packed map */
 int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const float *packed, float *fpsix,
                          float *fpsiy, float *fpsiz, float *fcolx, float *fcoly, float *fcolz, void *stream);

@@ -514,6 +514,81 @@ EXPORT void orc_march_ed8(int nx, int ny, int nz, float dx, float dt, float epsi
             }
 }
 
+/* hermite.py:1180-1256 calc_fd_3_from_grad: the mixed second derivatives of
+ * each psi_c from central differences of its stored gradient row T_c (index
+ * clamped at the walls, taichi_utils.py sample), then the triple derivative
+ * from central differences of those.  The dT loops finish before the d2T
+ * loops start (separate offloaded loops of one Taichi kernel). */
+EXPORT void orc_calc_fd_3_from_grad(int nx, int ny, int nz, float dx,
+                                    const float *Tx, const float *Ty, const float *Tz,
+                                    float *dTx, float *dTy, float *dTz, float *d2Tx, float *d2Ty, float *d2Tz) {
+    const float *T[3] = {Tx, Ty, Tz};
+    float *dT[3] = {dTx, dTy, dTz};
+    float *d2T[3] = {d2Tx, d2Ty, d2Tz};
+    for (int c = 0; c < 3; c++) {
+        const float *t = T[c];
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++)
+                for (int k = 0; k < nz; k++) {
+#define TS(a, b, d) samp_v(t, nx, ny, nz, 3, (a), (b), (d))
+                    float *o = dT[c] + 3 * ix3(i, j, k, ny, nz);
+                    o[0] = ((TS(i, j, k + 1)[1] - TS(i, j, k - 1)[1]) + (TS(i, j + 1, k)[2] - TS(i, j - 1, k)[2])) / 4.0f / dx;
+                    o[1] = ((TS(i, j, k + 1)[0] - TS(i, j, k - 1)[0]) + (TS(i + 1, j, k)[2] - TS(i - 1, j, k)[2])) / 4.0f / dx;
+                    o[2] = ((TS(i, j + 1, k)[0] - TS(i, j - 1, k)[0]) + (TS(i + 1, j, k)[1] - TS(i - 1, j, k)[1])) / 4.0f / dx;
+#undef TS
+                }
+    }
+    for (int c = 0; c < 3; c++) {
+        const float *t = dT[c];
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++)
+                for (int k = 0; k < nz; k++) {
+#define DS(a, b, d) samp_v(t, nx, ny, nz, 3, (a), (b), (d))
+                    d2T[c][ix3(i, j, k, ny, nz)] = ((DS(i + 1, j, k)[0] - DS(i - 1, j, k)[0]) +
+                                                    (DS(i, j + 1, k)[1] - DS(i, j - 1, k)[1]) +
+                                                    (DS(i, j, k + 1)[2] - DS(i, j, k - 1)[2])) / 6.0f / dx;
+#undef DS
+                }
+    }
+}
+
+/* hermite.py:1398-1424 advect_ps_garm (the GE march, run_ge.py:220-230):
+ * every cell centre is marched back by RK4 with its Jacobian from the
+ * identity (reset_to_identity_1, advance_map_1_transpose with -dt,
+ * hermite.py:643-654, 864-918), composed with the accumulated map by the full
+ * stored-derivative Hermite (interp_psi_hermite_garm, hermite.py:1024-1046),
+ * and dT, d2T of the new map come from calc_fd_3_from_grad. */
+EXPORT void orc_march_ge(int nx, int ny, int nz, float dx, float dt,
+                         const float *ux, const float *uy, const float *uz,
+                         const float *psi, const float *Tx, const float *Ty, const float *Tz,
+                         const float *dTx, const float *dTy, const float *dTz,
+                         const float *d2Tx, const float *d2Ty, const float *d2Tz,
+                         float *opsi, float *oTx, float *oTy, float *oTz,
+                         float *odTx, float *odTy, float *odTz, float *od2Tx, float *od2Ty, float *od2Tz) {
+    mac_t mac = mac_make(ux, uy, uz, nx, ny, nz, dx);
+    map_t m = {psi, {Tx, Ty, Tz}, {dTx, dTy, dTz}, {d2Tx, d2Ty, d2Tz}, nx, ny, nz, dx};
+    float *oT[3] = {oTx, oTy, oTz};
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                float P[3], T[3][3];
+                cell_pos(i, j, k, dx, P);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) T[a][b] = a == b ? 1.0f : 0.0f;
+                rk4_rows(&mac, P, T, -dt);
+                compose(HV_FULL, &m, P, T);
+                size_t o = ix3(i, j, k, ny, nz);
+                for (int c = 0; c < 3; c++) {
+                    opsi[3 * o + c] = P[c];
+                    for (int d = 0; d < 3; d++) oT[c][3 * o + d] = T[c][d];
+                }
+            }
+    orc_calc_fd_3_from_grad(nx, ny, nz, dx, oTx, oTy, oTz, odTx, odTy, odTz, od2Tx, od2Ty, od2Tz);
+}
+
 /* run_ed8.py:191-224 split_psi_hermite: full Hermite psi and Jacobian column
  * on each face grid (psi_f: vec3, T_f: vec3 = column `axis` of grad psi). */
 EXPORT void orc_split_psi_hermite(int nx, int ny, int nz, float dx,

@@ -159,6 +159,27 @@ def march_ed8(u, psi, T, dT, d2T, dx, dt, eps):
     return o[0], o[1:4], o[4:7], o[7:10]
 
 
+def calc_fd_3_from_grad(T, dx):
+    """hermite.py:1180-1256 -> (dT, d2T) from the gradient rows T."""
+    res = T[0].shape[:3]
+    dT = [np.empty(res + (3,), F32) for _ in range(3)]
+    d2T = [np.empty(res, F32) for _ in range(3)]
+    lib().orc_calc_fd_3_from_grad(*(_i(s) for s in res), _f(dx), *(_p(_c32(t)) for t in T), *(_p(a) for a in dT),
+                                  *(_p(a) for a in d2T))
+    return dT, d2T
+
+
+def march_ge(u, psi, T, dT, d2T, dx, dt):
+    """hermite.py:1398-1424 advect_ps_garm (GE)."""
+    u = [_c32(a) for a in u]
+    res = psi.shape[:3]
+    o = [np.empty(res + (3,), F32) for _ in range(7)] + [np.empty(res, F32) for _ in range(3)]
+    lib().orc_march_ge(*(_i(s) for s in res), _f(dx), _f(dt), *(_p(a) for a in u), _p(_c32(psi)),
+                       *(_p(_c32(t)) for t in T), *(_p(_c32(t)) for t in dT), *(_p(_c32(t)) for t in d2T),
+                       *(_p(a) for a in o))
+    return o[0], o[1:4], o[4:7], o[7:10]
+
+
 def split_psi_hermite(psi, T, dT, d2T, dx):
     """run_ed8.py:191-224 split_psi_hermite -> (psi_faces, T_faces)."""
     res = psi.shape[:3]
@@ -410,7 +431,8 @@ def emit_smoke(res, dx, centers, colors, radius, smoke):
 def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_clamp=True, dt=None,
                  abs_tol=1e-12, rel_tol=1e-12, variant="edge", solid=None, emitters=None, particles=None):
     """One iteration of run_edge.py:588-712 (variant "edge"), run_ed4.py:
-    402-484 ("ed4") or run_ed8.py:365-451 ("ed8"); no particles, no solids,
+    402-484 ("ed4"), run_ed8.py:365-451 ("ed8") or run_ge.py:363-448 ("ge",
+    the ED8 substep with the GE march); no particles, no solids,
     no frame bookkeeping: dt = CFL*dx/max_speed unless given.  Returns
     (dt, iters)."""
     if variant != "edge":
@@ -522,6 +544,8 @@ def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_
     it1 = poisson(st.u, base_level, abs_tol=abs_tol, rel_tol=rel_tol)[0]
     if variant == "ed4":
         st.psi, st.T = march_ed4(st.u, st.psi, st.T, dx, dt32, eps)
+    elif variant == "ge":
+        st.psi, st.T, st.dT, st.d2T = march_ge(st.u, st.psi, st.T, st.dT, st.d2T, dx, dt32)
     else:
         st.psi, st.T, st.dT, st.d2T = march_ed8(st.u, st.psi, st.T, st.dT, st.d2T, dx, dt32, eps)
     for a in range(3):

@@ -356,6 +356,40 @@ def march_ed8():
 
 
 @fixture
+def march_ge():
+    """GE march advect_ps_garm (hermite.py:1398-1424, which ends in
+    calc_fd_3_from_grad, hermite.py:1180-1256) followed by the face split of
+    run_ge.py:185-217."""
+    rng = np.random.default_rng(505)
+    g = Grid(*G_SMALL)
+    u = velocity(rng, g)
+    ms = map_state(rng, g, with_dT=True, with_d2T=True)
+    dt = dt_for(u, g)
+    inputs = {"psi": ms["psi"].to_numpy(), **{f"T_{a}": ms["T"][i].to_numpy() for i, a in enumerate("xyz")},
+              **{f"dT_{a}": ms["dT"][i].to_numpy() for i, a in enumerate("xyz")},
+              **{f"d2T_{a}": ms["d2T"][i].to_numpy() for i, a in enumerate("xyz")}}
+    tmp = [vfield(g.res) for _ in range(4)]
+    H.advect_ps_garm(*tmp, ms["psi"], *ms["T"], *ms["dT"], *ms["d2T"], *u, g.X, g.dx, dt)
+    fx, fy, fz = g.faces()
+    Tf = [vfield(fx), vfield(fy), vfield(fz)]
+    Pf = [vfield(fx), vfield(fy), vfield(fz)]
+    ns = load_driver_kernels("run_ge.py", ["split_psi_hermite"], dict(
+        T_x=Tf[0], T_y=Tf[1], T_z=Tf[2], psi_x=Pf[0], psi_y=Pf[1], psi_z=Pf[2],
+        psi_garm=ms["psi"], T_x_garm=ms["T"][0], T_y_garm=ms["T"][1], T_z_garm=ms["T"][2],
+        dT_x_garm=ms["dT"][0], dT_y_garm=ms["dT"][1], dT_z_garm=ms["dT"][2],
+        d2T_x_garm=ms["d2T"][0], d2T_y_garm=ms["d2T"][1], d2T_z_garm=ms["d2T"][2],
+        X_x=g.X_x, X_y=g.X_y, X_z=g.X_z, dx=g.dx))
+    ns["split_psi_hermite"]()
+    save("march_ge", meta_dx=g.dx, meta_dt=dt, res=np.array(g.res),
+         u_x=u[0], u_y=u[1], u_z=u[2], **{"in_" + k: v for k, v in inputs.items()},
+         out_psi=ms["psi"], out_T_x=ms["T"][0], out_T_y=ms["T"][1], out_T_z=ms["T"][2],
+         out_dT_x=ms["dT"][0], out_dT_y=ms["dT"][1], out_dT_z=ms["dT"][2],
+         out_d2T_x=ms["d2T"][0], out_d2T_y=ms["d2T"][1], out_d2T_z=ms["d2T"][2],
+         face_psi_x=Pf[0], face_psi_y=Pf[1], face_psi_z=Pf[2],
+         face_T_x=Tf[0], face_T_y=Tf[1], face_T_z=Tf[2])
+
+
+@fixture
 def advect_faces():
     """Semi-Lagrangian advect_u_semi_lagrangian (hermite.py:1578-1621), the
     forward-map march advance_map (run_edge.py:337-357), map_u

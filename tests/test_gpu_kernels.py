@@ -328,3 +328,95 @@ def test_packed_layout_roundtrip_and_march(ops, variant):
     ops.face_map_packed(variant, dx, packed, res, fp2, fc2)
     for a, b in zip(fp + fc, fp2 + fc2):
         assert rel_l2(N_(b), N_(a)) < 1e-6
+
+
+def test_march_ge_and_split(ops):
+    """GE march advect_ps_garm against the reference's own output."""
+    d = load_golden("march_ge")
+    u = [T_(d[k]) for k in ("u_x", "u_y", "u_z")]
+    psi = T_(d["in_psi"])
+    T = [T_(d["in_T_" + a]) for a in "xyz"]
+    dT = [T_(d["in_dT_" + a]) for a in "xyz"]
+    d2T = [T_(d["in_d2T_" + a]) for a in "xyz"]
+    o = [torch.empty_like(psi) for _ in range(7)] + [torch.empty_like(d2T[0]) for _ in range(3)]
+    ops.march_ge(u, float(d["meta_dx"]), float(d["meta_dt"]), psi, T, dT, d2T, o[0], o[1:4], o[4:7], o[7:10])
+    assert rel_l2(N_(o[0]), d["out_psi"]) < TOL
+    for i, a in enumerate("xyz"):
+        # T is marched and composed (no epsilon difference); dT, d2T are grid
+        # differences of T over 4 dx and 6 dx
+        assert rel_l2(N_(o[1 + i]), d["out_T_" + a]) < TOL
+        assert rel_l2(N_(o[4 + i]), d["out_dT_" + a]) < 1e-4
+        assert rel_l2(N_(o[7 + i]), d["out_d2T_" + a]) < 1e-4
+    # calc_fd_3_from_grad alone, on the reference's T: same float32 expressions
+    dT2 = [torch.empty_like(t) for t in T]
+    d2T2 = [torch.empty_like(t) for t in d2T]
+    ops.calc_fd_3_from_grad(float(d["meta_dx"]), [T_(d["out_T_" + a]) for a in "xyz"], dT2, d2T2)
+    for i, a in enumerate("xyz"):
+        assert rel_l2(N_(dT2[i]), d["out_dT_" + a]) < 1e-6
+        assert rel_l2(N_(d2T2[i]), d["out_d2T_" + a]) < 1e-6
+
+
+def test_march_ge_larger_grid_and_packed(ops):
+    """48x32x24 GE march against the oracle, and the packed-plane march equal
+    to the reference-layout one."""
+    rng = np.random.default_rng(55)
+    res = (48, 32, 24)
+    dx = 1.0 / 32
+    u = [(0.8 * np.sin(np.indices(s)[0] * 0.2 + a) * np.cos(np.indices(s)[1] * 0.15)).astype(np.float32)
+         for a, s in enumerate(O.face_shapes(res))]
+    psi = (O.center_coords(res, dx) + 0.3 * dx * rng.uniform(-1, 1, size=res + (3,))).astype(np.float32)
+    T = [(np.eye(3)[c] + 0.05 * rng.normal(size=res + (3,))).astype(np.float32) for c in range(3)]
+    dT = [(0.2 * rng.normal(size=res + (3,))).astype(np.float32) for _ in range(3)]
+    d2T = [(0.2 * rng.normal(size=res)).astype(np.float32) for _ in range(3)]
+    dt = 0.01
+    opsi, oT, odT, od2T = O.march_ge(u, psi, T, dT, d2T, dx, dt)
+    gu = [T_(a) for a in u]
+    g = [torch.empty(res + (3,), device="cuda") for _ in range(7)] + [torch.empty(res, device="cuda") for _ in range(3)]
+    gin = (T_(psi), [T_(t) for t in T], [T_(t) for t in dT], [T_(t) for t in d2T])
+    ops.march_ge(gu, dx, dt, *gin, g[0], g[1:4], g[4:7], g[7:10])
+    assert rel_l2(N_(g[0]), opsi) < TOL
+    for i in range(3):
+        assert rel_l2(N_(g[1 + i]), oT[i]) < TOL
+        assert rel_l2(N_(g[4 + i]), odT[i]) < 1e-4
+        assert rel_l2(N_(g[7 + i]), od2T[i]) < 1e-4
+    packed = torch.zeros((8,) + res + (4,), device="cuda")
+    ops.map_pack(2, *gin, packed)
+    out = torch.zeros_like(packed)
+    ops.march_ge_packed(gu, dx, dt, packed, out, res)
+    p = [torch.empty_like(t) for t in g]
+    ops.map_unpack(2, out, p[0], p[1:4], p[4:7], p[7:10])
+    for a, b in zip(p, g):
+        assert rel_l2(N_(a), N_(b)) < 1e-6
+
+
+def test_dropin_hermite_marches():
+    """The sim/hermite.py drop-in entry points, called with the reference's
+    arguments (fields in place, scratch fields, X), reproduce the reference's
+    marches on its golden vectors."""
+    from sim import hermite as H
+    for name in ("march_ed8", "march_ge", "march_edge"):
+        d = load_golden(name)
+        res = tuple(int(v) for v in d["res"])
+        dx, dt = float(d["meta_dx"]), float(d["meta_dt"])
+        X = T_(O.center_coords(res, dx))
+        u = [T_(d[k]) for k in ("u_x", "u_y", "u_z")]
+        psi = T_(d["in_psi"])
+        T = [T_(d["in_T_" + a]) for a in "xyz"]
+        dT = [T_(d["in_dT_" + a]) for a in "xyz"]
+        if name == "march_edge":
+            tmp = [torch.empty_like(psi) for _ in range(7)]
+            H.advect_psi_garm_ed4_fusion_unroll(*tmp, psi, *T, *dT, *u, X, dx, dt, float(d["meta_eps"]))
+        else:
+            d2T = [T_(d["in_d2T_" + a]) for a in "xyz"]
+            if name == "march_ed8":
+                tmp = [torch.empty_like(psi) for _ in range(8)]
+                H.advect_ps_hermite_ed8(*tmp, psi, *T, *dT, *d2T, *u, X, dx, dt, float(d["meta_eps"]))
+            else:
+                tmp = [torch.empty_like(psi) for _ in range(4)]
+                H.advect_ps_garm(*tmp, psi, *T, *dT, *d2T, *u, X, dx, dt)
+            for i, a in enumerate("xyz"):
+                assert rel_l2(N_(d2T[i]), d["out_d2T_" + a]) < TOL_D2T, name
+        assert rel_l2(N_(psi), d["out_psi"]) < TOL, name
+        for i, a in enumerate("xyz"):
+            assert rel_l2(N_(T[i]), d["out_T_" + a]) < TOL_T, name
+            assert rel_l2(N_(dT[i]), d["out_dT_" + a]) < TOL_DT, name

@@ -39,7 +39,7 @@ def test_edge_steps_golden():
 
 
 @pytest.mark.parametrize("packed", [False, True])
-@pytest.mark.parametrize("variant", ["edge", "ed4", "ed8"])
+@pytest.mark.parametrize("variant", ["edge", "ed4", "ed8", "ge"])
 def test_steps_vs_oracle(variant, packed):
     from edgeb200.sim import EdgeSim, leapfrog_init
     res = (32, 16, 16)

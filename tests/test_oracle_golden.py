@@ -82,6 +82,30 @@ def test_march_ed8_and_split():
         assert rel_l2(tf[i], d["face_T_" + a]) < TOL
 
 
+def test_march_ge_and_split():
+    d = load_golden("march_ge")
+    u = [d["u_x"], d["u_y"], d["u_z"]]
+    psi, T, dT, d2T = O.march_ge(u, d["in_psi"], [d["in_T_" + a] for a in "xyz"], [d["in_dT_" + a] for a in "xyz"],
+                                 [d["in_d2T_" + a] for a in "xyz"], float(d["meta_dx"]), d["meta_dt"])
+    assert rel_l2(psi, d["out_psi"]) < TOL
+    for i, a in enumerate("xyz"):
+        # no epsilon differences: the Jacobian is marched and composed, dT and
+        # d2T are grid differences of it
+        assert rel_l2(T[i], d["out_T_" + a]) < TOL
+        assert rel_l2(dT[i], d["out_dT_" + a]) < 1e-5
+        assert rel_l2(d2T[i], d["out_d2T_" + a]) < 1e-5
+    # calc_fd_3_from_grad alone on the reference's marched Jacobian
+    dT2, d2T2 = O.calc_fd_3_from_grad([d["out_T_" + a] for a in "xyz"], float(d["meta_dx"]))
+    for i, a in enumerate("xyz"):
+        assert rel_l2(dT2[i], d["out_dT_" + a]) < TOL
+        assert rel_l2(d2T2[i], d["out_d2T_" + a]) < TOL
+    pf, tf = O.split_psi_hermite(d["out_psi"], [d["out_T_" + a] for a in "xyz"], [d["out_dT_" + a] for a in "xyz"],
+                                 [d["out_d2T_" + a] for a in "xyz"], float(d["meta_dx"]))
+    for i, a in enumerate("xyz"):
+        assert rel_l2(pf[i], d["face_psi_" + a]) < TOL
+        assert rel_l2(tf[i], d["face_T_" + a]) < TOL
+
+
 def test_face_kernels():
     d = load_golden("advect_faces")
     u = [d["u_x"], d["u_y"], d["u_z"]]
