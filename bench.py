@@ -206,11 +206,13 @@ def instrumented_step(sim):
     mark("mgpcg_solve_1")
     it1 = sim.proj.result()[0]
     mark("_sync1")
-    sim._march(dt, j == 0)
+    sim._march(dt, j == 0, j)
     mark("march_edge")
     ops.advance_map(sim.u, dx, dt, sim.phi, sim.F)
     mark("advance_map")
-    if sim.packed:
+    if sim.variant == "efm":
+        pass  # the backtrack (march_edge stage) wrote the face map
+    elif sim.packed:
         ops.face_map_packed(sim.hv, dx, sim.pmaps[sim.cur], sim.res, sim.fpsi, sim.fcol)
     else:
         m = sim.map
@@ -375,14 +377,19 @@ def pcg_measure(res, reps=5):
 MARCH_FLOP_PER_CELL = {"edge": 27400, "ed4": 8400, "ed8": 16800, "ge": 5500}
 
 
-def march_roofline(stages, variant, peak_tflops, ncells):
+# EFM: RK4 of the face map with its Jacobian column through each cached field
+EFM_FLOP_PER_FACE_STEP = 3000
+
+
+def march_roofline(stages, variant, peak_tflops, ncells, flop_per_cell=None):
     ms = stages.get("march_edge", 0.0)
     if ms <= 0 or not peak_tflops:
         return None
-    flops = MARCH_FLOP_PER_CELL[variant] * ncells
-    ach = flops / (ms * 1e-3) / 1e12
-    return {"kernel": f"k_march_{variant}_p", "bound": "fp32", "achieved": ach, "peak": peak_tflops,
-            "unit": "TFLOP/s", "frac": ach / peak_tflops, "flop_per_cell": MARCH_FLOP_PER_CELL[variant],
+    fpc = MARCH_FLOP_PER_CELL[variant] if flop_per_cell is None else flop_per_cell
+    ach = fpc * ncells / (ms * 1e-3) / 1e12
+    kernel = "k_backtrack_faces" if variant == "efm" else f"k_march_{variant}_p"
+    return {"kernel": kernel, "bound": "fp32", "achieved": ach, "peak": peak_tflops,
+            "unit": "TFLOP/s", "frac": ach / peak_tflops, "flop_per_cell": round(fpc, 1),
             "peak_source": "measured here (edge_fma_peak, FP32 FMA chains)"}
 
 
@@ -572,7 +579,7 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "1 full substep of the same workload (first step after reinit), C/OpenMP restatement "
                          "of the reference kernels"}
-    # ED4 / ED8 / GE steps of the same workload (a few steps each, outside the
+    # ED4 / ED8 / GE / EFM steps of the same workload (a few steps each, outside the
     # timed region of the EDGE line)
     variants = {}
     fp32_peak = ops.fma_peak_tflops() if not args.no_extras else None
@@ -581,22 +588,31 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_variants and args.variant == "edge" and not args.res:
         del sim
         torch.cuda.empty_cache()
-        for v in ("ed4", "ed8", "ge"):
+        for v in ("ed4", "ed8", "ge", "efm"):
             vs = make_sim(v, args.res, packed=not args.unpacked)
             for _ in range(3):
                 vs.step()
             torch.cuda.synchronize()
+            # EFM's cost grows with the number of cached steps: time one whole
+            # reinitialisation interval
+            nsteps = REINIT if v == "efm" else 6
             a0 = torch.cuda.Event(enable_timing=True)
             a1 = torch.cuda.Event(enable_timing=True)
             a0.record()
-            for _ in range(6):
+            for _ in range(nsteps):
                 vs.step()
             a1.record()
             torch.cuda.synchronize()
             vst, _ = instrumented_step(vs)
-            variants[v] = {"ms_per_step": a0.elapsed_time(a1) / 6, "steps_per_s": 6e3 / a0.elapsed_time(a1),
-                           "march_ms": round(vst.get("march_edge", 0.0), 4),
-                           "march_roofline_fp32": march_roofline(vst, v, fp32_peak, NC)}
+            if v == "efm":
+                # the instrumented step backtracks through j + 1 cached fields
+                flop = EFM_FLOP_PER_FACE_STEP * NF * (vs.i % vs.reinit_every + 1)
+                roof = march_roofline(vst, v, fp32_peak, NC, flop_per_cell=flop / NC)
+            else:
+                roof = march_roofline(vst, v, fp32_peak, NC)
+            variants[v] = {"ms_per_step": a0.elapsed_time(a1) / nsteps,
+                           "steps_per_s": nsteps * 1e3 / a0.elapsed_time(a1),
+                           "march_ms": round(vst.get("march_edge", 0.0), 4), "march_roofline_fp32": roof}
             del vs
             torch.cuda.empty_cache()
     c2 = c2_measure() if not (args.res or args.no_extras) else None
@@ -661,7 +677,7 @@ def main():
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="edge", choices=["edge", "ed4", "ed8", "ge"])
+    ap.add_argument("--variant", default="edge", choices=["edge", "ed4", "ed8", "ge", "efm"])
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=2)
@@ -670,7 +686,7 @@ def main():
     ap.add_argument("--pcg-only", action="store_true", help="only the PCG-to-1e-6 measurement (profiling)")
     ap.add_argument("--learned-only", action="store_true", help="only the learned-preconditioner measurement")
     ap.add_argument("--c2-only", action="store_true", help="only the solid + particle configuration")
-    ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8/GE step timings")
+    ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8/GE/EFM step timings")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the EDGE steps (no ED4/ED8, PCG or FP32-peak measurements; profiling)")
     ap.add_argument("--res", type=int, nargs=3, default=None,

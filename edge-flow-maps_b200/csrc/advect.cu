@@ -617,6 +617,43 @@ __global__ void __launch_bounds__(128) k_advance_map(Mac mac, float dt, float* p
     }
 }
 
+// EFM backward map (run_efm.py:179-186 backtrack_psi_grid): every face starts
+// at the identity (reset_to_identity, run_efm.py:153-167) and is marched by
+// advance_map with -dts[s] through the cached velocities, newest first.  The
+// reference runs one advance_map kernel per cached step and stores psi, T in
+// between; here the whole chain runs in registers in one launch, so the map
+// crosses HBM once (the float32 values between steps are the same).
+constexpr int kMaxBacktrack = 64;
+struct VelRing {
+    const float* u[kMaxBacktrack][3];  // in application order (newest first)
+    float dt[kMaxBacktrack];           // signed steps (-dts[s])
+    int steps;
+};
+
+__global__ void __launch_bounds__(128) k_backtrack_faces(Mac mac, VelRing ring, float* px, float* py, float* pz,
+                                                         float* Tx, float* Ty, float* Tz) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
+    FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
+    float P[3], C[1][3];
+    face_pos(f.axis, f.i, f.j, f.k, mac.dx, P);
+    for (int c = 0; c < 3; c++) C[0][c] = c == f.axis ? 1.0f : 0.0f;
+#pragma unroll 1
+    for (int s = 0; s < ring.steps; s++) {
+        Mac m = mac;
+        m.u[0] = ring.u[s][0];
+        m.u[1] = ring.u[s][1];
+        m.u[2] = ring.u[s][2];
+        rk4_jac<1>(m, P, C, ring.dt[s]);
+    }
+    float* p = f.axis == 0 ? px : (f.axis == 1 ? py : pz);
+    float* T = f.axis == 0 ? Tx : (f.axis == 1 ? Ty : Tz);
+    for (int c = 0; c < 3; c++) {
+        p[3 * f.e + c] = P[c];
+        T[3 * f.e + c] = C[0][c];
+    }
+}
+
 // advect_u_semi_lagrangian (hermite.py:1578-1621)
 __global__ void __launch_bounds__(128) k_advect_sl(Mac mac, float dt, float* ox, float* oy, float* oz) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1186,6 +1223,32 @@ int edge_advance_map(int nx, int ny, int nz, float dx, float dt, const float* ux
     if (!dims_ok(nx, ny, nz) || !ux || !uy || !uz || !phix || !phiy || !phiz || !Fx || !Fy || !Fz) return EDGE_EINVAL;
     k_advance_map<<<grid_for(n_faces(nx, ny, nz), 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), dt,
                                                                              phix, phiy, phiz, Fx, Fy, Fz);
+    return launch_status();
+}
+
+int edge_efm_backtrack(int nx, int ny, int nz, float dx, int curr_step, const float* const* ux_cache,
+                       const float* const* uy_cache, const float* const* uz_cache, const float* dts, float* psix,
+                       float* psiy, float* psiz, float* Tx, float* Ty, float* Tz, void* stream) {
+    if (!dims_ok(nx, ny, nz) || curr_step < 0 || curr_step >= kMaxBacktrack || !ux_cache || !uy_cache ||
+        !uz_cache || !dts || !psix || !psiy || !psiz || !Tx || !Ty || !Tz)
+        return EDGE_EINVAL;
+    VelRing ring;
+    ring.steps = curr_step + 1;
+    for (int s = 0; s <= curr_step; s++) {
+        int src = curr_step - s;  // newest first
+        if (!ux_cache[src] || !uy_cache[src] || !uz_cache[src]) return EDGE_EINVAL;
+        ring.u[s][0] = ux_cache[src];
+        ring.u[s][1] = uy_cache[src];
+        ring.u[s][2] = uz_cache[src];
+        ring.dt[s] = -dts[src];
+    }
+    for (int s = ring.steps; s < kMaxBacktrack; s++) {
+        ring.u[s][0] = ring.u[s][1] = ring.u[s][2] = nullptr;
+        ring.dt[s] = 0.0f;
+    }
+    k_backtrack_faces<<<grid_for(n_faces(nx, ny, nz), 128), 128, 0, S(stream)>>>(
+        make_mac(ux_cache[curr_step], uy_cache[curr_step], uz_cache[curr_step], nx, ny, nz, dx), ring, psix, psiy,
+        psiz, Tx, Ty, Tz);
     return launch_status();
 }
 

@@ -138,6 +138,17 @@ def face_map(variant, dx, psi, T, dT, d2T, fpsi, fcol):
            *_p3(fcol), stream())
 
 
+def efm_backtrack(u_cache, dts, dx, psi, T):
+    """Backward face map of the EFM driver through the cached velocities
+    u_cache[0..j] (slot j = the current velocity) with step sizes dts[0..j]."""
+    n = len(u_cache)
+    nx, ny, nz = dims_from_faces(*u_cache[0])
+    arrs = [(ctypes.c_void_p * n)(*[ptr(u[a]) for u in u_cache]) for a in range(3)]
+    d = (ctypes.c_float * n)(*[float(x) for x in dts])
+    _call("edge_efm_backtrack", nx, ny, nz, F(dx), n - 1, *[ctypes.addressof(a) for a in arrs], ctypes.addressof(d),
+          *_p3(psi), *_p3(T), stream())
+
+
 def advance_map(u, dx, dt, phi, Fm):
     nx, ny, nz = dims_from_faces(*u)
     _call("edge_advance_map", nx, ny, nz, F(dx), F(dt), *_p3(u), *_p3(phi), *_p3(Fm), stream())

@@ -1,6 +1,6 @@
-"""The EDGE / ED4 / ED8 / GE substep on one B200 (run_edge.py:588-712,
-run_ed4.py:402-484, run_ed8.py:365-451, run_ge.py:363-448), on
-device-resident state.
+"""The EDGE / ED4 / ED8 / GE / EFM substep on one B200 (run_edge.py:588-712,
+run_ed4.py:402-484, run_ed8.py:365-451, run_ge.py:363-448,
+run_efm.py:319-406), on device-resident state.
 
 Differences from the reference's orchestration that do not change results:
   * the flow-map state is ping-ponged between two buffer sets instead of being
@@ -25,8 +25,9 @@ from .fields import face_shapes, zeros_cells, zeros_faces
 from .projection import Projection
 
 # GE (run_ge.py) keeps the ED8 map (psi, T, dT, d2T, full Hermite) and differs
-# from ED8 only in the march
-VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL, "ge": N.HERMITE_FULL}
+# from ED8 only in the march; EFM (run_efm.py) keeps no cell map: its backward
+# map is re-integrated on the faces every step through the cached velocities
+VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL, "ge": N.HERMITE_FULL, "efm": None}
 
 
 class EdgeSim:
@@ -58,7 +59,14 @@ class EdgeSim:
         # backward map state, two sets (ping-pong); `packed` keeps them as
         # float4 planes (edge_map_pack layout) instead of the reference layout
         self.packed = bool(packed)
-        if self.packed:
+        if variant == "efm":
+            # velocity cache of the current reinitialisation interval
+            # (run_efm.py:104-109) and its step sizes in float32 (dts field)
+            self.u_cache = [zeros_faces(r) for _ in range(self.reinit_every)]
+            self.dts = [0.0] * self.reinit_every
+            self.packed = False
+            self.maps = None
+        elif self.packed:
             planes = ops.PLANES[self.hv]
             self.pmaps = [torch.zeros((planes,) + r + (4,), dtype=torch.float32, device=device) for _ in range(2)]
             self._unpacked = None
@@ -105,7 +113,9 @@ class EdgeSim:
     @property
     def map(self):
         """The current backward map in the reference layout (unpacked on
-        demand when the driver keeps packed planes)."""
+        demand when the driver keeps packed planes); None for EFM."""
+        if self.variant == "efm":
+            return None
         if not self.packed:
             return self.maps[self.cur]
         m = self._map_set()
@@ -119,6 +129,57 @@ class EdgeSim:
 
     def set_smoke(self, smoke):
         self.smoke.copy_(smoke)
+
+    def state_dict(self):
+        """Everything a later step reads: velocity, dye, the interval's
+        initial fields, both maps (backward map state or EFM velocity cache,
+        forward map), the particles and the frame bookkeeping.  Loading it
+        into a simulation built with the same arguments continues bit for
+        bit, also in the middle of a reinitialisation interval (the
+        reference's checkpoints hold u and dye only and restart the maps,
+        run_edge.py:559-566)."""
+        d = {"u": list(self.u), "smoke": self.smoke, "init_u": list(self.init_u), "init_smoke": self.init_smoke,
+             "phi": list(self.phi), "F": list(self.F),
+             "scalars": dict(i=self.i, sub_t=self.sub_t, frame_idx=self.frame_idx, last_dt=self.last_dt,
+                             cur=self.cur, variant=self.variant, packed=self.packed, res=self.res)}
+        if self.variant == "efm":
+            d["u_cache"] = [list(c) for c in self.u_cache]
+            d["scalars"]["dts"] = list(self.dts)
+        elif self.packed:
+            d["pmap"] = self.pmaps[self.cur]
+        else:
+            d["map"] = self.maps[self.cur]
+        if self.particles is not None:
+            d["particles"] = {k: v for k, v in self.particles.items() if torch.is_tensor(v) or isinstance(v, list)}
+        return {k: _detach_copy(v) for k, v in d.items()}
+
+    def load_state_dict(self, d):
+        s = d["scalars"]
+        if s["variant"] != self.variant or tuple(s["res"]) != self.res or s["packed"] != self.packed:
+            raise ValueError("state was saved by a simulation with another variant, grid or map layout")
+        _copy_into(self.u, d["u"])
+        _copy_into(self.init_u, d["init_u"])
+        _copy_into(self.phi, d["phi"])
+        _copy_into(self.F, d["F"])
+        self.smoke.copy_(d["smoke"])
+        self.init_smoke.copy_(d["init_smoke"])
+        self.i, self.sub_t, self.frame_idx, self.last_dt = s["i"], s["sub_t"], s["frame_idx"], s["last_dt"]
+        self.cur = s["cur"]
+        if self.variant == "efm":
+            for dst, src in zip(self.u_cache, d["u_cache"]):
+                _copy_into(dst, src)
+            self.dts = list(s["dts"])
+        elif self.packed:
+            self.pmaps[self.cur].copy_(d["pmap"])
+        else:
+            m = self.maps[self.cur]
+            for k, v in d["map"].items():
+                _copy_into(m[k], v) if isinstance(v, list) else m[k].copy_(v)
+        if "particles" in d:
+            if self.particles is None:
+                raise ValueError("state holds particles: call add_particles first")
+            for k, v in d["particles"].items():
+                _copy_into(self.particles[k], v) if isinstance(v, list) else self.particles[k].copy_(v)
 
     def add_particles(self, pos, vel, rad, domain, St, gravity, density_ratio, epiral_radius_ratio, Re,
                       laden_radius):
@@ -200,7 +261,7 @@ class EdgeSim:
             ops.advance_map(self.u, dx, curr_dt, self.phi, self.F)          # run_edge.py:660
             ev_fwd = torch.cuda.Event()
             ev_fwd.record(side)
-        self._march(curr_dt, reinit)
+        self._march(curr_dt, reinit, j)
         main.wait_event(ev_fwd)
         if self.particles is not None:
             # the forcing integrated into the map's origin velocity through the
@@ -209,7 +270,9 @@ class EdgeSim:
             ops.pullback_u(P["vis"], dx, self.phi, self.F, self.tmp_u)
             for a, t in zip(self.init_u, self.tmp_u):
                 ops.axpy(a, t, curr_dt, a)
-        if self.packed:
+        if self.variant == "efm":
+            pass  # the backtrack wrote fpsi / fcol
+        elif self.packed:
             ops.face_map_packed(self.hv, dx, self.pmaps[self.cur], self.res, self.fpsi, self.fcol)
         else:
             m = self.maps[self.cur]
@@ -261,8 +324,15 @@ class EdgeSim:
         for v, d in zip(P["vis"], P["drag"]):
             ops.axpy(v, d, 1.0, v)
 
-    def _march(self, dt, reinit):
+    def _march(self, dt, reinit, j=0):
         dx, eps = self.dx, self.ed_eps
+        if self.variant == "efm":
+            # run_efm.py:360-365: cache u, then backtrack_psi_grid(j) onto the faces
+            for a, b in zip(self.u_cache[j], self.u):
+                ops.copy(b, a)
+            self.dts[j] = float(torch.tensor(dt, dtype=torch.float32))
+            ops.efm_backtrack(self.u_cache[:j + 1], self.dts[:j + 1], dx, self.fpsi, self.fcol)
+            return
         if self.packed:
             src, dst = self.pmaps[self.cur], self.pmaps[self.cur ^ 1]
             if reinit and self.variant != "edge":
@@ -292,6 +362,21 @@ class EdgeSim:
                 ops.march_ed8(self.u, dx, dt, eps, src["psi"], src["T"], src["dT"], src["d2T"], dst["psi"],
                               dst["T"], dst["dT"], dst["d2T"])
         self.cur ^= 1
+
+
+def _detach_copy(v):
+    if torch.is_tensor(v):
+        return v.detach().clone()
+    if isinstance(v, list):
+        return [_detach_copy(x) for x in v]
+    if isinstance(v, dict):
+        return {k: _detach_copy(x) for k, x in v.items()}
+    return v
+
+
+def _copy_into(dst, src):
+    for a, b in zip(dst, src):
+        a.copy_(b)
 
 
 class _NoTimer:
@@ -410,3 +495,53 @@ def uniform_flow(res, vel, device="cuda"):
     for c in range(3):
         u[c].fill_(float(vel[c]))
     return u
+
+
+# the two ink-drop cases of sim/lp_init.py: (sphere radius, centre x, centre z,
+# cell velocity inside the sphere, particle velocity)
+_INK = {
+    0: (3.0, 64.0, 64.0, (0.0, 1.0, 0.0), (0.0, 1.0, 0.0)),                        # lp_init.py:6-35
+    1: (8.0, 128.0 * 0.3, 128.0 * 0.3, (0.2, 0.5, 0.3), (0.0, 0.0, 0.0)),          # lp_init.py:69-104
+}
+
+
+def ink_particles(case, num, domain_range_y=256.0):
+    """ink_drop_particle_case0/1 (lp_init.py:6-20, 69-86): `num` positions
+    drawn by rejection from the cube around the sphere with Python's random
+    module seeded 0, in the reference's order (so the same particles)."""
+    import random
+
+    import numpy as np
+    r, cx, cz = _INK[case][:3]
+    cy = 0.05 * domain_range_y
+    out = np.zeros((num, 3), np.float64)
+    rng = random.Random(0)
+    n = 0
+    while n < num:
+        x = rng.random() * r * 2 + cx - r
+        y = rng.random() * r * 2 + cy
+        z = rng.random() * r * 2 + cz - r
+        if (x - cx) ** 2 + (y - cy - r) ** 2 + (z - cz) ** 2 < r ** 2:
+            out[n] = (x, y, z)
+            n += 1
+    return out
+
+
+def ink_init(case, res, dx, num, laden_radius, domain_range_y=256.0, device="cuda"):
+    """ink_init_case0/1 (lp_init.py:48-66, 107-125) followed by
+    split_central_vector: face velocities (the sphere of cells moving with the
+    case's velocity), particle positions and velocities, and the per-particle
+    reference radius (compute_laden_radius for all)."""
+    import numpy as np
+    r, cx, cz, ucell, upart = _INK[case]
+    cy = 0.05 * domain_range_y
+    X = (np.indices(res).astype(np.float32) + np.float32(0.5)) * np.float32(dx)
+    inside = (X[0] - cx) ** 2 + (X[1] - cy - r) ** 2 + (X[2] - cz) ** 2 < r ** 2
+    uc = np.zeros(tuple(res) + (3,), np.float32)
+    uc[inside] = np.asarray(ucell, np.float32)
+    u = zeros_faces(res, None, device)
+    ops.split_central_vector(torch.from_numpy(uc).to(device), u)
+    pos = torch.from_numpy(ink_particles(case, num, domain_range_y).astype(np.float32)).to(device)
+    vel = torch.tensor(upart, dtype=torch.float32, device=device).expand(num, 3).contiguous()
+    rad = torch.full((num,), float(laden_radius), dtype=torch.float32, device=device)
+    return u, pos, vel, rad

@@ -151,6 +151,16 @@ int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const fl
 /* forward map on the faces, advance_map x3, run_edge.py:330-357 (in place) */
 int edge_advance_map(int nx, int ny, int nz, float dx, float dt, const float *ux, const float *uy, const float *uz,
                      float *phix, float *phiy, float *phiz, float *Fx, float *Fy, float *Fz, void *stream);
+/* EFM backward map on the faces, backtrack_psi_grid(curr_step),
+ * run_efm.py:179-186 (with reset_to_identity 153-167, march_no_neural 170-176,
+ * advance_map 194-215): from the identity, advance_map with -dts[s] through
+ * the cached velocities s = curr_step, ..., 0, all in one launch.
+ * u?_cache and dts are HOST arrays of curr_step + 1 entries (device field
+ * pointers and float step sizes); slot curr_step is the current velocity, as
+ * the reference copies it there first.  curr_step < 64. */
+int edge_efm_backtrack(int nx, int ny, int nz, float dx, int curr_step, const float *const *ux_cache,
+                       const float *const *uy_cache, const float *const *uz_cache, const float *dts, float *psix,
+                       float *psiy, float *psiz, float *Tx, float *Ty, float *Tz, void *stream);
 
 /* ---- velocity / dye transport ------------------------------------------ */
 /* advect_u_semi_lagrangian, hermite.py:1578-1621 (dt as passed; the driver

@@ -215,6 +215,19 @@ def advance_map(u, phi, F, axis, dx, dt):
     lib().orc_advance_map(*(_i(s) for s in res), _i(axis), _f(dx), _f(dt), *(_p(a) for a in u), _p(phi), _p(F))
 
 
+def efm_backtrack(u_cache, dts, dx):
+    """run_efm.py:179-186 backtrack_psi_grid(len(u_cache) - 1): the face map
+    reset to the identity, then advance_map with -dts[s] through the cached
+    velocities, newest first.  Returns (psi_faces, T_faces)."""
+    res = _res_from_u(u_cache[0])
+    psi = [face_coords(res, dx, a).astype(F32) for a in range(3)]
+    T = [np.broadcast_to(np.eye(3, dtype=F32)[a], s + (3,)).copy() for a, s in enumerate(face_shapes(res))]
+    for s in reversed(range(len(u_cache))):
+        for a in range(3):
+            advance_map(u_cache[s], psi[a], T[a], a, dx, -F32(dts[s]))
+    return psi, T
+
+
 def map_u(u0, F, phi, dx):
     """run_edge.py:361-373 map_u."""
     u0 = [_c32(a) for a in u0]
@@ -431,8 +444,10 @@ def emit_smoke(res, dx, centers, colors, radius, smoke):
 def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_clamp=True, dt=None,
                  abs_tol=1e-12, rel_tol=1e-12, variant="edge", solid=None, emitters=None, particles=None):
     """One iteration of run_edge.py:588-712 (variant "edge"), run_ed4.py:
-    402-484 ("ed4"), run_ed8.py:365-451 ("ed8") or run_ge.py:363-448 ("ge",
-    the ED8 substep with the GE march); no particles, no solids,
+    402-484 ("ed4"), run_ed8.py:365-451 ("ed8"), run_ge.py:363-448 ("ge",
+    the ED8 substep with the GE march) or run_efm.py:319-406 ("efm", the ED8
+    substep with the face map backtracked through the cached velocities); no
+    particles, no solids,
     no frame bookkeeping: dt = CFL*dx/max_speed unless given.  Returns
     (dt, iters)."""
     if variant != "edge":
@@ -542,7 +557,14 @@ def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_
         st.init_smoke = st.smoke.copy()
     st.u = advect_u_semi_lagrangian(st.u, dx, F32(0.5 * dt))
     it1 = poisson(st.u, base_level, abs_tol=abs_tol, rel_tol=rel_tol)[0]
-    if variant == "ed4":
+    if variant == "efm":
+        # run_efm.py:360-365: cache the projected velocity, backtrack the faces
+        if not hasattr(st, "u_cache"):
+            st.u_cache, st.dts = {}, {}
+        st.u_cache[j] = [a.copy() for a in st.u]
+        st.dts[j] = dt32
+        pf, tf = efm_backtrack([st.u_cache[s] for s in range(j + 1)], [st.dts[s] for s in range(j + 1)], dx)
+    elif variant == "ed4":
         st.psi, st.T = march_ed4(st.u, st.psi, st.T, dx, dt32, eps)
     elif variant == "ge":
         st.psi, st.T, st.dT, st.d2T = march_ge(st.u, st.psi, st.T, st.dT, st.d2T, dx, dt32)
@@ -556,7 +578,8 @@ def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_
         smoke_new = map_smoke_psi(HV_FD, st.init_smoke, st.psi, st.T, None, dx)
     else:
         # run_ed8.py:226-230, 410-433: psi and T on the faces, then map_u / map_smoke
-        pf, tf = split_psi_hermite(st.psi, st.T, st.dT, st.d2T, dx)
+        if variant != "efm":
+            pf, tf = split_psi_hermite(st.psi, st.T, st.dT, st.d2T, dx)
         u_new = map_u(st.init_u, tf, pf, dx)
         smoke_new = map_smoke(st.init_smoke, pf, dx)
     err_u = map_u(u_new, st.F, st.phi, dx)

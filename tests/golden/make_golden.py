@@ -1,6 +1,7 @@
 """Generate the golden vectors in tests/golden/*.npz by executing the EDGE
 reference's own Python sources (sim/*.py, util/taichi_utils.py and the step
-kernels of run_edge.py / run_ed4.py / run_ed8.py) on tiny seeded grids.
+kernels of run_edge.py / run_ed4.py / run_ed8.py / run_ge.py / run_efm.py) on
+tiny seeded grids.
 
 Taichi 1.7.3 is not installable here, so the sources run on the numpy
 emulation of the Taichi subset they use (``_taichi_emu/taichi``); it keeps
@@ -387,6 +388,49 @@ def march_ge():
          out_d2T_x=ms["d2T"][0], out_d2T_y=ms["d2T"][1], out_d2T_z=ms["d2T"][2],
          face_psi_x=Pf[0], face_psi_y=Pf[1], face_psi_z=Pf[2],
          face_T_x=Tf[0], face_T_y=Tf[1], face_T_z=Tf[2])
+
+
+@fixture
+def efm_backtrack():
+    """EFM backward map: backtrack_psi_grid (run_efm.py:179-186) through three
+    cached velocity fields with their step sizes, from the identity."""
+    rng = np.random.default_rng(606)
+    g = Grid(*G_SMALL)
+    nsteps = 3
+    cache = [velocity(rng, g, amp=0.7) for _ in range(nsteps)]
+    u_cur = [from_np(c.to_numpy()) for c in cache[-1]]  # the driver copies u into slot j before backtracking
+    dts = sfield((nsteps,))
+    dts.from_numpy(np.array([dt_for(c, g, 0.4) for c in cache], F32))
+    fx, fy, fz = g.faces()
+    psi = [vfield(fx), vfield(fy), vfield(fz)]
+    T = [vfield(fx), vfield(fy), vfield(fz)]
+    tmp = [sfield(s) for s in g.faces()]
+    ns = load_driver_kernels("run_efm.py", ["reset_to_identity", "advance_map", "march_no_neural",
+                                            "backtrack_psi_grid"], dict(
+        psi_x=psi[0], psi_y=psi[1], psi_z=psi[2], T_x=T[0], T_y=T[1], T_z=T[2],
+        u_x=u_cur[0], u_y=u_cur[1], u_z=u_cur[2], tmp_u_x=tmp[0], tmp_u_y=tmp[1], tmp_u_z=tmp[2],
+        u_x_cache=[c[0] for c in cache], u_y_cache=[c[1] for c in cache], u_z_cache=[c[2] for c in cache],
+        dts=dts, X_x=g.X_x, X_y=g.X_y, X_z=g.X_z, dx=g.dx))
+    ns["backtrack_psi_grid"](nsteps - 1)
+    out = dict(meta_dx=g.dx, res=np.array(g.res), dts=dts, out_psi_x=psi[0], out_psi_y=psi[1], out_psi_z=psi[2],
+               out_T_x=T[0], out_T_y=T[1], out_T_z=T[2])
+    for s, c in enumerate(cache):
+        for a, f in zip("xyz", c):
+            out[f"u{s}_{a}"] = f
+    save("efm_backtrack", **out)
+
+
+@fixture
+def lp_init_positions():
+    """Laden-particle initial positions of the ink cases (lp_init.py:6-20,
+    69-86): the reference's seeded rejection sampling, 300 particles each."""
+    import sim.lp_init as LPI
+    out = {}
+    for case, fn in ((0, LPI.ink_drop_particle_case0), (1, LPI.ink_drop_particle_case1)):
+        pos = ti.Vector.field(3, float, shape=(300,))
+        fn(pos, 300)
+        out[f"pos_case{case}"] = pos
+    save("lp_init_positions", **out)
 
 
 @fixture

@@ -420,3 +420,34 @@ def test_dropin_hermite_marches():
         for i, a in enumerate("xyz"):
             assert rel_l2(N_(T[i]), d["out_T_" + a]) < TOL_T, name
             assert rel_l2(N_(dT[i]), d["out_dT_" + a]) < TOL_DT, name
+
+
+def test_efm_backtrack(ops):
+    """EFM backward face map through cached velocities: against the
+    reference's backtrack_psi_grid, and against the oracle at 48x32x24 with
+    twelve cached steps (one launch for the whole chain)."""
+    d = load_golden("efm_backtrack")
+    n = len(d["dts"])
+    res = tuple(int(v) for v in d["res"])
+    cache = [[T_(d[f"u{s}_{a}"]) for a in "xyz"] for s in range(n)]
+    psi = [torch.empty(s + (3,), device="cuda") for s in O.face_shapes(res)]
+    T = [torch.empty(s + (3,), device="cuda") for s in O.face_shapes(res)]
+    ops.efm_backtrack(cache, [float(x) for x in d["dts"]], float(d["meta_dx"]), psi, T)
+    for i, a in enumerate("xyz"):
+        assert rel_l2(N_(psi[i]), d["out_psi_" + a]) < TOL
+        assert rel_l2(N_(T[i]), d["out_T_" + a]) < TOL
+    rng = np.random.default_rng(77)
+    res = (48, 32, 24)
+    dx = 1.0 / 32
+    cache = []
+    for s in range(12):
+        cache.append([(0.6 * np.sin(np.indices(sh)[0] * 0.2 + a + 0.1 * s) * np.cos(np.indices(sh)[1] * 0.15)
+                       + 0.05 * rng.normal(size=sh)).astype(np.float32) for a, sh in enumerate(O.face_shapes(res))])
+    dts = [np.float32(0.4 * dx / 0.7) for _ in cache]
+    opsi, oT = O.efm_backtrack(cache, dts, dx)
+    psi = [torch.empty(s + (3,), device="cuda") for s in O.face_shapes(res)]
+    T = [torch.empty(s + (3,), device="cuda") for s in O.face_shapes(res)]
+    ops.efm_backtrack([[T_(a) for a in c] for c in cache], [float(x) for x in dts], dx, psi, T)
+    for i in range(3):
+        assert rel_l2(N_(psi[i]), opsi[i]) < TOL
+        assert rel_l2(N_(T[i]), oT[i]) < 1e-4

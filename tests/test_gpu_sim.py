@@ -39,7 +39,7 @@ def test_edge_steps_golden():
 
 
 @pytest.mark.parametrize("packed", [False, True])
-@pytest.mark.parametrize("variant", ["edge", "ed4", "ed8", "ge"])
+@pytest.mark.parametrize("variant", ["edge", "ed4", "ed8", "ge", "efm"])
 def test_steps_vs_oracle(variant, packed):
     from edgeb200.sim import EdgeSim, leapfrog_init
     res = (32, 16, 16)
@@ -55,7 +55,12 @@ def test_steps_vs_oracle(variant, packed):
         for c in range(3):
             assert rel_l2(N_(sim.u[c]), st.u[c]) < 5e-4, (variant, i, c)
         assert rel_l2(N_(sim.smoke), st.smoke) < 5e-4, (variant, i)
-        assert rel_l2(N_(sim.map["psi"]), st.psi) < 1e-5
+        if variant == "efm":
+            for c in range(3):  # the backtracked face map
+                assert rel_l2(N_(sim.fpsi[c]), O.efm_backtrack(
+                    [st.u_cache[s] for s in range(i % 3 + 1)], [st.dts[s] for s in range(i % 3 + 1)], dx)[0][c]) < 1e-5
+        else:
+            assert rel_l2(N_(sim.map["psi"]), st.psi) < 1e-5
 
 
 def test_solid_emitter_steps_vs_oracle():
@@ -112,3 +117,34 @@ def test_particle_coupled_steps_vs_oracle():
         for c in range(3):
             assert rel_l2(N_(sim.u[c]), st.u[c]) < 1e-3, (i, c)
             assert rel_l2(N_(sim.particles["vis"][c]), P["vis"][c]) < 1e-3, (i, c)
+
+
+@pytest.mark.parametrize("variant,packed", [("edge", True), ("ed8", False), ("efm", False)])
+def test_state_dict_resume_is_exact(variant, packed):
+    """Saving the state in the middle of a reinitialisation interval and
+    loading it into a fresh simulation continues bit for bit."""
+    from edgeb200.sim import EdgeSim, leapfrog_init
+    res = (32, 16, 16)
+    dx = 1.0 / 16
+    u, smoke = leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.06, circulation=0.2, num_samples=200)
+
+    def make():
+        s = EdgeSim(res, dx, variant=variant, reinit_every=4, base_level=2, visualize_dt=0.05, packed=packed)
+        s.set_velocity(*u)
+        s.set_smoke(smoke)
+        return s
+
+    a = make()
+    for _ in range(2):
+        a.step()
+    state = a.state_dict()
+    for _ in range(3):
+        a.step()
+    b = make()
+    b.load_state_dict(state)
+    for _ in range(3):
+        b.step()
+    for c in range(3):
+        assert torch.equal(a.u[c], b.u[c])
+    assert torch.equal(a.smoke, b.smoke)
+    assert (a.i, a.frame_idx, a.sub_t) == (b.i, b.frame_idx, b.sub_t)

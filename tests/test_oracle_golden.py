@@ -106,6 +106,16 @@ def test_march_ge_and_split():
         assert rel_l2(tf[i], d["face_T_" + a]) < TOL
 
 
+def test_efm_backtrack():
+    d = load_golden("efm_backtrack")
+    nsteps = len(d["dts"])
+    cache = [[d[f"u{s}_{a}"] for a in "xyz"] for s in range(nsteps)]
+    psi, T = O.efm_backtrack(cache, d["dts"], float(d["meta_dx"]))
+    for i, a in enumerate("xyz"):
+        assert rel_l2(psi[i], d["out_psi_" + a]) < TOL
+        assert rel_l2(T[i], d["out_T_" + a]) < TOL
+
+
 def test_face_kernels():
     d = load_golden("advect_faces")
     u = [d["u_x"], d["u_y"], d["u_z"]]
