@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(128) k_march_edge(Mac mac, MapF m, float dt, f
 // EDGE march on the packed layout (same algorithm as k_march_edge); output
 // planes 0-6 of `out` (n cells per plane).
 template <bool IDENT>
-__global__ void __launch_bounds__(128) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+__global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
     if (e >= n) return;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(128) k_march_edge_p(Mac mac, MapP m, float dt,
             }
         } else {
             float val[3], G[3][3];
-            hermite3p<HV_GARM, true>(m, P, val, G);
+            hermite3p<HV_GARM_P, true>(m, P, val, G);
             for (int r = 0; r < 3; r++)
                 for (int d = 0; d < 3; d++) T[r][d] = G[r][0] * C[d][0] + G[r][1] * C[d][1] + G[r][2] * C[d][2];
             for (int c = 0; c < 3; c++) P[c] = val[c];
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(128) k_march_ed4_p(Mac mac, MapP m, float dt, 
         for (int c = 0; c < 3; c++) p[c] = X[c] + c_ed4_off[q][c] * eps;
         rk4_pos(mac, p, -dt);
         float v[3];
-        hermite3p<HV_FD, false>(m, p, v, nullptr);
+        hermite3p<HV_FD_P, false>(m, p, v, nullptr);
         for (int c = 0; c < 3; c++) P[q][c] = v[c];
     }
     float o[4][3];
@@ -457,9 +457,74 @@ __global__ void k_fd3_d2T_p(int nx, int ny, int nz, float dx, float4* __restrict
     g[(size_t)7 * n + e] = f4div(s, 6.0f, dx);
 }
 
-// face map on the packed layout
+// The derived planes of a packed ED4 (V = HV_FD: planes 4-7) or EDGE
+// (V = HV_GARM: plane 7) map: the finite-difference Hermite coefficients of
+// each cell as a corner (hcoef_p's expressions with the cell's +-1 neighbours
+// clamped to the grid), before their final multiplications by dx, which the
+// evaluation applies; so they do not depend on dx and the evaluation's
+// coefficients are bit for bit the ones hcoef_p forms.
 template <int V>
-__global__ void __launch_bounds__(128) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
+__global__ void k_coef_p(MapP m, float4* __restrict__ g) {
+    const int n = m.n, n1 = m.ny, n2 = m.nz;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int kk = e % m.nz, jj = (e / m.nz) % m.ny, ii = e / (m.ny * m.nz);
+    const int im = max(ii - 1, 0), ip = min(ii + 1, m.nx - 1), jm = max(jj - 1, 0), jp = min(jj + 1, m.ny - 1);
+    const int km = max(kk - 1, 0), kp = min(kk + 1, m.nz - 1);
+    float o[4][3];
+    if (V == HV_FD) {
+        // hermite.py:104-148
+        const int ekp = idx3(ii, jj, kp, n1, n2), ekm = idx3(ii, jj, km, n1, n2);
+        const int ejp = idx3(ii, jp, kk, n1, n2), ejm = idx3(ii, jm, kk, n1, n2);
+        const int eip = idx3(ip, jj, kk, n1, n2), eim = idx3(im, jj, kk, n1, n2);
+        float4 kp1 = ldp(m, 2, ekp), km1 = ldp(m, 2, ekm), kp0 = ldp(m, 1, ekp), km0 = ldp(m, 1, ekm);
+        float4 jp2 = ldp(m, 3, ejp), jm2 = ldp(m, 3, ejm), jp0 = ldp(m, 1, ejp), jm0 = ldp(m, 1, ejm);
+        float4 ip2 = ldp(m, 3, eip), im2 = ldp(m, 3, eim), ip1 = ldp(m, 2, eip), im1 = ldp(m, 2, eim);
+        float4 a30 = ldp(m, 2, idx3(ip, jj, kp, n1, n2)), b30 = ldp(m, 2, idx3(ip, jj, km, n1, n2));
+        float4 c30 = ldp(m, 3, idx3(ip, jp, kk, n1, n2)), d30 = ldp(m, 3, idx3(ip, jm, kk, n1, n2));
+        float4 a31 = ldp(m, 2, idx3(im, jj, kp, n1, n2)), b31 = ldp(m, 2, idx3(im, jj, km, n1, n2));
+        float4 c31 = ldp(m, 3, idx3(im, jp, kk, n1, n2)), d31 = ldp(m, 3, idx3(im, jm, kk, n1, n2));
+        float4 a32 = ldp(m, 1, idx3(ii, jp, kp, n1, n2)), b32 = ldp(m, 1, idx3(ii, jp, km, n1, n2));
+        float4 c32 = ldp(m, 3, idx3(ip, jp, kk, n1, n2)), d32 = ldp(m, 3, idx3(im, jp, kk, n1, n2));
+        float4 a33 = ldp(m, 1, idx3(ii, jm, kp, n1, n2)), b33 = ldp(m, 1, idx3(ii, jm, km, n1, n2));
+        float4 c33 = ldp(m, 3, idx3(ip, jm, kk, n1, n2)), d33 = ldp(m, 3, idx3(im, jm, kk, n1, n2));
+        float4 a34 = ldp(m, 1, idx3(ii, jp, kp, n1, n2)), b34 = ldp(m, 1, idx3(ii, jm, kp, n1, n2));
+        float4 c34 = ldp(m, 2, idx3(ip, jj, kp, n1, n2)), d34 = ldp(m, 2, idx3(im, jj, kp, n1, n2));
+        float4 a35 = ldp(m, 1, idx3(ii, jp, km, n1, n2)), b35 = ldp(m, 1, idx3(ii, jm, km, n1, n2));
+        float4 c35 = ldp(m, 2, idx3(ip, jj, km, n1, n2)), d35 = ldp(m, 2, idx3(im, jj, km, n1, n2));
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            o[0][c] = ((c4(kp1, c) - c4(km1, c)) + (c4(jp2, c) - c4(jm2, c))) / 4.0f;
+            o[1][c] = ((c4(kp0, c) - c4(km0, c)) + (c4(ip2, c) - c4(im2, c))) / 4.0f;
+            o[2][c] = ((c4(jp0, c) - c4(jm0, c)) + (c4(ip1, c) - c4(im1, c))) / 4.0f;
+            float v30 = ((c4(a30, c) - c4(b30, c)) + (c4(c30, c) - c4(d30, c))) / 4.0f;
+            float v31 = ((c4(a31, c) - c4(b31, c)) + (c4(c31, c) - c4(d31, c))) / 4.0f;
+            float v32 = ((c4(a32, c) - c4(b32, c)) + (c4(c32, c) - c4(d32, c))) / 4.0f;
+            float v33 = ((c4(a33, c) - c4(b33, c)) + (c4(c33, c) - c4(d33, c))) / 4.0f;
+            float v34 = ((c4(a34, c) - c4(b34, c)) + (c4(c34, c) - c4(d34, c))) / 4.0f;
+            float v35 = ((c4(a35, c) - c4(b35, c)) + (c4(c35, c) - c4(d35, c))) / 4.0f;
+            o[3][c] = (v30 - v31 + v32 - v33 + v34 - v35) / 6.0f;
+        }
+        g[(size_t)4 * n + e] = make_float4(o[0][0], o[0][1], o[0][2], 0.f);
+        g[(size_t)5 * n + e] = make_float4(o[1][0], o[1][1], o[1][2], 0.f);
+        g[(size_t)6 * n + e] = make_float4(o[2][0], o[2][1], o[2][2], 0.f);
+    } else {
+        // hermite.py:346-351
+        float4 xp = ldp(m, 4, idx3(ip, jj, kk, n1, n2)), xm = ldp(m, 4, idx3(im, jj, kk, n1, n2));
+        float4 yp = ldp(m, 5, idx3(ii, jp, kk, n1, n2)), ym = ldp(m, 5, idx3(ii, jm, kk, n1, n2));
+        float4 zp = ldp(m, 6, idx3(ii, jj, kp, n1, n2)), zm = ldp(m, 6, idx3(ii, jj, km, n1, n2));
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            o[3][c] = ((c4(xp, c) - c4(xm, c)) + (c4(yp, c) - c4(ym, c)) + (c4(zp, c) - c4(zm, c))) / 6.0f;
+    }
+    g[(size_t)7 * n + e] = make_float4(o[3][0], o[3][1], o[3][2], 0.f);
+}
+
+// face map on the packed layout
+// (ED4 / EDGE: at most 128 registers, 4 CTAs per SM, measured faster than
+// the unbounded build; the ED8 form needs fewer registers unbounded)
+template <int V>
+__global__ void __launch_bounds__(128, V == HV_FULL ? 1 : 4) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
                                                     float* fcy, float* fcz) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(m.nx, m.ny, m.nz)) return;
@@ -471,7 +536,7 @@ __global__ void __launch_bounds__(128) k_face_map_p(MapP m, float* fpx, float* f
     float* fc = f.axis == 0 ? fcx : (f.axis == 1 ? fcy : fcz);
     for (int c = 0; c < 3; c++) {
         fp[3 * f.e + c] = val[c];
-        fc[3 * f.e + c] = G[c][f.axis];
+        fc[3 * f.e + c] = sel3(G[c], f.axis);
     }
 }
 
@@ -593,7 +658,7 @@ __global__ void __launch_bounds__(128) k_face_map(MapF m, float* fpx, float* fpy
     float* fc = f.axis == 0 ? fcx : (f.axis == 1 ? fcy : fcz);
     for (int c = 0; c < 3; c++) {
         fp[3 * f.e + c] = val[c];
-        fc[3 * f.e + c] = G[c][f.axis];
+        fc[3 * f.e + c] = sel3(G[c], f.axis);
     }
 }
 
@@ -671,11 +736,14 @@ __global__ void __launch_bounds__(128) k_advect_sl(Mac mac, float dt, float* ox,
     for (int c = 0; c < 3; c++) q[c] = p1[c] - (v1[c] + 2.0f * v2[c] + 2.0f * v3[c] + v4[c]) / 6.0f * dt;
     mac_sample<false>(mac, q, v5, nullptr);
     float* o = f.axis == 0 ? ox : (f.axis == 1 ? oy : oz);
-    o[f.e] = v5[f.axis];
+    o[f.e] = sel3(v5, f.axis);
 }
 
 struct Face3 {
     const float* p[3];
+    // select with constant indices only: a run-time index into a kernel
+    // parameter array makes the compiler copy the parameter to local memory
+    EDGE_D const float* at(int a) const { return a == 0 ? p[0] : (a == 1 ? p[1] : p[2]); }
 };
 
 // map_u / map_u_psi pullback with fused BFECC arithmetic (edge_pullback_u)
@@ -684,14 +752,14 @@ __global__ void __launch_bounds__(256) k_pullback_u(Mac mac, Face3 pos, Face3 co
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
     FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
-    const float* P = pos.p[f.axis] + 3 * f.e;
-    const float* Cc = col.p[f.axis] + 3 * f.e;
+    const float* P = pos.at(f.axis) + 3 * f.e;
+    const float* Cc = col.at(f.axis) + 3 * f.e;
     float p[3] = {__ldg(P), __ldg(P + 1), __ldg(P + 2)};
     float v[3];
     mac_sample<false>(mac, p, v, nullptr);
     float out = __ldg(Cc) * v[0] + __ldg(Cc + 1) * v[1] + __ldg(Cc + 2) * v[2];
-    if (init.p[f.axis]) out = scale * (out - __ldg(init.p[f.axis] + f.e));
-    if (sub.p[f.axis]) out = __ldg(sub.p[f.axis] + f.e) - out;
+    if (init.at(f.axis)) out = scale * (out - __ldg(init.at(f.axis) + f.e));
+    if (sub.at(f.axis)) out = __ldg(sub.at(f.axis) + f.e) - out;
     float* o = f.axis == 0 ? ox : (f.axis == 1 ? oy : oz);
     o[f.e] = out;
 }
@@ -706,7 +774,7 @@ __global__ void __launch_bounds__(128) k_map_u_psi(Mac mac, MapF m, float* ox, f
     face_pos(f.axis, f.i, f.j, f.k, m.dx, X);
     hermite3<V, true>(m, X, P, G);
     mac_sample<false>(mac, P, v, nullptr);
-    float out = G[0][f.axis] * v[0] + G[1][f.axis] * v[1] + G[2][f.axis] * v[2];
+    float out = sel3(G[0], f.axis) * v[0] + sel3(G[1], f.axis) * v[1] + sel3(G[2], f.axis) * v[2];
     float* o = f.axis == 0 ? ox : (f.axis == 1 ? oy : oz);
     o[f.e] = out;
 }
@@ -791,7 +859,7 @@ __global__ void k_clamp_u(int nx, int ny, int nz, Face3 u, Face3 u1, float* ox, 
     if (t >= n_faces(nx, ny, nz)) return;
     FaceIdx f = face_decompose(t, nx, ny, nz);
     int n0 = nx + (f.axis == 0), n1 = ny + (f.axis == 1), n2 = nz + (f.axis == 2);
-    const float* a = u1.p[f.axis];
+    const float* a = u1.at(f.axis);
     int im = max(f.i - 1, 0), ip = min(f.i + 1, n0 - 1);
     int jm = max(f.j - 1, 0), jp = min(f.j + 1, n1 - 1);
     int km = max(f.k - 1, 0), kp = min(f.k + 1, n2 - 1);
@@ -801,7 +869,7 @@ __global__ void k_clamp_u(int nx, int ny, int nz, Face3 u, Face3 u1, float* ox, 
     float mx = fmaxf(fmaxf(fmaxf(fmaxf(fmaxf(l, r), b), tt), aa), cc);
     float mn = fminf(fminf(fminf(fminf(fminf(l, r), b), tt), aa), cc);
     float* o = f.axis == 0 ? ox : (f.axis == 1 ? oy : oz);
-    o[f.e] = fminf(fmaxf(__ldg(u.p[f.axis] + f.e), mn), mx);
+    o[f.e] = fminf(fmaxf(__ldg(u.at(f.axis) + f.e), mn), mx);
 }
 
 __global__ void k_set_float(float* p, float v) { *p = v; }
@@ -911,9 +979,8 @@ __global__ void k_split_central(int nx, int ny, int nz, const float* __restrict_
     if (t >= n_faces(nx, ny, nz)) return;
     FaceIdx f = face_decompose(t, nx, ny, nz);
     int hi[3] = {min(f.i, nx - 1), min(f.j, ny - 1), min(f.k, nz - 1)};
-    int lo[3] = {hi[0], hi[1], hi[2]};
-    int I[3] = {f.i, f.j, f.k};
-    lo[f.axis] = max(I[f.axis] - 1, 0);
+    int lo[3] = {f.axis == 0 ? max(f.i - 1, 0) : hi[0], f.axis == 1 ? max(f.j - 1, 0) : hi[1],
+                 f.axis == 2 ? max(f.k - 1, 0) : hi[2]};
     float r = vc[3 * idx3(hi[0], hi[1], hi[2], ny, nz) + f.axis];
     float l = vc[3 * idx3(lo[0], lo[1], lo[2], ny, nz) + f.axis];
     float* o = f.axis == 0 ? ux : (f.axis == 1 ? uy : uz);
@@ -1131,6 +1198,14 @@ static int planes_of(int variant) {
     return variant == HV_FD ? kPlanesED4 : (variant == HV_GARM ? kPlanesEDGE : (variant == HV_FULL ? kPlanesED8 : -1));
 }
 
+// fill the derived coefficient planes of a packed ED4 / EDGE map
+static void derive_planes(int variant, int nx, int ny, int nz, float* packed, cudaStream_t st) {
+    MapP m = make_mapp(packed, nx, ny, nz, 1.0f);
+    int n = nx * ny * nz;
+    if (variant == HV_FD) k_coef_p<HV_FD><<<grid_for(n), kBlock, 0, st>>>(m, (float4*)packed);
+    else if (variant == HV_GARM) k_coef_p<HV_GARM><<<grid_for(n), kBlock, 0, st>>>(m, (float4*)packed);
+}
+
 int edge_map_pack(int variant, int nx, int ny, int nz, const float* psi, const float* Tx, const float* Ty,
                   const float* Tz, const float* dTx, const float* dTy, const float* dTz, const float* d2Tx,
                   const float* d2Ty, const float* d2Tz, float* packed, void* stream) {
@@ -1142,8 +1217,11 @@ int edge_map_pack(int variant, int nx, int ny, int nz, const float* psi, const f
     int n = nx * ny * nz;
     k_map_pack<<<grid_for(n), kBlock, 0, S(stream)>>>(n, pl, psi, Tx, Ty, Tz, dTx, dTy, dTz, d2Tx, d2Ty, d2Tz,
                                                       (float4*)packed);
+    derive_planes(variant, nx, ny, nz, packed, S(stream));
     return launch_status();
 }
+
+int edge_packed_planes(int variant) { return planes_of(variant) < 0 ? EDGE_EINVAL : kPlanesStored; }
 
 int edge_map_unpack(int variant, int nx, int ny, int nz, const float* packed, float* psi, float* Tx, float* Ty,
                     float* Tz, float* dTx, float* dTy, float* dTz, float* d2Tx, float* d2Ty, float* d2Tz,
@@ -1180,6 +1258,7 @@ int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, f
     } else {
         k_march_ed8_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
     }
+    derive_planes(variant, nx, ny, nz, out_packed, S(stream));
     return launch_status();
 }
 
@@ -1191,8 +1270,8 @@ int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const fl
     if (!al16(packed)) return EDGE_EALIGN;
     MapP m = make_mapp(packed, nx, ny, nz, dx);
     int g = grid_for(n_faces(nx, ny, nz), 128);
-    if (variant == HV_FD) k_face_map_p<HV_FD><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
-    else if (variant == HV_GARM) k_face_map_p<HV_GARM><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
+    if (variant == HV_FD) k_face_map_p<HV_FD_P><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
+    else if (variant == HV_GARM) k_face_map_p<HV_GARM_P><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
     else k_face_map_p<HV_FULL><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
     return launch_status();
 }

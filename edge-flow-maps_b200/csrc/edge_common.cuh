@@ -25,6 +25,9 @@ namespace edge {
 static inline float clamp_bound(int dim, int minus) { return (float)((double)(dim - minus) - 1e-6); }
 
 EDGE_HD int idx3(int i, int j, int k, int n1, int n2) { return (i * n1 + j) * n2 + k; }
+// v[a] with constant indices only (a run-time index into a register array
+// or a kernel-parameter array puts it in local memory)
+EDGE_D float sel3(const float v[3], int a) { return a == 0 ? v[0] : (a == 1 ? v[1] : v[2]); }
 EDGE_D int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // ---------------------------------------------------------------------------
@@ -403,9 +406,21 @@ EDGE_D void hermite3(const MapF& m, const float p[3], float val[3], float grad[3
 //   planes 4..6: psi_yz, psi_xz, psi_xy               (EDGE dT, ED8 dT)
 //   plane 7: psi_xyz                                   (ED8 d2T)
 // One 128-bit load then serves all three components of a Hermite stencil
-// point.
+// point.  The ED4 and EDGE maps carry fewer state planes (4 and 7); their
+// remaining planes hold the Hermite coefficients the reference derives by
+// finite differences at every evaluation (ED4: the fgg, gfg, ggf, ggg terms
+// from the gradient, hermite.py:104-148; EDGE: the ggg term from the mixed
+// derivatives, hermite.py:346-351), computed once per map by k_coef_p up to
+// their final multiplications by dx, which the evaluation applies.  The
+// corners a Hermite evaluation visits are cells 1..n-1 of each axis and the
+// reference's neighbour indices there are the cell's own +-1 clamped to the
+// grid, so a per-cell table with clamped neighbours holds exactly the values
+// the reference computes per corner.  Every packed map is 8 planes.
 // ---------------------------------------------------------------------------
-constexpr int kPlanesED4 = 4, kPlanesEDGE = 7, kPlanesED8 = 8;
+constexpr int kPlanesED4 = 4, kPlanesEDGE = 7, kPlanesED8 = 8;  // state planes
+constexpr int kPlanesStored = 8;
+// internal variants: ED4 / EDGE Hermite reading the precomputed planes
+constexpr int HV_FD_P = 3, HV_GARM_P = 4;
 
 struct MapP {
     const float4* __restrict__ g;  // planes, plane q at g + q * n
@@ -443,7 +458,16 @@ EDGE_D void hcoef_p(const MapP& m, int ii, int jj, int kk, int im, int ip, int j
         t[c][2] = c4(G1, c) * dx;
         t[c][1] = c4(G2, c) * dx;
     }
-    if (VARIANT == HV_FD) {
+    if (VARIANT == HV_FD_P) {
+        float4 A = ldp(m, 4, e), B = ldp(m, 5, e), C = ldp(m, 6, e), D = ldp(m, 7, e);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            t[c][3] = c4(A, c) * dx;
+            t[c][5] = c4(B, c) * dx;
+            t[c][6] = c4(C, c) * dx;
+            t[c][7] = c4(D, c) * dx;
+        }
+    } else if (VARIANT == HV_FD) {
         // hermite.py:104-148: FD of the stored gradient (plane 1+d = d psi/dx_d)
         const int ekp = idx3(ii, jj, kp, n1, n2), ekm = idx3(ii, jj, km, n1, n2);
         const int ejp = idx3(ii, jp, kk, n1, n2), ejm = idx3(ii, jm, kk, n1, n2);
@@ -479,7 +503,11 @@ EDGE_D void hcoef_p(const MapP& m, int ii, int jj, int kk, int im, int ip, int j
         }
     } else {
         float4 D0 = ldp(m, 4, e), D1 = ldp(m, 5, e), D2 = ldp(m, 6, e);
-        if (VARIANT == HV_GARM) {
+        if (VARIANT == HV_GARM_P) {
+            float4 X3 = ldp(m, 7, e);
+#pragma unroll
+            for (int c = 0; c < 3; c++) t[c][7] = c4(X3, c) * dx * dx;
+        } else if (VARIANT == HV_GARM) {
             float4 xp = ldp(m, 4, idx3(ip, jj, kk, n1, n2)), xm = ldp(m, 4, idx3(im, jj, kk, n1, n2));
             float4 yp = ldp(m, 5, idx3(ii, jp, kk, n1, n2)), ym = ldp(m, 5, idx3(ii, jm, kk, n1, n2));
             float4 zp = ldp(m, 6, idx3(ii, jj, kp, n1, n2)), zm = ldp(m, 6, idx3(ii, jj, km, n1, n2));

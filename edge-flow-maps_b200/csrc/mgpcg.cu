@@ -89,7 +89,21 @@ struct G {  // what every solver kernel needs
     cudaGraphConditionalHandle cond;
     int use_cond;  // 0: kernels run outside a graph (eager mode), no loop condition
     int bt[6];
+    int walls;     // bit b set when bt[b] == 2 (device code tests bits: a pointer
+                   // into or a run-time index of a kernel-parameter array makes
+                   // the compiler copy the parameter struct to local memory)
 };
+
+// x[i] of a two-entry parameter array with only constant indices
+template <class T>
+EDGE_D T pick(const T (&a)[2], int i) { return i ? a[1] : a[0]; }
+template <class T>
+EDGE_D T pick2(const T (&a)[2][2], int i, int j) {
+    return i ? (j ? a[1][1] : a[1][0]) : (j ? a[0][1] : a[0][0]);
+}
+template <class T>
+EDGE_D T pick3(const T (&a)[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
+EDGE_D bool wall(int walls, int side) { return (walls >> side) & 1; }
 
 struct Fine {  // fine-level CG vectors
     float* x[2];
@@ -135,14 +149,14 @@ EDGE_D Slot slot_of(const LV& L, int t) {
 
 // num_fluid_neighbors of the plain solver (mgpcg.py:100-110)
 template <class LV>
-EDGE_D float nf_walls(const int* bt, const LV& L, int i, int j, int k) {
+EDGE_D float nf_walls(int walls, const LV& L, int i, int j, int k) {
     float num = 6.0f;
-    if (i <= 0 && bt[0] == 2) num -= 1.0f;
-    if (i >= L.n0 - 1 && bt[1] == 2) num -= 1.0f;
-    if (j <= 0 && bt[2] == 2) num -= 1.0f;
-    if (j >= L.n1 - 1 && bt[3] == 2) num -= 1.0f;
-    if (k <= 0 && bt[4] == 2) num -= 1.0f;
-    if (k >= L.n2 - 1 && bt[5] == 2) num -= 1.0f;
+    if (i <= 0 && wall(walls, 0)) num -= 1.0f;
+    if (i >= L.n0 - 1 && wall(walls, 1)) num -= 1.0f;
+    if (j <= 0 && wall(walls, 2)) num -= 1.0f;
+    if (j >= L.n1 - 1 && wall(walls, 3)) num -= 1.0f;
+    if (k <= 0 && wall(walls, 4)) num -= 1.0f;
+    if (k >= L.n2 - 1 && wall(walls, 5)) num -= 1.0f;
     return num;
 }
 
@@ -154,8 +168,8 @@ EDGE_D unsigned range_code(const LV& L, int i, int j, int k) {
 }
 
 template <bool SOLID, class LV>
-EDGE_D float nf_of(const int* bt, const LV& L, unsigned code, int i, int j, int k) {
-    return SOLID ? (float)(code >> 8) : nf_walls(bt, L, i, j, k);
+EDGE_D float nf_of(int walls, const LV& L, unsigned code, int i, int j, int k) {
+    return SOLID ? (float)(code >> 8) : nf_walls(walls, L, i, j, k);
 }
 
 // neighbour_sum (mgpcg.py:86-99, mgpcg_solid.py:99-111) in the reference's
@@ -243,7 +257,7 @@ template <class ZT, class LV>
 EDGE_D float parent_zg(const LV& C, int i, int j, int k) {
     int I = i >> 1, J = j >> 1, K = k >> 1;
     int e = (I * C.n1 + J) * C.H + (K >> 1);
-    return Zs<ZT>::ld(C.z[(I + J + K) & 1], e);
+    return Zs<ZT>::ld(pick(C.z, (I + J + K) & 1), e);
 }
 
 // ---------------------------------------------------------------------------
@@ -346,7 +360,7 @@ struct Faces {
 __global__ void k_apply_walls(G g, int nx, int ny, int nz, Faces U) {
     count_launch(g.st);
     const int side = blockIdx.y;
-    if (g.bt[side] != 2) return;
+    if (!wall(g.walls, side)) return;
     const int a = side >> 1, hi = side & 1;
     const int d1 = a == 0 ? ny : nx;  // the plane's two axes, in order
     const int d2 = a == 2 ? ny : nz;
@@ -356,7 +370,7 @@ __global__ void k_apply_walls(G g, int nx, int ny, int nz, Faces U) {
         if (a == 0) e = idx3(hi ? nx : 0, u, w, ny, nz);
         else if (a == 1) e = idx3(u, hi ? ny : 0, w, ny + 1, nz);
         else e = idx3(u, w, hi ? nz : 0, ny, nz + 1);
-        U.u[a][e] = 0.0f;
+        pick3(U.u, a)[e] = 0.0f;
     }
 }
 
@@ -410,7 +424,7 @@ __global__ void __launch_bounds__(256) k_setup_rhs(G g, Lvl L, Fine f, Faces U, 
             }
             f.div[e] = d;
             float r = d * -1.0f;
-            L.r[c0 ^ h][t] = r;
+            pick(L.r, c0 ^ h)[t] = r;
             if (fl) {
                 v[0] += d;
                 v[1] += 1.0;
@@ -458,12 +472,12 @@ __global__ void __launch_bounds__(256) k_solid_fix(G g, Lvl L, Fine f) {
             const int k = 2 * s.kk + h;
             if (k >= L.n2) break;
             const int e = idx3(s.i, s.j, k, L.n1, L.n2);
-            float r = L.r[c0 ^ h][t];
+            float r = pick(L.r, c0 ^ h)[t];
             if (fix && L.bm[e] <= 0) {
                 float d = f.div[e] - avg;
                 f.div[e] = d;
                 r = d * -1.0f;
-                L.r[c0 ^ h][t] = r;
+                pick(L.r, c0 ^ h)[t] = r;
             }
             v[0] += r;
         }
@@ -513,19 +527,19 @@ __global__ void __launch_bounds__(256) k_codes(G g, Lvl L) {
             bool dn_solid = has_dn && solid(dn[0], dn[1], dn[2]);
             if (has_up && !up_solid) code |= 1u << (2 * a);
             if (has_dn && !dn_solid) code |= 2u << (2 * a);
-            if (!has_dn && g.bt[2 * a] == 2) num -= 1;
+            if (!has_dn && wall(g.walls, 2 * a)) num -= 1;
             else if (dn_solid) num -= 1;
-            if (!has_up && g.bt[2 * a + 1] == 2) num -= 1;
+            if (!has_up && wall(g.walls, 2 * a + 1)) num -= 1;
             else if (up_solid) num -= 1;
         }
         code |= (unsigned)num << 8;
-        L.code[(i + j + k) & 1][(i * n1 + j) * L.H + (k >> 1)] = (unsigned short)code;
+        pick(L.code, (i + j + k) & 1)[(i * n1 + j) * L.H + (k >> 1)] = (unsigned short)code;
     }
 }
 
 template <bool SOLID>
 EDGE_D unsigned code_at(const Lvl& L, int plane, int e, int i, int j, int k) {
-    return SOLID ? (unsigned)L.code[plane][e] : range_code(L, i, j, k);
+    return SOLID ? (unsigned)pick(L.code, plane)[e] : range_code(L, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -561,18 +575,18 @@ __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
             const unsigned code = code_at<SOLID>(L, pl, t, s.i, s.j, k);
             float pe = 0.0f;
             if (code & CELL_FLUID) {
-                const float* __restrict__ zo = L.z[pl ^ 1];
-                const float* __restrict__ po = f.p[pc][pl ^ 1];
-                const float zt = Zs<ZT>::ld(L.z[pl], t);
-                pe = first ? zt : __fadd_rn(zt, __fmul_rn(beta, __ldg(f.p[pc][pl] + t)));
+                const float* __restrict__ zo = pick(L.z, pl ^ 1);
+                const float* __restrict__ po = pick2(f.p, pc, pl ^ 1);
+                const float zt = Zs<ZT>::ld(pick(L.z, pl), t);
+                pe = first ? zt : __fadd_rn(zt, __fmul_rn(beta, __ldg(pick2(f.p, pc, pl) + t)));
                 float ns = nbr_sum(L, code, t, k, [&](int e, int) {
                     const float ze = Zs<ZT>::ld(zo, e);
                     return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e)));
                 });
-                float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, L, code, s.i, s.j, k), pe), ns);
+                float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.walls, L, code, s.i, s.j, k), pe), ns);
                 v[0] += (double)pe * (double)ape;
             }
-            f.p[pc ^ 1][pl][t] = pe;
+            pick2(f.p, pc ^ 1, pl)[t] = pe;
         }
     }
     if (last_block<1>(g, 2, v)) {
@@ -608,20 +622,20 @@ __global__ void __launch_bounds__(256) k_cg_xr(G g, Lvl L, Fine f) {
             const int k = 2 * s.kk + h, pl = c0 ^ h;
             if (k >= L.n2) break;
             const unsigned code = code_at<SOLID>(L, pl, t, s.i, s.j, k);
-            float r = L.r[pl][t] - mean;
-            float* xp = f.x[pl] + t;
+            float r = pick(L.r, pl)[t] - mean;
+            float* xp = pick(f.x, pl) + t;
             if (code & CELL_FLUID) {
-                const float* __restrict__ po = f.p[pc][pl ^ 1];
-                const float pe = __ldg(f.p[pc][pl] + t);
+                const float* __restrict__ po = pick2(f.p, pc, pl ^ 1);
+                const float pe = __ldg(pick2(f.p, pc, pl) + t);
                 *xp = first ? __fmul_rn(alpha, pe) : __fadd_rn(*xp, __fmul_rn(alpha, pe));
                 float ns = nbr_sum(L, code, t, k, [&](int e, int) { return __ldg(po + e); });
-                float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, L, code, s.i, s.j, k), pe), ns);
+                float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.walls, L, code, s.i, s.j, k), pe), ns);
                 r = __fsub_rn(r, __fmul_rn(alpha, ape));
                 v[0] += (double)r * (double)r;
             } else if (first) {
                 *xp = 0.0f;
             }
-            L.r[pl][t] = r;
+            pick(L.r, pl)[t] = r;
             v[1] += r;
         }
     }
@@ -664,9 +678,9 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
     }
     const float mean = level0 ? g.st->mean : 0.0f;
     const int oc = color ^ 1;
-    const float* __restrict__ rs = L.r[color];
-    const float* __restrict__ zo = L.z[oc];
-    float* __restrict__ zs = L.z[color];
+    const float* __restrict__ rs = pick(L.r, color);
+    const float* __restrict__ zo = pick(L.z, oc);
+    float* __restrict__ zs = pick(L.z, color);
     double v[1] = {0.0};
     GRID_STRIDE(t, L.P) {
         Slot s = slot_of(L, t);
@@ -685,7 +699,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
                 } else if (MODE != HS_FIRST) {
                     ns = nbr_sum(L, code, t, k, [&](int e, int) { return Zs<ZT>::ld(zo, e); });
                 }
-                const float zn = (rv + ns) / nf_of<SOLID>(g.bt, L, code, s.i, s.j, k);
+                const float zn = (rv + ns) / nf_of<SOLID>(g.walls, L, code, s.i, s.j, k);
                 Zs<ZT>::st(zs, t, zn);
                 if (MODE == HS_ZR) v[0] += (double)zn * (double)rv;
             }
@@ -694,7 +708,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
             // the other cell of the slot (final from the previous half sweep)
             const int ko = 2 * s.kk + ((s.i + s.j + oc) & 1);
             if (ko < L.n2 && (code_at<SOLID>(L, oc, t, s.i, s.j, ko) & CELL_FLUID))
-                v[0] += (double)Zs<ZT>::ld(zo, t) * (double)(rld<ZT>(L.r[oc], t, level0) - mean);
+                v[0] += (double)Zs<ZT>::ld(zo, t) * (double)(rld<ZT>(pick(L.r, oc), t, level0) - mean);
         }
     }
     if (MODE == HS_ZR) {
@@ -734,18 +748,18 @@ __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0,
                     const int e = (i * F.n1 + j) * F.H + K;
                     const unsigned code = code_at<SOLID>(F, pl, e, i, j, k);
                     if (!(code & CELL_FLUID)) continue;
-                    const float* __restrict__ zo = F.z[pl ^ 1];
+                    const float* __restrict__ zo = pick(F.z, pl ^ 1);
                     float ns = nbr_sum(F, code, e, k, [&](int ee, int) { return Zs<ZT>::ld(zo, ee); });
-                    float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, F, code, i, j, k), Zs<ZT>::ld(F.z[pl], e)), ns);
-                    float res = (rld<ZT>(F.r[pl], e, level0) - mean) - az;
+                    float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.walls, F, code, i, j, k), Zs<ZT>::ld(pick(F.z, pl), e)), ns);
+                    float res = (rld<ZT>(pick(F.r, pl), e, level0) - mean) - az;
                     acc += res * 0.5f;
                 }
         const int pc = (I + J + K) & 1;
         const int ec = (I * C.n1 + J) * C.H + (K >> 1);
-        Zs<ZT>::st(C.r[pc], ec, acc);
+        Zs<ZT>::st(pick(C.r, pc), ec, acc);
         if (first && pc == 0) {
             const unsigned cc = code_at<SOLID>(C, 0, ec, I, J, K);
-            if (cc & CELL_FLUID) Zs<ZT>::st(C.z[0], ec, (acc + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K));
+            if (cc & CELL_FLUID) Zs<ZT>::st(C.z[0], ec, (acc + 0.0f) / nf_of<SOLID>(g.walls, C, cc, I, J, K));
         }
     }
 }
@@ -781,7 +795,7 @@ EDGE_D Quad quad_of(const LV& L, int t) {
 template <bool SOLID>
 EDGE_D void quad_codes(const Lvl& L, int plane, const Quad& q, int p, unsigned (&code)[4]) {
     if (SOLID) {
-        ushort4 c = *reinterpret_cast<const ushort4*>(L.code[plane] + q.t0);
+        ushort4 c = *reinterpret_cast<const ushort4*>(pick(L.code, plane) + q.t0);
         code[0] = c.x; code[1] = c.y; code[2] = c.z; code[3] = c.w;
     } else {
 #pragma unroll
@@ -940,7 +954,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
 #pragma unroll
                     for (int m = 0; m < 4; m++)
                         if (code[m] & CELL_FLUID)
-                            zz[m] = (rr[m] + ns[m]) / nf_of<SOLID>(g.bt, q, code[m], qd.i, qd.j, 2 * (qd.kk0 + m) + p);
+                            zz[m] = (rr[m] + ns[m]) / nf_of<SOLID>(g.walls, q, code[m], qd.i, qd.j, 2 * (qd.kk0 + m) + p);
                     *reinterpret_cast<float4*>(z + qd.t0) = make_float4(zz[0], zz[1], zz[2], zz[3]);
                 }
             } else {
@@ -960,7 +974,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
                             return zo[e] + pz(s.i + di, s.j + dj, k + dk);
                         });
                     }
-                    z[t] = (r[t] + ns) / nf_of<SOLID>(g.bt, q, code, s.i, s.j, k);
+                    z[t] = (r[t] + ns) / nf_of<SOLID>(g.walls, q, code, s.i, s.j, k);
                 }
             }
         }
@@ -995,7 +1009,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
                         if (!(code & CELL_FLUID)) continue;
                         const float* zo = sh + q.zoff + (pl ^ 1) * q.P;
                         float ns = nbr_sum(q, code, e, k, [&](int ee, int) { return zo[ee]; });
-                        float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.bt, q, code, i, j, k), sh[q.zoff + pl * q.P + e]),
+                        float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.walls, q, code, i, j, k), sh[q.zoff + pl * q.P + e]),
                                              ns);
                         float res = sh[q.roff + pl * q.P + e] - az;
                         acc += res * 0.5f;
@@ -1004,12 +1018,69 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
         }
         __syncthreads();
     }
-    // bottom (mgpcg.py:186-189)
-    half(L - 1, 0, 0);
-    half(L - 1, 1, 1);
-    for (int it = 1; it < 20; it++) {
-        half(L - 1, 0, 1);
+    // bottom (mgpcg.py:186-189): 20 red-black iterations.  When the level
+    // has at most blockDim.x slots per plane, thread t owns slot t of both
+    // planes with its codes, divisors, residuals and neighbour offsets held in
+    // registers for all 40 half sweeps, and only the warps that own slots
+    // synchronise (named barrier 1); the arithmetic is half()'s.
+    if (cl[L - 1].P <= (int)blockDim.x) {
+        const CLvl& q = cl[L - 1];
+        const int nt = (q.P + 31) & ~31;
+        const int t = threadIdx.x;
+        if (t < nt) {
+            bool act[2];
+            unsigned code[2];
+            float nf[2], rr[2];
+            int kk[2];
+            const int sx = q.n1 * q.H;
+            Slot s = slot_of(q, t < q.P ? t : 0);
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                kk[c] = 2 * s.kk + ((s.i + s.j + c) & 1);
+                act[c] = t < q.P && kk[c] < q.n2;
+                code[c] = 0;
+                nf[c] = 1.0f;
+                rr[c] = 0.0f;
+                if (act[c]) {
+                    code[c] = SOLID ? (unsigned)codes[q.coff + c * q.P + t] : range_code(q, s.i, s.j, kk[c]);
+                    act[c] = (code[c] & CELL_FLUID) != 0;
+                    nf[c] = nf_of<SOLID>(g.walls, q, code[c], s.i, s.j, kk[c]);
+                    rr[c] = sh[q.roff + c * q.P + t];
+                }
+            }
+            float* z0 = sh + q.zoff;
+            float* z1 = z0 + q.P;
+            auto sweep = [&](int c, bool from_zero) {
+                if (act[c]) {
+                    const float* zo = c ? z0 : z1;
+                    float ns = 0.0f;
+                    if (!from_zero) {
+                        const int k = kk[c];
+                        if (code[c] & NB_XP) ns += zo[t + sx];
+                        if (code[c] & NB_XM) ns += zo[t - sx];
+                        if (code[c] & NB_YP) ns += zo[t + q.H];
+                        if (code[c] & NB_YM) ns += zo[t - q.H];
+                        if (code[c] & NB_ZP) ns += zo[t + (k & 1)];
+                        if (code[c] & NB_ZM) ns += zo[t - 1 + (k & 1)];
+                    }
+                    (c ? z1 : z0)[t] = (rr[c] + ns) / nf[c];
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+            };
+            sweep(0, true);
+            sweep(1, false);
+            for (int it = 1; it < 20; it++) {
+                sweep(0, false);
+                sweep(1, false);
+            }
+        }
+    } else {
+        half(L - 1, 0, 0);
         half(L - 1, 1, 1);
+        for (int it = 1; it < 20; it++) {
+            half(L - 1, 0, 1);
+            half(L - 1, 1, 1);
+        }
     }
     __syncthreads();
     // up
@@ -1053,9 +1124,9 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
     }
     const float mean = level0 ? g.st->mean : 0.0f;
     const int oc = color ^ 1;
-    const float* __restrict__ rs = L.r[color];
-    const float* __restrict__ zo = L.z[oc];
-    float* __restrict__ zs = L.z[color];
+    const float* __restrict__ rs = pick(L.r, color);
+    const float* __restrict__ zo = pick(L.z, oc);
+    float* __restrict__ zs = pick(L.z, color);
     double v[1] = {0.0};
     GRID_STRIDE(t, L.n0 * L.n1 * (L.H >> 2)) {
         const Quad q = quad_of(L, t);
@@ -1076,7 +1147,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             rv[m] = rv[m] - mean;
-            zn[m] = (code[m] & CELL_FLUID) ? (rv[m] + ns[m]) / nf_of<SOLID>(g.bt, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
+            zn[m] = (code[m] & CELL_FLUID) ? (rv[m] + ns[m]) / nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
                                            : 0.0f;
             if (MODE == HS_ZR && (code[m] & CELL_FLUID)) v[0] += (double)zn[m] * (double)rv[m];
         }
@@ -1086,7 +1157,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
             unsigned co[4];
             quad_codes<SOLID>(L, oc, q, p ^ 1, co);
             float ro[4], zz[4];
-            rld4<ZT>(L.r[oc], q.t0, level0, ro);
+            rld4<ZT>(pick(L.r, oc), q.t0, level0, ro);
             Zs<ZT>::ld4(zo, q.t0, zz);
 #pragma unroll
             for (int m = 0; m < 4; m++)
@@ -1123,8 +1194,8 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
             const int pl = c0 ^ h;
             unsigned code[4];
             quad_codes<SOLID>(L, pl, q, h, code);
-            const float* __restrict__ zo = L.z[pl ^ 1];
-            const float* __restrict__ po = f.p[pc][pl ^ 1];
+            const float* __restrict__ zo = pick(L.z, pl ^ 1);
+            const float* __restrict__ po = pick2(f.p, pc, pl ^ 1);
             auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
                 Zs<ZT>::ld4(zz, e, o);
                 if (!first) {
@@ -1135,7 +1206,7 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
                 }
             };
             float pe[4], ns[4];
-            pn4(L.z[pl], f.p[pc][pl], q.t0, pe);
+            pn4(pick(L.z, pl), pick2(f.p, pc, pl), q.t0, pe);
             quad_nbr_sum<false>(
                 L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
                 [&](int e) { const float ze = Zs<ZT>::ld(zo, e); return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e))); },
@@ -1143,14 +1214,14 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
 #pragma unroll
             for (int m = 0; m < 4; m++) {
                 if (code[m] & CELL_FLUID) {
-                    float nf = nf_of<SOLID>(g.bt, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
+                    float nf = nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
                     float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
                     v[0] += (double)pe[m] * (double)ape;
                 } else {
                     pe[m] = 0.0f;
                 }
             }
-            st4(f.p[pc ^ 1][pl] + q.t0, pe);
+            st4(pick2(f.p, pc ^ 1, pl) + q.t0, pe);
         }
     }
     if (last_block<1>(g, 2, v)) {
@@ -1182,11 +1253,11 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
             const int pl = c0 ^ h;
             unsigned code[4];
             quad_codes<SOLID>(L, pl, q, h, code);
-            const float* __restrict__ po = f.p[pc][pl ^ 1];
+            const float* __restrict__ po = pick2(f.p, pc, pl ^ 1);
             float pe[4], ns[4], r[4], x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            ld4(f.p[pc][pl] + q.t0, pe);
-            ld4c(L.r[pl] + q.t0, r);
-            if (!first) ld4c(f.x[pl] + q.t0, x);
+            ld4(pick2(f.p, pc, pl) + q.t0, pe);
+            ld4c(pick(L.r, pl) + q.t0, r);
+            if (!first) ld4c(pick(f.x, pl) + q.t0, x);
             quad_nbr_sum<false>(
                 L, q, h, code, [&](int e, float(&o)[4]) { ld4(po + e, o); }, [&](int e) { return __ldg(po + e); },
                 NoParent(), ns);
@@ -1195,15 +1266,15 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
                 r[m] = r[m] - mean;
                 if (code[m] & CELL_FLUID) {
                     x[m] = first ? __fmul_rn(alpha, pe[m]) : __fadd_rn(x[m], __fmul_rn(alpha, pe[m]));
-                    float nf = nf_of<SOLID>(g.bt, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
+                    float nf = nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
                     float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
                     r[m] = __fsub_rn(r[m], __fmul_rn(alpha, ape));
                     v[0] += (double)r[m] * (double)r[m];
                 }
                 v[1] += r[m];
             }
-            st4(f.x[pl] + q.t0, x);
-            st4(L.r[pl] + q.t0, r);
+            st4(pick(f.x, pl) + q.t0, x);
+            st4(pick(L.r, pl) + q.t0, r);
         }
     }
     if (last_block<2>(g, 3, v)) {
@@ -1247,17 +1318,17 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
                     const int pl = c0 ^ h;
                     unsigned code[4];
                     quad_codes<SOLID>(F, pl, q, h, code);
-                    const float* __restrict__ zo = F.z[pl ^ 1];
+                    const float* __restrict__ zo = pick(F.z, pl ^ 1);
                     float ns[4], zc[4], rc[4];
                     quad_nbr_sum<false>(
                         F, q, h, code, [&](int e, float(&o)[4]) { Zs<ZT>::ld4(zo, e, o); },
                         [&](int e) { return Zs<ZT>::ld(zo, e); }, NoParent(), ns);
-                    Zs<ZT>::ld4(F.z[pl], q.t0, zc);
-                    rld4<ZT>(F.r[pl], q.t0, level0, rc);
+                    Zs<ZT>::ld4(pick(F.z, pl), q.t0, zc);
+                    rld4<ZT>(pick(F.r, pl), q.t0, level0, rc);
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         if (!(code[m] & CELL_FLUID)) continue;
-                        float nf = nf_of<SOLID>(g.bt, F, code[m], i, j, 2 * (K0 + m) + h);
+                        float nf = nf_of<SOLID>(g.walls, F, code[m], i, j, 2 * (K0 + m) + h);
                         float az = __fsub_rn(__fmul_rn(nf, zc[m]), ns[m]);
                         float res = (rc[m] - mean) - az;
                         acc[m] += res * 0.5f;
@@ -1268,8 +1339,8 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
         // at slots ecb, ecb+1
         const int ecb = (I * C.n1 + J) * C.H + (K0 >> 1);
         const int pa = (I + J) & 1;
-        Zs<ZT>::st2(C.r[pa], ecb, acc[0], acc[2]);
-        Zs<ZT>::st2(C.r[pa ^ 1], ecb, acc[1], acc[3]);
+        Zs<ZT>::st2(pick(C.r, pa), ecb, acc[0], acc[2]);
+        Zs<ZT>::st2(pick(C.r, pa ^ 1), ecb, acc[1], acc[3]);
         if (first) {
             // first half sweep of the coarse level: z = r / n_fluid on colour 0
             const int m0 = pa;  // the colour-0 cells are m0 and m0 + 2
@@ -1278,7 +1349,7 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
             for (int u = 0; u < 2; u++) {
                 const int m = m0 + 2 * u, K = K0 + m;
                 const unsigned cc = SOLID ? (unsigned)C.code[0][ecb + u] : range_code(C, I, J, K);
-                zz[u] = (cc & CELL_FLUID) ? (acc[m] + 0.0f) / nf_of<SOLID>(g.bt, C, cc, I, J, K) : 0.0f;
+                zz[u] = (cc & CELL_FLUID) ? (acc[m] + 0.0f) / nf_of<SOLID>(g.walls, C, cc, I, J, K) : 0.0f;
             }
             Zs<ZT>::st2(C.z[0], ecb, zz[0], zz[1]);
         }
@@ -1289,11 +1360,13 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
 // wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479).
 // One thread per slot: the faces on the low side of its two cells in each
 // axis, and the high boundary faces of cells on the high boundary.
-EDGE_D void face_update(const G& g, Faces& U, int a, int e, float gr, bool wall) {
-    float u = U.u[a][e] - gr;
-    if (wall) u = 0.0f;
-    U.u[a][e] = u;
-    if (U.f[a]) U.f[a][e] = -gr;
+EDGE_D void face_update(const G& g, const Faces& U, int a, int e, float gr, bool at_wall) {
+    float* ua = pick3(U.u, a);
+    float* fa = pick3(U.f, a);
+    float u = ua[e] - gr;
+    if (at_wall) u = 0.0f;
+    ua[e] = u;
+    if (fa) fa[e] = -gr;
 }
 
 __global__ void __launch_bounds__(256) k_grad_p(G g, Lvl L, Fine f, Faces U) {
@@ -1307,17 +1380,17 @@ __global__ void __launch_bounds__(256) k_grad_p(G g, Lvl L, Fine f, Faces U) {
         for (int h = 0; h < 2; h++) {
             const int k = 2 * s.kk + h, pl = c0 ^ h;
             if (k >= nz) break;
-            const float* xo = f.x[pl ^ 1];
-            const float xc = xv ? f.x[pl][t] : 0.0f;
+            const float* xo = pick(f.x, pl ^ 1);
+            const float xc = xv ? pick(f.x, pl)[t] : 0.0f;
             const float xl = (xv && i > 0) ? xo[t - sx] : 0.0f;
-            face_update(g, U, 0, idx3(i, j, k, ny, nz), xc - xl, i == 0 && g.bt[0] == 2);
-            if (i == nx - 1) face_update(g, U, 0, idx3(nx, j, k, ny, nz), 0.0f - xc, g.bt[1] == 2);
+            face_update(g, U, 0, idx3(i, j, k, ny, nz), xc - xl, i == 0 && wall(g.walls, 0));
+            if (i == nx - 1) face_update(g, U, 0, idx3(nx, j, k, ny, nz), 0.0f - xc, wall(g.walls, 1));
             const float yl = (xv && j > 0) ? xo[t - L.H] : 0.0f;
-            face_update(g, U, 1, idx3(i, j, k, ny + 1, nz), xc - yl, j == 0 && g.bt[2] == 2);
-            if (j == ny - 1) face_update(g, U, 1, idx3(i, ny, k, ny + 1, nz), 0.0f - xc, g.bt[3] == 2);
+            face_update(g, U, 1, idx3(i, j, k, ny + 1, nz), xc - yl, j == 0 && wall(g.walls, 2));
+            if (j == ny - 1) face_update(g, U, 1, idx3(i, ny, k, ny + 1, nz), 0.0f - xc, wall(g.walls, 3));
             const float zl = (xv && k > 0) ? xo[t - 1 + (k & 1)] : 0.0f;
-            face_update(g, U, 2, idx3(i, j, k, ny, nz + 1), xc - zl, k == 0 && g.bt[4] == 2);
-            if (k == nz - 1) face_update(g, U, 2, idx3(i, j, nz, ny, nz + 1), 0.0f - xc, g.bt[5] == 2);
+            face_update(g, U, 2, idx3(i, j, k, ny, nz + 1), xc - zl, k == 0 && wall(g.walls, 4));
+            if (k == nz - 1) face_update(g, U, 2, idx3(i, j, nz, ny, nz + 1), 0.0f - xc, wall(g.walls, 5));
         }
     }
 }
@@ -1351,17 +1424,17 @@ __global__ void k_to_rb(Lvl L, const float* src, float* p0, float* p1) {
 }
 
 // num_fluid_neighbors from the lexicographic mask (edge_mgpcg_apply_A)
-EDGE_D float n_fluid_lex(const int* bt, const Lvl& L, int i, int j, int k) {
+EDGE_D float n_fluid_lex(int walls, const Lvl& L, int i, int j, int k) {
     float num = 6.0f;
     int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        if (I[a] <= 0 && bt[2 * a] == 2) num -= 1.0f;
+        if (I[a] <= 0 && wall(walls, 2 * a)) num -= 1.0f;
         else if (L.bm && I[a] > 0) {
             int e = idx3(i - (a == 0), j - (a == 1), k - (a == 2), L.n1, L.n2);
             if (__ldg(L.bm + e) > 0) num -= 1.0f;
         }
-        if (I[a] >= D[a] - 1 && bt[2 * a + 1] == 2) num -= 1.0f;
+        if (I[a] >= D[a] - 1 && wall(walls, 2 * a + 1)) num -= 1.0f;
         else if (L.bm && I[a] < D[a] - 1) {
             int e = idx3(i + (a == 0), j + (a == 1), k + (a == 2), L.n1, L.n2);
             if (__ldg(L.bm + e) > 0) num -= 1.0f;
@@ -1388,7 +1461,7 @@ __global__ void k_apply_A(G g, Lvl L, const float* p, float* Ap) {
         if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += p[e + stride[a]];
         if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
     }
-    Ap[e] = __fsub_rn(__fmul_rn(n_fluid_lex(g.bt, L, i, j, k), p[e]), ns);
+    Ap[e] = __fsub_rn(__fmul_rn(n_fluid_lex(g.walls, L, i, j, k), p[e]), ns);
 }
 
 // the same operator in float64 (the FP64 reference solve of the precision study)
@@ -1408,7 +1481,7 @@ __global__ void k_apply_A64(G g, Lvl L, const double* p, double* Ap) {
         if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += p[e + stride[a]];
         if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
     }
-    Ap[e] = (double)n_fluid_lex(g.bt, L, i, j, k) * p[e] - ns;
+    Ap[e] = (double)n_fluid_lex(g.walls, L, i, j, k) * p[e] - ns;
 }
 
 // ---------------------------------------------------------------------------
@@ -1767,6 +1840,8 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     c.lv.L = L;
     c.zbf16 = precision == 1;
     for (int q = 0; q < 6; q++) c.g.bt[q] = bt[q];
+    c.g.walls = 0;
+    for (int q = 0; q < 6; q++) c.g.walls |= (bt[q] == 2) << q;
     int r = EDGE_OK;
     for (int l = 0; l < L && r == EDGE_OK; l++) {
         Lvl& V = c.lv.lv[l];
@@ -2017,6 +2092,8 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     memset(&c, 0, sizeof(c));
     c.lv.L = L;
     for (int q = 0; q < 6; q++) c.g.bt[q] = bt[q];
+    c.g.walls = 0;
+    for (int q = 0; q < 6; q++) c.g.walls |= (bt[q] == 2) << q;
     long long off = 0;
     auto take = [&](long long count) {
         float* p = A->scratch + off;

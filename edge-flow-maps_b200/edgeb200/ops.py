@@ -106,12 +106,20 @@ def calc_fd_3_from_grad(dx, T, dT, d2T):
     _call("edge_calc_fd_3_from_grad", nx, ny, nz, F(dx), *_p3(T), *_p3(dT), *_p3(d2T), stream())
 
 
-PLANES = {0: 4, 1: 7, 2: 8}  # packed float4 planes per Hermite variant
+PLANES = {0: 8, 1: 8, 2: 8}  # packed float4 planes per Hermite variant (edge_packed_planes)
 
 
 def map_pack(variant, psi, T, dT, d2T, packed):
     nx, ny, nz = cell_dims(psi)
+    _check_packed(variant, packed, (nx, ny, nz))
     _call("edge_map_pack", variant, nx, ny, nz, ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), ptr(packed), stream())
+    _launched[0] += variant != 2  # the derived-plane pass of ED4 / EDGE maps
+
+
+def _check_packed(variant, packed, res):
+    want = (N.load().edge_packed_planes(variant),) + tuple(res) + (4,)
+    if tuple(packed.shape) != want or packed.dtype != torch.float32 or not packed.is_contiguous():
+        raise ValueError(f"packed map must be a contiguous float32 tensor of shape {want}")
 
 
 def map_unpack(variant, packed, psi, T, dT, d2T):
@@ -120,8 +128,10 @@ def map_unpack(variant, packed, psi, T, dT, d2T):
 
 
 def march_packed(variant, u, dx, dt, eps, packed_in, packed_out, res, identity=False):
+    _check_packed(variant, packed_out, res)
     _call("edge_march_packed", variant, *res, F(dx), F(dt), F(eps), *_p3(u), ptr(packed_in), ptr(packed_out),
           int(bool(identity)), stream())
+    _launched[0] += variant != 2
 
 
 def march_ge_packed(u, dx, dt, packed_in, packed_out, res):

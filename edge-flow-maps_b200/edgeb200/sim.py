@@ -33,7 +33,7 @@ VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL, 
 class EdgeSim:
     def __init__(self, res, dx, variant="edge", cfl=0.5, reinit_every=12, ed_eps=None, base_level=3,
                  bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda", solid=None,
-                 emitters=None, packed=False):
+                 emitters=None, packed=True):
         if variant not in VARIANTS:
             raise ValueError(f"variant must be one of {sorted(VARIANTS)}")
         N.load()

@@ -122,12 +122,18 @@ int edge_face_map(int variant, int nx, int ny, int nz, float dx, const float *ps
                   const float *Tz, const float *dTx, const float *dTy, const float *dTz, const float *d2Tx,
                   const float *d2Ty, const float *d2Tz, float *fpsix, float *fpsiy, float *fpsiz, float *fcolx,
                   float *fcoly, float *fcolz, void *stream);
-/* The backward map in the packed layout the device driver keeps: float4
- * planes of n = nx*ny*nz cells (plane q at packed + 4*q*n floats):
- * 0 psi, 1-3 the columns d psi/dx, d psi/dy, d psi/dz, 4-6 the mixed
- * derivatives (psi_yz, psi_xz, psi_xy) per component, 7 psi_xyz; ED4 uses
- * planes 0-3, EDGE 0-6, ED8 0-7.  pack/unpack convert from/to the reference
- * layout (psi, T_c rows, dT_c, d2T_c as above; no reference counterpart). */
+/* The backward map in the packed layout the device driver keeps: 8 float4
+ * planes of n = nx*ny*nz cells (plane q at packed + 4*q*n floats) for every
+ * variant (edge_packed_planes): 0 psi, 1-3 the columns d psi/dx, d psi/dy,
+ * d psi/dz, 4-6 the mixed derivatives (psi_yz, psi_xz, psi_xy) per
+ * component, 7 psi_xyz.  ED8 keeps all eight as state; EDGE keeps 0-6 and
+ * plane 7 holds the finite-difference triple-derivative coefficient the
+ * reference re-derives from planes 4-6 at every Hermite evaluation; ED4 keeps
+ * 0-3 and planes 4-7 hold the finite-difference coefficients derived from
+ * planes 1-3.  pack and the marches fill the derived planes.  pack/unpack
+ * convert from/to the reference layout (psi, T_c rows, dT_c, d2T_c as above;
+ * no reference counterpart). */
+int edge_packed_planes(int variant);
 int edge_map_pack(int variant, int nx, int ny, int nz, const float *psi, const float *Tx, const float *Ty,
                   const float *Tz, const float *dTx, const float *dTy, const float *dTz, const float *d2Tx,
                   const float *d2Ty, const float *d2Tz, float *packed, void *stream);

@@ -287,7 +287,7 @@ def test_packed_layout_roundtrip_and_march(ops, variant):
     rng = np.random.default_rng(21 + variant)
     res = (24, 16, 12)
     dx = 1.0 / 16
-    planes = {0: 4, 1: 7, 2: 8}[variant]
+    planes = 8  # every packed map (edge_packed_planes)
     psi = T_(O.center_coords(res, dx) + 0.3 * dx * rng.uniform(-1, 1, size=res + (3,)))
     T = [T_(np.eye(3)[c] + 0.05 * rng.normal(size=res + (3,))) for c in range(3)]
     dT = [T_(0.2 * rng.normal(size=res + (3,))) for _ in range(3)] if variant else None
