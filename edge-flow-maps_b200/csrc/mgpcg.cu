@@ -122,6 +122,10 @@ struct Ctx {
     Fine f;
     int csmem;  // dynamic shared memory of k_coarse (bytes)
     int zbf16;  // 1: the V-cycle's level arrays are BF16 (mixed-precision solver)
+    // k_mid: levels lm..lcc-1 on a cluster of cmid thread blocks, lcc..L-1 in
+    // block 0's shared memory (csmem_mid bytes); cmid == 0: per-level kernels
+    // down to lc and k_coarse
+    int lm = 0, lcc = 0, cmid = 0, csmem_mid = 0;
 };
 
 EDGE_D void set_cond(const G& g, unsigned v) {
@@ -246,6 +250,32 @@ struct Zs<__nv_bfloat16> {
 // r of a level: FP32 at level 0, else the level storage type
 template <class ZT>
 EDGE_D float rld(const float* b, int e, int level0) { return level0 ? __ldg(b + e) : Zs<ZT>::ld(b, e); }
+
+// Loads of data that another thread block of the same cluster wrote earlier
+// in the same launch: through L2 (ld.global.cg), never the read-only path.
+template <class ZT>
+struct Zc;
+template <>
+struct Zc<float> {
+    static EDGE_D float ld(const float* b, int e) { return __ldcg(b + e); }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        float4 t = __ldcg(reinterpret_cast<const float4*>(b + e));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+};
+template <>
+struct Zc<__nv_bfloat16> {
+    static EDGE_D float ld(const float* b, int e) {
+        unsigned short u = __ldcg(reinterpret_cast<const unsigned short*>(b) + e);
+        return __bfloat162float(__ushort_as_bfloat16(u));
+    }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        const uint2 u = __ldcg(reinterpret_cast<const uint2*>(reinterpret_cast<const __nv_bfloat16*>(b) + e));
+        const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&u.x);
+        const __nv_bfloat162 c = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
+        v[0] = __low2float(a); v[1] = __high2float(a); v[2] = __low2float(c); v[3] = __high2float(c);
+    }
+};
 template <class ZT>
 EDGE_D void rld4(const float* b, int e, int level0, float (&v)[4]) {
     if (level0) Zs<float>::ld4(b, e, v);
@@ -862,22 +892,26 @@ struct CLvl {
     int roff, zoff, coff;  // float offsets of the r and z planes, ushort offset of the codes
 };
 
-template <bool ZR, bool SOLID, class ZT>
-__global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
-    extern __shared__ float sh[];
-    __shared__ CLvl cl[16];
-    count_launch(g.st);
-    if (!running(g)) {
-        if (ZR && threadIdx.x == 0) set_cond(g, 0);
-        return;
-    }
-    const int L = a.L, lc = a.lc;
+// The level structs of a launch's Levels parameter, copied to shared memory
+// with constant indices (a run-time index into the parameter would put the
+// whole parameter in local memory).
+EDGE_D void copy_levels(const Levels& a, Lvl* sl) {
+#pragma unroll
+    for (int l = 0; l < 16; l++)
+        if ((int)threadIdx.x == l && l < a.L) sl[l] = a.lv[l];
+}
+
+// Body of the coarse group (levels lc..L-1, lvs in shared memory), run by one
+// thread block; COH: r[lc] was written earlier in the same launch by another
+// thread block of the cluster (coherent loads).
+template <bool ZR, bool SOLID, class ZT, bool COH>
+EDGE_D void coarse_body(const G& g, const Lvl* lvs, int L, int lc, float* sh, CLvl* cl) {
     if (threadIdx.x == 0) {
         // per level: r plane 0, r plane 1, z plane 0, z plane 1 (floats); the
         // solid codes (two planes per level) follow all the floats
         int off = 0;
         for (int l = lc; l < L; l++) {
-            const Lvl& V = a.lv[l];
+            const Lvl& V = lvs[l];
             CLvl q;
             q.n0 = V.n0; q.n1 = V.n1; q.n2 = V.n2; q.H = V.H; q.P = V.P;
             q.dH = V.dH; q.d1 = V.d1; q.d2 = V.d2; q.dQ = V.dQ;
@@ -899,14 +933,15 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     {
         const CLvl& q = cl[lc];
         for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
-            const float* src = e < q.P ? a.lv[lc].r[0] : a.lv[lc].r[1];
-            sh[q.roff + e] = rld<ZT>(src, e < q.P ? e : e - q.P, lc == 0) - mean;
+            const float* src = e < q.P ? lvs[lc].r[0] : lvs[lc].r[1];
+            const int ee = e < q.P ? e : e - q.P;
+            sh[q.roff + e] = (COH ? Zc<ZT>::ld(src, ee) : rld<ZT>(src, ee, lc == 0)) - mean;
         }
         if (SOLID)
             for (int l = lc; l < L; l++) {
                 const CLvl& u = cl[l];
                 for (int e = threadIdx.x; e < 2 * u.P; e += blockDim.x)
-                    codes[u.coff + e] = e < u.P ? a.lv[l].code[0][e] : a.lv[l].code[1][e - u.P];
+                    codes[u.coff + e] = e < u.P ? lvs[l].code[0][e] : lvs[l].code[1][e - u.P];
             }
     }
     __syncthreads();
@@ -1095,7 +1130,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     {
         const CLvl& q = cl[lc];
         for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
-            float* dst = e < q.P ? a.lv[lc].z[0] : a.lv[lc].z[1];
+            float* dst = e < q.P ? lvs[lc].z[0] : lvs[lc].z[1];
             Zs<ZT>::st(dst, e < q.P ? e : e - q.P, sh[q.zoff + e]);
         }
     }
@@ -1113,6 +1148,21 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
         block_sum<1>(v);
         if (threadIdx.x == 0) zr_epilogue(g, v[0]);
     }
+}
+
+template <bool ZR, bool SOLID, class ZT>
+__global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
+    extern __shared__ float sh[];
+    __shared__ CLvl cl[16];
+    __shared__ Lvl sl[16];
+    count_launch(g.st);
+    if (!running(g)) {
+        if (ZR && threadIdx.x == 0) set_cond(g, 0);
+        return;
+    }
+    copy_levels(a, sl);
+    __syncthreads();
+    coarse_body<ZR, SOLID, ZT, false>(g, sl, a.L, a.lc, sh, cl);
 }
 
 template <int MODE, bool SOLID, class ZT>
@@ -1356,6 +1406,161 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
     }
 }
 
+// ---------------------------------------------------------------------------
+// The middle of the V-cycle in one thread-block cluster (k_mid): levels
+// lm..lcc-1 (small enough to live in L2, too small to fill the GPU) run the
+// four-slot half sweeps and restrictions of k_hsweep4 / k_restrict4 spread
+// over the cluster's threads, a cluster barrier between phases instead of a
+// kernel boundary; block 0 then runs the shared-memory coarse group
+// (levels lcc..L-1) and the cluster runs the up sweeps.  Data written in the
+// launch is read through L2 (Zc).  Same arithmetic as the per-level kernels.
+// ---------------------------------------------------------------------------
+EDGE_D void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+EDGE_D unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+EDGE_D unsigned cluster_size() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+
+template <class ZT>
+EDGE_D float parent_zc(const Lvl& C, int i, int j, int k) {
+    int I = i >> 1, J = j >> 1, K = k >> 1;
+    int e = (I * C.n1 + J) * C.H + (K >> 1);
+    return Zc<ZT>::ld(pick(C.z, (I + J + K) & 1), e);
+}
+
+// k_hsweep4 (HS_PLAIN / HS_PROLONG) on a level >= 1, threads t0, t0+stride, ...
+template <int MODE, bool SOLID, class ZT>
+EDGE_D void cl_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int t0, int stride) {
+    const int oc = color ^ 1;
+    const float* rs = pick(L.r, color);
+    const float* zo = pick(L.z, oc);
+    float* zs = pick(L.z, color);
+    const int nq = L.n0 * L.n1 * (L.H >> 2);
+    for (int t = t0; t < nq; t += stride) {
+        const Quad q = quad_of(L, t);
+        const int p = (q.i + q.j + color) & 1;
+        unsigned code[4];
+        quad_codes<SOLID>(L, color, q, p, code);
+        float rv[4], ns[4] = {0.0f, 0.0f, 0.0f, 0.0f}, zn[4];
+        Zc<ZT>::ld4(rs, q.t0, rv);
+        auto v4 = [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); };
+        auto v1 = [&](int e) { return Zc<ZT>::ld(zo, e); };
+        if (MODE == HS_PROLONG)
+            quad_nbr_sum<true>(L, q, p, code, v4, v1, [&](int i, int j, int k) { return parent_zc<ZT>(C, i, j, k); },
+                               ns);
+        else
+            quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            zn[m] = (code[m] & CELL_FLUID)
+                        ? ((rv[m] - 0.0f) + ns[m]) / nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
+                        : 0.0f;
+        Zs<ZT>::st4(zs, q.t0, zn);
+    }
+}
+
+// k_restrict4 on a level >= 1
+template <bool SOLID, class ZT>
+EDGE_D void cl_restrict(const G& g, const Lvl& F, const Lvl& C, bool first, int t0, int stride) {
+    const int nq = F.H >> 2;
+    for (int t = t0; t < C.n0 * C.n1 * nq; t += stride) {
+        const int rowc = fdiv(t, F.dQ);
+        const int K0 = (t - rowc * nq) << 2;
+        const int I = fdiv(rowc, C.d1);
+        const int J = rowc - I * C.n1;
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const int i = 2 * I + a, j = 2 * J + b;
+                const Quad q{i, j, K0, (i * F.n1 + j) * F.H + K0};
+                const int c0 = (i + j) & 1;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int pl = c0 ^ h;
+                    unsigned code[4];
+                    quad_codes<SOLID>(F, pl, q, h, code);
+                    const float* __restrict__ zo = pick(F.z, pl ^ 1);
+                    float ns[4], zc[4], rc[4];
+                    quad_nbr_sum<false>(
+                        F, q, h, code, [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); },
+                        [&](int e) { return Zc<ZT>::ld(zo, e); }, NoParent(), ns);
+                    Zc<ZT>::ld4(pick(F.z, pl), q.t0, zc);
+                    Zc<ZT>::ld4(pick(F.r, pl), q.t0, rc);
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        if (!(code[m] & CELL_FLUID)) continue;
+                        float nf = nf_of<SOLID>(g.walls, F, code[m], i, j, 2 * (K0 + m) + h);
+                        float az = __fsub_rn(__fmul_rn(nf, zc[m]), ns[m]);
+                        float res = (rc[m] - 0.0f) - az;
+                        acc[m] += res * 0.5f;
+                    }
+                }
+            }
+        const int ecb = (I * C.n1 + J) * C.H + (K0 >> 1);
+        const int pa = (I + J) & 1;
+        Zs<ZT>::st2(pick(C.r, pa), ecb, acc[0], acc[2]);
+        Zs<ZT>::st2(pick(C.r, pa ^ 1), ecb, acc[1], acc[3]);
+        if (first) {
+            const int m0 = pa;
+            float zz[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int m = m0 + 2 * u, K = K0 + m;
+                const unsigned cc = SOLID ? (unsigned)C.code[0][ecb + u] : range_code(C, I, J, K);
+                zz[u] = (cc & CELL_FLUID) ? (acc[m] + 0.0f) / nf_of<SOLID>(g.walls, C, cc, I, J, K) : 0.0f;
+            }
+            Zs<ZT>::st2(C.z[0], ecb, zz[0], zz[1]);
+        }
+    }
+}
+
+constexpr int kMidThreads = 512;
+
+template <bool SOLID, class ZT>
+__global__ void __launch_bounds__(kMidThreads) k_mid(G g, Levels a, int lm, int lcc) {
+    extern __shared__ float sh[];
+    __shared__ CLvl cl[16];
+    __shared__ Lvl sl[16];
+    count_launch(g.st);
+    copy_levels(a, sl);
+    __syncthreads();
+    if (!running(g)) return;  // the same in every block: the status only changes between launches
+    const int rank = (int)cluster_rank();
+    const int t0 = rank * blockDim.x + threadIdx.x, stride = (int)cluster_size() * blockDim.x;
+    for (int l = lm; l < lcc; l++) {
+        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
+        cluster_sync();
+        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 0, t0, stride);
+        cluster_sync();
+        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
+        cluster_sync();
+        cl_restrict<SOLID, ZT>(g, sl[l], sl[l + 1], l + 1 < lcc, t0, stride);
+        cluster_sync();
+    }
+    if (rank == 0) coarse_body<false, SOLID, ZT, true>(g, sl, a.L, lcc, sh, cl);
+    cluster_sync();
+    for (int l = lcc - 1; l >= lm; l--) {
+        cl_sweep<HS_PROLONG, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
+        cluster_sync();
+        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 0, t0, stride);
+        cluster_sync();
+        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
+        cluster_sync();
+        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 0, t0, stride);
+        if (l > lm) cluster_sync();
+    }
+}
+
 // mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
 // wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479).
 // One thread per slot: the faces on the low side of its two cells in each
@@ -1562,6 +1767,84 @@ void plan_coarse(Ctx& c, bool solid) {
     }
 }
 
+// shared memory of the coarse group lc..L-1 (see k_coarse)
+static size_t coarse_bytes(const Levels& V, int lc, bool solid) {
+    size_t floats = 0, codes = 0;
+    for (int l = lc; l < V.L; l++) {
+        floats += 4 * (size_t)V.lv[l].P;
+        codes += 2 * (size_t)V.lv[l].P;
+    }
+    return floats * sizeof(float) + (solid ? codes * sizeof(unsigned short) : 0) + 16;
+}
+
+// k_mid takes the levels with at most 65536 slots per plane (the per-level
+// kernels of those run a few microseconds each, mostly launch and ramp) down
+// to the first level of at most 1024 slots, which starts block 0's
+// shared-memory group.  Opt-in with EDGE_MGPCG_CLUSTER=1: measured at
+// 256x128x128 it takes 80 us per V-cycle against 66 us for the per-level
+// kernels and k_coarse it replaces (the phases wait on block 0's coarse
+// group and on a cluster barrier each); off when a level in between is not
+// four-slot or the grid has too few levels.
+void plan_mid(Ctx& c, bool solid) {
+    c.cmid = 0;
+    const char* env = getenv("EDGE_MGPCG_CLUSTER");
+    if (!env || env[0] != '1') return;
+    const Levels& V = c.lv;
+    int lm = -1, lcc = -1;
+    for (int l = 1; l < V.L - 1; l++)
+        if (V.lv[l].P <= 65536) { lm = l; break; }
+    if (lm < 1) return;
+    for (int l = lm + 1; l < V.L; l++)
+        if (V.lv[l].P <= 1024) { lcc = l; break; }
+    if (lcc < 0) return;
+    for (int l = lm; l < lcc; l++)
+        if (!V.lv[l].vec) return;
+    size_t bytes = coarse_bytes(V, lcc, solid);
+    if (bytes > kCoarseSmem) return;
+    c.lm = lm;
+    c.lcc = lcc;
+    c.csmem_mid = (int)bytes;
+}
+
+// cluster size for k_mid: 16 blocks (non-portable) if the device schedules
+// such clusters with this shared memory, else 8, else the per-level path
+template <bool S, class ZT>
+static int mid_attrs(int smem) {
+    if (cudaFuncSetAttribute(k_mid<S, ZT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
+    if (cudaFuncSetAttribute(k_mid<S, ZT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 1;
+    return 0;
+}
+void prepare_mid_kernels(Ctx& c) {
+    if (c.lm < 1) return;
+    int bad = mid_attrs<false, float>(c.csmem_mid) | mid_attrs<true, float>(c.csmem_mid) |
+              mid_attrs<false, __nv_bfloat16>(c.csmem_mid) | mid_attrs<true, __nv_bfloat16>(c.csmem_mid);
+    if (bad) {
+        cudaGetLastError();
+        c.cmid = 0;
+        return;
+    }
+    for (int size : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = size;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(size);
+        cfg.blockDim = dim3(kMidThreads);
+        cfg.dynamicSmemBytes = c.csmem_mid;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, k_mid<false, float>, &cfg) == cudaSuccess && n >= 1) {
+            c.cmid = size;
+            return;
+        }
+        cudaGetLastError();
+    }
+    c.cmid = 0;
+}
+
 int prepare_coarse_kernels(const Ctx& c) {
     if ((size_t)c.csmem > kCoarseSmem) return EDGE_EINVAL;  // the coarsest level alone must fit
     if (c.csmem > 48 * 1024) {
@@ -1586,11 +1869,13 @@ int prepare_coarse_kernels(const Ctx& c) {
 template <bool S, class ZT>
 void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
     const Levels& V = c.lv;
-    const int lc = V.lc;
+    const bool mid = c.cmid > 0;
+    const int lc = mid ? c.lm : V.lc;         // levels 0..lc-1 run per-level kernels
+    const int lgroup = mid ? c.lcc : V.lc;    // first level of the shared-memory group
     for (int l = 0; l < lc; l++) {
         const Lvl& L = V.lv[l];
         const Lvl& C = V.lv[l + 1];
-        const int l0 = l == 0, first = l + 1 < lc;
+        const int l0 = l == 0, first = l + 1 < lgroup;
         if (L.vec) {
             const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
             if (l == 0) k_hsweep4<HS_FIRST, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
@@ -1607,8 +1892,25 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
             k_restrict<S, ZT><<<rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c.g, L, C, l0, first);
         }
     }
-    if (final_zr && lc == 0) k_coarse<true, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
-    else k_coarse<false, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
+    if (mid) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = c.cmid;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(c.cmid);
+        cfg.blockDim = dim3(kMidThreads);
+        cfg.dynamicSmemBytes = c.csmem_mid;
+        cfg.stream = stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k_mid<S, ZT>, c.g, V, c.lm, c.lcc);
+    } else if (final_zr && lc == 0) {
+        k_coarse<true, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
+    } else {
+        k_coarse<false, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
+    }
     for (int l = lc - 1; l >= 0; l--) {
         const Lvl& L = V.lv[l];
         const Lvl& C = V.lv[l + 1];
@@ -1864,6 +2166,10 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     }
     plan_coarse(c, s->solid);
     if (r == EDGE_OK) r = prepare_coarse_kernels(c);
+    if (r == EDGE_OK) {
+        plan_mid(c, s->solid);
+        prepare_mid_kernels(c);
+    }
     const size_t pa0 = plane_alloc(c.lv.lv[0].P);
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.x[0], 2 * pa0 * sizeof(float));
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.p[0][0], 4 * pa0 * sizeof(float));
@@ -2117,6 +2423,10 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     c.g.use_cond = 0;
     plan_coarse(c, false);
     r = prepare_coarse_kernels(c);
+    if (r == EDGE_OK) {
+        plan_mid(c, false);
+        prepare_mid_kernels(c);
+    }
     if (r != EDGE_OK) return r;
     // the loop state starts clean on every call (the arrays keep the last
     // call's contents; the set-up and the first iteration overwrite what is read)

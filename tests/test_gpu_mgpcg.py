@@ -244,3 +244,33 @@ def test_mixed_precision_vs_fp64():
         errs.append(rel_error(x, ref))
     assert its[1] <= its[0] + 2
     assert errs[0] < 1e-3 and errs[1] < 3 * errs[0] + 1e-6, errs
+
+
+@pytest.mark.parametrize("res,base_level,solid", [((256, 128, 128), 2, False), ((128, 64, 64), 1, False),
+                                                  ((128, 64, 64), 1, True)])
+def test_cluster_vcycle_matches_per_level_kernels(res, base_level, solid, monkeypatch):
+    """The middle levels on one thread-block cluster (k_mid) run the same
+    arithmetic as the per-level kernels: solutions and iteration counts are
+    identical bit for bit."""
+    from edgeb200.projection import Projection
+    rng = np.random.default_rng(3)
+    b = rng.normal(size=res).astype(np.float32)
+    b -= b.mean()
+    mask = bvel = None
+    if solid:
+        m = np.zeros(res, np.int32)
+        m[res[0] // 3:res[0] // 3 + 6, res[1] // 3:2 * res[1] // 3, res[2] // 4:res[2] // 2] = 1
+        mask, bvel = torch.from_numpy(m).cuda(), torch.zeros(res + (3,), device="cuda")
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("EDGE_MGPCG_CLUSTER", flag)
+        P = Projection(res, base_level=base_level, mask=mask, bvel=bvel)
+        x = torch.zeros(res, device="cuda")
+        z = torch.empty(res, device="cuda")
+        P.vcycle(T_(b), z)
+        P.solve(T_(b), x, abs_tol=0.0, rel_tol=1e-6)
+        out.append((N_(z), N_(x), P.result()))
+        P.close()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
