@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(128) k_march_edge(Mac mac, MapF m, float dt, f
             // Hermite of the identity map reproduces the (clamped) position;
             // its gradient is the identity.
             for (int c = 0; c < 3; c++) {
-                float u = P[c] / m.dx - 0.5f;
+                float u = over_dx(P[c], m.dx, m.inv_dx, m.pow2) - 0.5f;
                 float s = fmaxf(1.0f, fminf(u, m.hi[c]));
                 P[c] = (s + 0.5f) * m.dx;
                 for (int d = 0; d < 3; d++) T[c][d] = C[d][c];
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float 
         float T[3][3];
         if (IDENT) {
             for (int c = 0; c < 3; c++) {
-                float u = P[c] / m.dx - 0.5f;
+                float u = over_dx(P[c], m.dx, m.inv_dx, m.pow2) - 0.5f;
                 float s = fmaxf(1.0f, fminf(u, m.hi[c]));
                 P[c] = (s + 0.5f) * m.dx;
                 for (int d = 0; d < 3; d++) T[c][d] = C[d][c];
@@ -521,10 +521,10 @@ __global__ void k_coef_p(MapP m, float4* __restrict__ g) {
 }
 
 // face map on the packed layout
-// (ED4 / EDGE: at most 128 registers, 4 CTAs per SM, measured faster than
-// the unbounded build; the ED8 form needs fewer registers unbounded)
+// (register caps: ED4 / EDGE 128 registers, 4 CTAs per SM; ED8 102, 5 CTAs
+// per SM; both measured faster than the uncapped builds)
 template <int V>
-__global__ void __launch_bounds__(128, V == HV_FULL ? 1 : 4) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
+__global__ void __launch_bounds__(128, V == HV_FULL ? 5 : 4) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
                                                     float* fcy, float* fcz) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(m.nx, m.ny, m.nz)) return;

@@ -25,6 +25,14 @@ namespace edge {
 static inline float clamp_bound(int dim, int minus) { return (float)((double)(dim - minus) - 1e-6); }
 
 EDGE_HD int idx3(int i, int j, int k, int n1, int n2) { return (i * n1 + j) * n2 + k; }
+// x / dx as the reference writes it; when dx is a power of two (every grid
+// spacing 1/res or 256/res of the drivers) the quotient is the exact scaling
+// x * (1/dx), so the multiply gives the same float
+static inline bool pow2f(float x) {
+    int e;
+    return x > 0.0f && frexpf(x, &e) == 0.5f;
+}
+EDGE_D float over_dx(float x, float dx, float inv_dx, bool pow2) { return pow2 ? x * inv_dx : x / dx; }
 // v[a] with constant indices only (a run-time index into a register array
 // or a kernel-parameter array puts it in local memory)
 EDGE_D float sel3(const float v[3], int a) { return a == 0 ? v[0] : (a == 1 ? v[1] : v[2]); }
@@ -124,6 +132,7 @@ struct Mac {
     const float* __restrict__ u[3];
     int nx, ny, nz;
     float dx, inv_dx;
+    int pow2;      // dx is a power of two
     float hi0[3];  // axis d, BL = 0   (the face field normal to d): dim = n_d + 1
     float hi5[3];  // axis d, BL = 0.5 (a face field tangential to d): dim = n_d
 };
@@ -132,7 +141,7 @@ static inline Mac make_mac(const float* ux, const float* uy, const float* uz, in
     Mac m;
     m.u[0] = ux; m.u[1] = uy; m.u[2] = uz;
     m.nx = nx; m.ny = ny; m.nz = nz;
-    m.dx = dx; m.inv_dx = 1.0f / dx;
+    m.dx = dx; m.inv_dx = 1.0f / dx; m.pow2 = pow2f(dx);
     int n[3] = {nx, ny, nz};
     for (int d = 0; d < 3; d++) {
         m.hi0[d] = clamp_bound(n[d] + 1, 2);
@@ -145,7 +154,8 @@ static inline Mac make_mac(const float* ux, const float* uy, const float* uz, in
 // gradients of u_x, u_y, u_z.
 template <bool GRAD>
 EDGE_D void mac_sample(const Mac& m, const float p[3], float v[3], float G[3][3]) {
-    float q[3] = {p[0] / m.dx, p[1] / m.dx, p[2] / m.dx};
+    float q[3] = {over_dx(p[0], m.dx, m.inv_dx, m.pow2), over_dx(p[1], m.dx, m.inv_dx, m.pow2),
+                  over_dx(p[2], m.dx, m.inv_dx, m.pow2)};
     Axis3 A0[3], A5[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -162,12 +172,13 @@ EDGE_D void mac_sample(const Mac& m, const float p[3], float v[3], float G[3][3]
 // ---------------------------------------------------------------------------
 struct Dye {
     int nx, ny, nz;
-    float dx;
+    float dx, inv_dx;
+    int pow2;
     float hi[3];  // dim-1-eps
 };
 static inline Dye make_dye(int nx, int ny, int nz, float dx) {
     Dye d;
-    d.nx = nx; d.ny = ny; d.nz = nz; d.dx = dx;
+    d.nx = nx; d.ny = ny; d.nz = nz; d.dx = dx; d.inv_dx = 1.0f / dx; d.pow2 = pow2f(dx);
     d.hi[0] = clamp_bound(nx, 1);
     d.hi[1] = clamp_bound(ny, 1);
     d.hi[2] = clamp_bound(nz, 1);
@@ -180,7 +191,8 @@ struct Lin8 {
 EDGE_D Lin8 lin_setup(const Dye& d, const float p[3]) {
     Lin8 L;
     float s[3];
-    float u[3] = {p[0] / d.dx - 0.5f, p[1] / d.dx - 0.5f, p[2] / d.dx - 0.5f};
+    float u[3] = {over_dx(p[0], d.dx, d.inv_dx, d.pow2) - 0.5f, over_dx(p[1], d.dx, d.inv_dx, d.pow2) - 0.5f,
+                  over_dx(p[2], d.dx, d.inv_dx, d.pow2) - 0.5f};
 #pragma unroll
     for (int a = 0; a < 3; a++) s[a] = fmaxf(1.0f, fminf(u[a], d.hi[a]));
     float iu = floorf(s[0]), iv = floorf(s[1]), iw = floorf(s[2]);
@@ -237,7 +249,8 @@ struct MapF {
     const float* __restrict__ dT[3];
     const float* __restrict__ d2T[3];
     int nx, ny, nz;
-    float dx;
+    float dx, inv_dx;
+    int pow2;
     float hi[3];  // dim-2-eps
 };
 static inline MapF make_map(const float* psi, const float* const T[3], const float* const dT[3],
@@ -249,7 +262,7 @@ static inline MapF make_map(const float* psi, const float* const T[3], const flo
         m.dT[c] = dT ? dT[c] : nullptr;
         m.d2T[c] = d2T ? d2T[c] : nullptr;
     }
-    m.nx = nx; m.ny = ny; m.nz = nz; m.dx = dx;
+    m.nx = nx; m.ny = ny; m.nz = nz; m.dx = dx; m.inv_dx = 1.0f / dx; m.pow2 = pow2f(dx);
     m.hi[0] = clamp_bound(nx, 2);
     m.hi[1] = clamp_bound(ny, 2);
     m.hi[2] = clamp_bound(nz, 2);
@@ -345,7 +358,8 @@ EDGE_D void hcoef(const MapF& m, int comp, int ii, int jj, int kk, int im, int i
 // the 2x2x2 corner stencil are contracted axis by axis (z, then y, then x).
 template <int VARIANT, bool GRAD>
 EDGE_D void hermite3(const MapF& m, const float p[3], float val[3], float grad[3][3]) {
-    float q[3] = {p[0] / m.dx - 0.5f, p[1] / m.dx - 0.5f, p[2] / m.dx - 0.5f};
+    float q[3] = {over_dx(p[0], m.dx, m.inv_dx, m.pow2) - 0.5f, over_dx(p[1], m.dx, m.inv_dx, m.pow2) - 0.5f,
+                  over_dx(p[2], m.dx, m.inv_dx, m.pow2) - 0.5f};
     HAxis X = haxis(q[0], m.hi[0], m.nx), Y = haxis(q[1], m.hi[1], m.ny), Z = haxis(q[2], m.hi[2], m.nz);
 #pragma unroll
     for (int comp = 0; comp < 3; comp++) {
@@ -426,14 +440,15 @@ struct MapP {
     const float4* __restrict__ g;  // planes, plane q at g + q * n
     int n;                          // cells
     int nx, ny, nz;
-    float dx;
+    float dx, inv_dx;
+    int pow2;
     float hi[3];
 };
 static inline MapP make_mapp(const float* planes, int nx, int ny, int nz, float dx) {
     MapP m;
     m.g = reinterpret_cast<const float4*>(planes);
     m.n = nx * ny * nz;
-    m.nx = nx; m.ny = ny; m.nz = nz; m.dx = dx;
+    m.nx = nx; m.ny = ny; m.nz = nz; m.dx = dx; m.inv_dx = 1.0f / dx; m.pow2 = pow2f(dx);
     m.hi[0] = clamp_bound(nx, 2);
     m.hi[1] = clamp_bound(ny, 2);
     m.hi[2] = clamp_bound(nz, 2);
@@ -533,7 +548,8 @@ EDGE_D void hcoef_p(const MapP& m, int ii, int jj, int kk, int im, int ip, int j
 // three components.
 template <int VARIANT, bool GRAD>
 EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[3][3]) {
-    float q[3] = {p[0] / m.dx - 0.5f, p[1] / m.dx - 0.5f, p[2] / m.dx - 0.5f};
+    float q[3] = {over_dx(p[0], m.dx, m.inv_dx, m.pow2) - 0.5f, over_dx(p[1], m.dx, m.inv_dx, m.pow2) - 0.5f,
+                  over_dx(p[2], m.dx, m.inv_dx, m.pow2) - 0.5f};
     HAxis X = haxis(q[0], m.hi[0], m.nx), Y = haxis(q[1], m.hi[1], m.ny), Z = haxis(q[2], m.hi[2], m.nz);
     float v[3] = {0.f, 0.f, 0.f}, gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
 #pragma unroll

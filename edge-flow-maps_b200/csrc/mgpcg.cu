@@ -223,6 +223,7 @@ struct Zs<float> {
         *reinterpret_cast<float4*>(b + e) = make_float4(v[0], v[1], v[2], v[3]);
     }
     static EDGE_D void st2(float* b, int e, float x, float y) { *reinterpret_cast<float2*>(b + e) = make_float2(x, y); }
+    static EDGE_D float2 ld2(const float* b, int e) { return __ldg(reinterpret_cast<const float2*>(b + e)); }
 };
 template <>
 struct Zs<__nv_bfloat16> {
@@ -246,6 +247,10 @@ struct Zs<__nv_bfloat16> {
     static EDGE_D void st2(float* b, int e, float x, float y) {
         *reinterpret_cast<__nv_bfloat162*>(h(b) + e) = __floats2bfloat162_rn(x, y);
     }
+    static EDGE_D float2 ld2(const float* b, int e) {
+        const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(h(b) + e);
+        return make_float2(__low2float(v), __high2float(v));
+    }
 };
 // r of a level: FP32 at level 0, else the level storage type
 template <class ZT>
@@ -258,6 +263,7 @@ struct Zc;
 template <>
 struct Zc<float> {
     static EDGE_D float ld(const float* b, int e) { return __ldcg(b + e); }
+    static EDGE_D float2 ld2(const float* b, int e) { return __ldcg(reinterpret_cast<const float2*>(b + e)); }
     static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
         float4 t = __ldcg(reinterpret_cast<const float4*>(b + e));
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
@@ -268,6 +274,11 @@ struct Zc<__nv_bfloat16> {
     static EDGE_D float ld(const float* b, int e) {
         unsigned short u = __ldcg(reinterpret_cast<const unsigned short*>(b) + e);
         return __bfloat162float(__ushort_as_bfloat16(u));
+    }
+    static EDGE_D float2 ld2(const float* b, int e) {
+        unsigned u = __ldcg(reinterpret_cast<const unsigned*>(reinterpret_cast<const unsigned short*>(b) + e));
+        const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(&u);
+        return make_float2(__low2float(v), __high2float(v));
     }
     static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
         const uint2 u = __ldcg(reinterpret_cast<const uint2*>(reinterpret_cast<const __nv_bfloat16*>(b) + e));
@@ -879,6 +890,90 @@ struct NoParent {
     EDGE_D float operator()(int, int, int) const { return 0.0f; }
 };
 
+// The prolongation terms a quad's six neighbour directions take
+// (prolongate, mgpcg.py:155-158: the coarse z at each neighbour's parent),
+// gathered with vector loads: when the fine row length is a multiple of 8,
+// the parents of cells k = 2 (kk0 + m) + p, m = 0..3, are coarse cells
+// K = kk0 + m of at most three coarse columns, two consecutive slots of each
+// colour plane per column.  ld2(plane, slot) returns slots slot, slot + 1 of
+// a coarse plane, ld1(plane, slot) one.  Values of neighbours outside the grid
+// are 0 and never used.
+struct QParents {
+    float xp[4], xm[4], yp[4], ym[4], zp[4], zm[4];
+};
+template <class LV, class CV, class L2, class L1>
+EDGE_D void quad_parents(const LV& F, const CV& C, int i, int j, int kk0, int p, L2 ld2, L1 ld1, QParents& o) {
+    const int I = i >> 1, J = j >> 1, s = kk0 >> 1;
+    auto col = [&](int Ic, int Jc, float(&v)[4]) {
+        const int base = (Ic * C.n1 + Jc) * C.H + s;
+        const int A = (Ic + Jc) & 1;
+        const float2 a = ld2(A, base), b = ld2(A ^ 1, base);
+        v[0] = a.x; v[1] = b.x; v[2] = a.y; v[3] = b.y;
+    };
+    float c[4];
+    col(I, J, c);
+#pragma unroll
+    for (int m = 0; m < 4; m++) { o.xp[m] = o.xm[m] = o.yp[m] = o.ym[m] = c[m]; }
+    // the x and y neighbours on the side of the other parent
+    if (i & 1) {
+        if (i + 1 < F.n0) col(I + 1, J, o.xp);
+    } else if (i > 0) {
+        col(I - 1, J, o.xm);
+    }
+    if (j & 1) {
+        if (j + 1 < F.n1) col(I, J + 1, o.yp);
+    } else if (j > 0) {
+        col(I, J - 1, o.ym);
+    }
+    // z: parents of k + 1 and k - 1 are K = kk0 + m + p and kk0 + m + p - 1
+    const int A = (I + J) & 1;
+    const int rowb = (I * C.n1 + J) * C.H;
+    const float lo = (p == 0 && kk0 > 0) ? ld1(A ^ 1, rowb + s - 1) : 0.0f;            // K = kk0 - 1
+    const float hi = (p == 1 && 2 * kk0 + 8 < F.n2) ? ld1(A, rowb + s + 2) : 0.0f;    // K = kk0 + 4
+    const float e6[6] = {lo, c[0], c[1], c[2], c[3], hi};                               // K = kk0 - 1 .. kk0 + 4
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        o.zp[m] = e6[m + 1 + p];
+        o.zm[m] = e6[m + p];
+    }
+}
+
+// quad_nbr_sum with the prolongation terms of quad_parents
+template <class LV, class V4, class V1>
+EDGE_D void quad_nbr_sum_pro(const LV& L, const Quad& q, int p, const unsigned (&code)[4], V4 v4, V1 v1,
+                             const QParents& P, float (&ns)[4]) {
+    const int sx = L.n1 * L.H;
+    float xp[4] = {0, 0, 0, 0}, xm[4] = {0, 0, 0, 0}, yp[4] = {0, 0, 0, 0}, ym[4] = {0, 0, 0, 0};
+    float ov[4], o[6];
+    if (q.i < L.n0 - 1) v4(q.t0 + sx, xp);
+    if (q.i > 0) v4(q.t0 - sx, xm);
+    if (q.j < L.n1 - 1) v4(q.t0 + L.H, yp);
+    if (q.j > 0) v4(q.t0 - L.H, ym);
+    v4(q.t0, ov);
+    o[0] = (p == 0 && q.kk0 > 0) ? v1(q.t0 - 1) : 0.0f;
+    o[1] = ov[0]; o[2] = ov[1]; o[3] = ov[2]; o[4] = ov[3];
+    o[5] = (p == 1 && q.kk0 + 4 < L.H) ? v1(q.t0 + 4) : 0.0f;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const unsigned c = code[m];
+        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = o[m + 1 + p], vzm = o[m + p];
+        if (c & NB_XP) vxp = vxp + P.xp[m];
+        if (c & NB_XM) vxm = vxm + P.xm[m];
+        if (c & NB_YP) vyp = vyp + P.yp[m];
+        if (c & NB_YM) vym = vym + P.ym[m];
+        if (c & NB_ZP) vzp = vzp + P.zp[m];
+        if (c & NB_ZM) vzm = vzm + P.zm[m];
+        float r = 0.0f;
+        if (c & NB_XP) r += vxp;
+        if (c & NB_XM) r += vxm;
+        if (c & NB_YP) r += vyp;
+        if (c & NB_YM) r += vym;
+        if (c & NB_ZP) r += vzp;
+        if (c & NB_ZM) r += vzm;
+        ns[m] = r;
+    }
+}
+
 // The coarse levels lc..L-1 of a V-cycle in one thread block out of shared
 // memory (same red-black layout): down sweeps + restriction, 20 bottom
 // sweeps, prolongation + up sweeps (mgpcg.py:177-195); z[lc] is written back
@@ -981,8 +1076,18 @@ EDGE_D void coarse_body(const G& g, const Lvl* lvs, int L, int lc, float* sh, CL
                         o[0] = w.x; o[1] = w.y; o[2] = w.z; o[3] = w.w;
                     };
                     auto v1 = [&](int e) { return zo[e]; };
-                    if (mode == 1) quad_nbr_sum<false>(q, qd, p, code, v4, v1, NoParent(), ns);
-                    else if (mode == 2) quad_nbr_sum<true>(q, qd, p, code, v4, v1, pz, ns);
+                    if (mode == 1) {
+                        quad_nbr_sum<false>(q, qd, p, code, v4, v1, NoParent(), ns);
+                    } else if (mode == 2 && q.n2 % 8 == 0) {
+                        QParents P;
+                        quad_parents(
+                            q, u, qd.i, qd.j, qd.kk0, p,
+                            [&](int pl, int e) { return *reinterpret_cast<const float2*>((pl ? zc1 : zc0) + e); },
+                            [&](int pl, int e) { return (pl ? zc1 : zc0)[e]; }, P);
+                        quad_nbr_sum_pro(q, qd, p, code, v4, v1, P, ns);
+                    } else if (mode == 2) {
+                        quad_nbr_sum<true>(q, qd, p, code, v4, v1, pz, ns);
+                    }
                     float4 rv = *reinterpret_cast<const float4*>(r + qd.t0);
                     float4 zv = *reinterpret_cast<const float4*>(z + qd.t0);
                     float rr[4] = {rv.x, rv.y, rv.z, rv.w}, zz[4] = {zv.x, zv.y, zv.z, zv.w};
@@ -1188,7 +1293,12 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
         if (MODE != HS_FIRST) {
             auto v4 = [&](int e, float(&o)[4]) { Zs<ZT>::ld4(zo, e, o); };
             auto v1 = [&](int e) { return Zs<ZT>::ld(zo, e); };
-            if (MODE == HS_PROLONG)
+            if (MODE == HS_PROLONG && L.n2 % 8 == 0) {
+                QParents P;
+                quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return Zs<ZT>::ld2(pick(C.z, pl), e); },
+                             [&](int pl, int e) { return Zs<ZT>::ld(pick(C.z, pl), e); }, P);
+                quad_nbr_sum_pro(L, q, p, code, v4, v1, P, ns);
+            } else if (MODE == HS_PROLONG)
                 quad_nbr_sum<true>(L, q, p, code, v4, v1,
                                    [&](int i, int j, int k) { return parent_zg<ZT>(C, i, j, k); }, ns);
             else
@@ -1453,7 +1563,12 @@ EDGE_D void cl_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int t0, 
         Zc<ZT>::ld4(rs, q.t0, rv);
         auto v4 = [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); };
         auto v1 = [&](int e) { return Zc<ZT>::ld(zo, e); };
-        if (MODE == HS_PROLONG)
+        if (MODE == HS_PROLONG && L.n2 % 8 == 0) {
+            QParents P;
+            quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return Zc<ZT>::ld2(pick(C.z, pl), e); },
+                         [&](int pl, int e) { return Zc<ZT>::ld(pick(C.z, pl), e); }, P);
+            quad_nbr_sum_pro(L, q, p, code, v4, v1, P, ns);
+        } else if (MODE == HS_PROLONG)
             quad_nbr_sum<true>(L, q, p, code, v4, v1, [&](int i, int j, int k) { return parent_zc<ZT>(C, i, j, k); },
                                ns);
         else
