@@ -311,7 +311,7 @@ PCG_REL = 1e-6
 # launches of that solve (4 CG iterations), one ncu capture of
 # `bench.py --pcg-only` with the host-driven solver loop (EDGE_MGPCG_EAGER=1);
 # ncu flushes the caches before every launch, so this is the cold-L2 figure
-PCG_TRAFFIC = 1509646080
+PCG_TRAFFIC = 1379416320
 
 
 def pcg_measure(res, reps=5):
