@@ -100,6 +100,7 @@ class EdgeSim:
         self.frame_idx = 0
         self.last_dt = 0.0
         self.last_iters = (None, None)
+        self._io = None  # step_host: events and copy stream of the host round trip
 
     def _map_set(self):
         r = self.res
@@ -227,6 +228,9 @@ class EdgeSim:
         self.last_dt = curr_dt
         dx = self.dx
         reinit = j == 0
+        io = self._io
+        if io is not None and (reinit or self.emitters is not None):
+            torch.cuda.current_stream().wait_event(io["smoke_in"])
         if reinit:
             # run_edge.py:616-625
             ops.reset_faces(self.res, dx, self.phi, self.F)
@@ -283,11 +287,18 @@ class EdgeSim:
             # dye: smoke = smoke_init(psi); err = 0.5*(smoke(phi) - smoke_init);
             # smoke - err(psi), clamped                     run_edge.py:670, 677-689
             side.wait_event(ev_map)
+            if io is not None:
+                side.wait_event(io["smoke_in"])  # the dye chain overwrites the dye the copy brings in
             ops.pullback_dye(self.init_smoke, dx, self.fpsi, self.smoke)
             ops.pullback_dye(self.smoke, dx, self.phi, self.err_smoke, init=self.init_smoke, scale=0.5)
             ops.pullback_dye(self.err_smoke, dx, self.fpsi, self.smoke, sub=self.smoke, clampsrc=self.init_smoke)
             ev_dye = torch.cuda.Event()
             ev_dye.record(side)
+        if io is not None:
+            # the step's dye is final: copy it out while the velocity chain runs
+            io["copy"].wait_event(ev_dye)
+            with torch.cuda.stream(io["copy"]):
+                io["host_smoke"].copy_(self.smoke, non_blocking=True)
         # u = (grad psi)^T u_init(psi)                                 run_edge.py:669
         ops.pullback_u(self.init_u, dx, self.fpsi, self.fcol, self.u)
         # err = 0.5*(F^T u(phi) - u_init)                             run_edge.py:671-676
@@ -310,6 +321,41 @@ class EdgeSim:
             self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
         tm.stop("substep")
         return curr_dt
+
+    def step_host(self, host_u, host_smoke, dt=None):
+        """One step whose state comes from and goes back to pinned host
+        buffers (the three face velocity arrays and the dye), as a caller
+        that keeps the fields on the host drives the simulation.  The copies
+        run on a copy stream beside the computation: the velocity in before
+        the step starts; the dye in while the step's first half runs (a step
+        reads the incoming dye only at a reinitialisation or with emitters,
+        and otherwise the dye chain overwrites it, so only those wait for
+        it); the dye out as soon as the dye chain ends, during the velocity
+        chain and the projection; the velocity out at the end.  Returns dt;
+        the host buffers hold the step's results once the current stream and
+        `self.copy_stream` have completed (torch.cuda.synchronize())."""
+        if not hasattr(self, "copy_stream"):
+            self.copy_stream = torch.cuda.Stream(device=self.u[0].device)
+        main = torch.cuda.current_stream()
+        cs = self.copy_stream
+        cs.wait_event(main.record_event())  # the previous step's kernels are done with the buffers
+        with torch.cuda.stream(cs):
+            for d, h in zip(self.u, host_u):
+                d.copy_(h, non_blocking=True)
+            u_in = cs.record_event()
+            self.smoke.copy_(host_smoke, non_blocking=True)
+            smoke_in = cs.record_event()
+        main.wait_event(u_in)
+        self._io = {"copy": cs, "smoke_in": smoke_in, "host_smoke": host_smoke}
+        try:
+            dt = self.step(dt=dt)
+        finally:
+            self._io = None
+        cs.wait_event(main.record_event())
+        with torch.cuda.stream(cs):
+            for h, d in zip(host_u, self.u):
+                h.copy_(d, non_blocking=True)
+        return dt
 
     def _particles_forces(self, dt):
         """run_edge.py:627-641: G2P, particle update, P2G drag, viscous force."""
