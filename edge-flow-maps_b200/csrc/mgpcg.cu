@@ -136,6 +136,16 @@ EDGE_D bool running(const G& g) { return *((volatile int*)&g.st->status) == ST_R
 
 // every solver kernel counts itself once (block 0, thread 0), including the
 // ones that return early once the loop has finished
+// Programmatic dependent launch: the CG-loop kernels are launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization, so the next kernel's
+// launch and block scheduling overlap this one's tail; each of them waits
+// here for the previous kernel to complete (and its writes to be visible)
+// before reading anything, and lets the next one be scheduled right away.
+EDGE_D void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 EDGE_D void count_launch(SolveState* st) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) atomicAdd(&st->kernels, 1ull);
 }
@@ -593,6 +603,7 @@ EDGE_D unsigned code_at(const Lvl& L, int plane, int e, int i, int j, int k) {
 // reference's separate kernels round them.
 template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
+    pdl_enter();
     count_launch(g.st);
     // The loop stops unless the iteration's last kernel completes its
     // reduction and asks to continue: a lost reduction can never spin.
@@ -648,6 +659,7 @@ __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
 // (mgpcg_solid.py:197-202).
 template <bool SOLID>
 __global__ void __launch_bounds__(256) k_cg_xr(G g, Lvl L, Fine f) {
+    pdl_enter();
     count_launch(g.st);
     if (!running(g)) return;
     SolveState* st = g.st;
@@ -712,6 +724,7 @@ enum { HS_FIRST = 0, HS_PLAIN = 1, HS_PROLONG = 2, HS_ZR = 3 };
 
 template <int MODE, bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, int color) {
+    pdl_enter();
     count_launch(g.st);
     if (!running(g)) {
         if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
@@ -769,6 +782,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
 // half sweep of the coarse level (z = r / n_fluid on colour 0).
 template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0, int first) {
+    pdl_enter();
     count_launch(g.st);
     if (!running(g)) return;
     const float mean = level0 ? g.st->mean : 0.0f;
@@ -1257,6 +1271,7 @@ EDGE_D void coarse_body(const G& g, const Lvl* lvs, int L, int lc, float* sh, CL
 
 template <bool ZR, bool SOLID, class ZT>
 __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
+    pdl_enter();
     extern __shared__ float sh[];
     __shared__ CLvl cl[16];
     __shared__ Lvl sl[16];
@@ -1272,6 +1287,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
 
 template <int MODE, bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, int color) {
+    pdl_enter();
     count_launch(g.st);
     if (!running(g)) {
         if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
@@ -1335,6 +1351,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
 
 template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
+    pdl_enter();
     count_launch(g.st);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         set_cond(g, 0);
@@ -1398,6 +1415,7 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
 
 template <bool SOLID>
 __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
+    pdl_enter();
     count_launch(g.st);
     if (!running(g)) return;
     SolveState* st = g.st;
@@ -1456,6 +1474,7 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
 // are slots K0..K0+3 of both planes in the four fine rows (2I+a, 2J+b)
 template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0, int first) {
+    pdl_enter();
     count_launch(g.st);
     if (!running(g)) return;
     const float mean = level0 ? g.st->mean : 0.0f;
@@ -1643,6 +1662,7 @@ constexpr int kMidThreads = 512;
 
 template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(kMidThreads) k_mid(G g, Levels a, int lm, int lcc) {
+    pdl_enter();
     extern __shared__ float sh[];
     __shared__ CLvl cl[16];
     __shared__ Lvl sl[16];
@@ -1979,6 +1999,22 @@ int prepare_coarse_kernels(const Ctx& c) {
     return EDGE_OK;
 }
 
+// launch with the programmatic-dependent-launch attribute (see pdl_enter)
+template <class... KArgs, class... Args>
+static void launch_pdl(void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // One V-cycle (mgpcg.py:177-195); with final_zr the last kernel also forms
 // z.r and the end-of-iteration bookkeeping (mgpcg.py:263-277).
 template <bool S, class ZT>
@@ -1993,38 +2029,40 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
         const int l0 = l == 0, first = l + 1 < lgroup;
         if (L.vec) {
             const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-            if (l == 0) k_hsweep4<HS_FIRST, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_restrict4<S, ZT><<<rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream>>>(c.g, L, C, l0, first);
+            if (l == 0) launch_pdl(k_hsweep4<HS_FIRST, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            launch_pdl(k_restrict4<S, ZT>, rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream, c.g, L, C, l0, first);
         } else {
             const int g = rgrid(L.P);
-            if (l == 0) k_hsweep<HS_FIRST, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_restrict<S, ZT><<<rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream>>>(c.g, L, C, l0, first);
+            if (l == 0) launch_pdl(k_hsweep<HS_FIRST, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            launch_pdl(k_restrict<S, ZT>, rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream, c.g, L, C, l0, first);
         }
     }
     if (mid) {
         cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute at[1];
+        cudaLaunchAttribute at[2];
         at[0].id = cudaLaunchAttributeClusterDimension;
         at[0].val.clusterDim.x = c.cmid;
         at[0].val.clusterDim.y = 1;
         at[0].val.clusterDim.z = 1;
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
         cfg.gridDim = dim3(c.cmid);
         cfg.blockDim = dim3(kMidThreads);
         cfg.dynamicSmemBytes = c.csmem_mid;
         cfg.stream = stream;
         cfg.attrs = at;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = 2;
         cudaLaunchKernelEx(&cfg, k_mid<S, ZT>, c.g, V, c.lm, c.lcc);
     } else if (final_zr && lc == 0) {
-        k_coarse<true, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
+        launch_pdl(k_coarse<true, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
     } else {
-        k_coarse<false, S, ZT><<<1, 1024, c.csmem, stream>>>(c.g, V);
+        launch_pdl(k_coarse<false, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
     }
     for (int l = lc - 1; l >= 0; l--) {
         const Lvl& L = V.lv[l];
@@ -2033,18 +2071,18 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
         const bool zr = l == 0 && final_zr;
         if (L.vec) {
             const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-            k_hsweep4<HS_PROLONG, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            if (zr) k_hsweep4<HS_ZR, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            else k_hsweep4<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep4<HS_PROLONG, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            if (zr) launch_pdl(k_hsweep4<HS_ZR, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            else launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
         } else {
             const int g = rgrid(L.P);
-            k_hsweep<HS_PROLONG, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 1);
-            if (zr) k_hsweep<HS_ZR, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
-            else k_hsweep<HS_PLAIN, S, ZT><<<g, 256, 0, stream>>>(c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep<HS_PROLONG, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
+            if (zr) launch_pdl(k_hsweep<HS_ZR, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            else launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
         }
     }
 }
@@ -2064,11 +2102,11 @@ void cg_kernels(const Ctx& c, cudaStream_t stream) {
     const Lvl& L = c.lv.lv[0];
     if (L.vec) {
         const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-        k_cg_ap4<S, ZT><<<g, 256, 0, stream>>>(c.g, L, c.f);
-        k_cg_xr4<S><<<g, 256, 0, stream>>>(c.g, L, c.f);
+        launch_pdl(k_cg_ap4<S, ZT>, g, 256, 0, stream, c.g, L, c.f);
+        launch_pdl(k_cg_xr4<S>, g, 256, 0, stream, c.g, L, c.f);
     } else {
-        k_cg_ap<S, ZT><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
-        k_cg_xr<S><<<rgrid(L.P), 256, 0, stream>>>(c.g, L, c.f);
+        launch_pdl(k_cg_ap<S, ZT>, rgrid(L.P), 256, 0, stream, c.g, L, c.f);
+        launch_pdl(k_cg_xr<S>, rgrid(L.P), 256, 0, stream, c.g, L, c.f);
     }
 }
 
