@@ -8,8 +8,9 @@ vtk/pyevtk are not installed), particle/field_<frame>.vtu for the laden
 particle cases, the velocity checkpoints ckpts/vel_{x,y,z}_numpy_<frame>.npy
 (run_edge.py:719-737); and also the dye (smoke_numpy_<frame>.npy, which the
 reference's resume path reads at run_edge.py:565-566 but never writes) and
-the whole simulation state (mapstate_<frame>.pt) for an exact resume in the
-middle of a reinitialisation interval (--from-frame).
+with --save-state the whole simulation state (mapstate_<frame>.pt) for an
+exact resume in the middle of a reinitialisation interval (--from-frame).
+Checkpoints follow the case's ckpt_every (run_edge.py:731).
 """
 import argparse
 import math
@@ -28,20 +29,20 @@ CASES = {
     # run_edge.py:25-77 (case 0 leapfrog, case 1 four vortices; the same two
     # cases in run_ed4.py, run_ed8.py, run_ge.py, run_efm.py)
     0: dict(init="leapfrog", res=(384, 128, 128), visualize_dt=0.1, reinit_every=20, cfl=0.5, total_frames=500,
-            bfecc_clamp=False, ed_eps_frac=0.01),
+            bfecc_clamp=False, ed_eps_frac=0.01, ckpt_every=1),
     1: dict(init="fourvorts", res=(128, 128, 256), visualize_dt=0.1, reinit_every=20, cfl=0.5, total_frames=500,
-            bfecc_clamp=True, ed_eps_frac=0.025),
+            bfecc_clamp=True, ed_eps_frac=0.025, ckpt_every=1),
     # run_edge.py:78-95: delta wing (solid obstacle, MGPCG_Solid_3, dye emitters)
     2: dict(init="delta", res=(256, 128, 128), visualize_dt=0.05, reinit_every=10, cfl=0.5, total_frames=120,
-            bfecc_clamp=True, ed_eps_frac=0.02, only="edge"),
+            bfecc_clamp=True, ed_eps_frac=0.02, only="edge", ckpt_every=1),
     # run_edge.py:96-127 / 128-159: ink circle and ink drop (two-way coupled
     # laden particles); dx = domain_range_y / res_y
     3: dict(init="inkcircle", res=(128, 256, 128), visualize_dt=10.0, reinit_every=60, cfl=0.25, total_frames=300,
-            bfecc_clamp=True, ed_eps_frac=0.02, only="edge", lp=dict(
+            bfecc_clamp=True, ed_eps_frac=0.02, only="edge", ckpt_every=100, lp=dict(
                 case=0, Re=5.5, St=6.6e-5, gravity=1.0, density_ratio=2.0 / 3, erad=35.0, num=1000000,
                 laden_radius=0.01)),
     4: dict(init="inkdrop", res=(256, 512, 256), visualize_dt=10.0, reinit_every=80, cfl=0.25, total_frames=120,
-            bfecc_clamp=True, ed_eps_frac=0.02, only="edge", lp=dict(
+            bfecc_clamp=True, ed_eps_frac=0.02, only="edge", ckpt_every=1, lp=dict(
                 case=1, Re=1000.0, St=5e-5, gravity=1.0, density_ratio=0.6, erad=35.0, num=4000000,
                 laden_radius=0.01)),
 }
@@ -94,6 +95,8 @@ def parse(variant):
     ap.add_argument("--logdir", default="logs")
     ap.add_argument("--from-frame", type=int, default=0,
                     help="resume from this frame's checkpoint in the experiment's ckpts/ (exact with mapstate)")
+    ap.add_argument("--save-state", action="store_true",
+                    help="also write the whole simulation state (mapstate_<frame>.pt) with each checkpoint")
     return ap.parse_args()
 
 
@@ -176,16 +179,19 @@ def main(variant):
         curl(uc, w, dx)
         write_vtks_4channel_smoke(torch.linalg.vector_norm(w, dim=-1).cpu().numpy(), sim.smoke.cpu().numpy(),
                                   vtkdir, frame)
+        if sim.particles is not None:
+            os.makedirs(pdir, exist_ok=True)
+            write_to_vtks_lp(sim.particles["pos"].cpu().numpy(), {}, {}, os.path.join(pdir, "field_{:03d}".format(frame)))
+        if frame % cfg["ckpt_every"] != 0:
+            return
         for c, a in enumerate("xyz"):
             np.save(os.path.join(ckptdir, f"vel_{a}_numpy_{frame}"), sim.u[c].cpu().numpy())
         # the reference's resume path reads this file (run_edge.py:565-566)
         # but never writes it
         np.save(os.path.join(ckptdir, f"smoke_numpy_{frame}"), sim.smoke.cpu().numpy())
-        if sim.particles is not None:
-            os.makedirs(pdir, exist_ok=True)
-            write_to_vtks_lp(sim.particles["pos"].cpu().numpy(), {}, {}, os.path.join(pdir, "field_{:03d}".format(frame)))
         # the whole state, for an exact resume in the middle of an interval
-        torch.save(sim.state_dict(), os.path.join(ckptdir, f"mapstate_{frame}.pt"))
+        if args.save_state:
+            torch.save(sim.state_dict(), os.path.join(ckptdir, f"mapstate_{frame}.pt"))
 
     if start <= 0:
         save(0)
