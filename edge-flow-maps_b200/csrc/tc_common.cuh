@@ -79,6 +79,21 @@ EDGE_D bool mbar_wait(uint32_t mbar, uint32_t parity, int max_polls) {
     return false;
 }
 
+// expect `bytes` of asynchronous copies on mbar (one arrival)
+EDGE_D void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// bulk copy (TMA, no tensor map, no multicast) of `bytes` (a multiple of 16,
+// both addresses 16-byte aligned) from global memory into this CTA's shared
+// memory, completion counted on mbar
+EDGE_D void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"((unsigned long long)__cvta_generic_to_global(src)), "r"(bytes), "r"(mbar)
+        : "memory");
+}
+
 // generic-proxy shared-memory writes -> visible to the tensor cores
 EDGE_D void fence_smem_to_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 EDGE_D void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }

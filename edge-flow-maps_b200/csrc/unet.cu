@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 
 #include "tc_common.cuh"
@@ -303,6 +304,154 @@ __global__ void __launch_bounds__(128) k_conv_tc(Geo g, ConvIn in0, ConvIn in1, 
     if (warp == 0) tc::tmem_free(tbase, NCOLS);
 }
 
+// The same convolution with the staging done by the bulk-copy engine into one
+// or two stages: thread 0 issues, per phase (input, dx), one 2080-byte bulk copy per
+// (dy, channel chunk) row and one for the phase's weights into a stage, the
+// MMAs of a phase read the other stage while the next phase's copies land,
+// and the epilogue of a tile overlaps the copies of the next tile's first
+// phase (two stages).  Stage contents, descriptors and the MMA sequence are k_conv_tc's,
+// so the result is identical.  With nstage = 1 (the default) a phase's
+// copies wait for the previous phase's MMAs; the other blocks on the SM fill
+// that gap.
+template <int COUT>
+__global__ void __launch_bounds__(128) k_conv_bulk(Geo g, ConvIn in0, ConvIn in1, int nin,
+                                                   const float* __restrict__ bias, int flags,
+                                                   __nv_bfloat16* __restrict__ y, int* err, int nstage,
+                                                   uint32_t stage_bytes) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[2], mdone[2], tdone, fin;
+    __shared__ uint32_t tslot;
+    __shared__ int s_bad;
+    constexpr uint32_t NCOLS = COUT < 32 ? 32 : COUT;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nchmax = max(in0.cin, nin > 1 ? in1.cin : 0) / 8;
+    const uint32_t wofs = 3u * nchmax * kSegBytes;
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), NCOLS);
+    if (tid == 0) {
+        for (int s = 0; s < 2; s++) {
+            tc::mbar_init(tc::smem_u32(&full[s]), 1);
+            tc::mbar_init(tc::smem_u32(&mdone[s]), 1);
+        }
+        tc::mbar_init(tc::smem_u32(&tdone), 1);
+        tc::mbar_init(tc::smem_u32(&fin), 1);
+        s_bad = 0;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = tslot;
+    const uint32_t idesc = tc::idesc_bf16(128, COUT, false, false);
+    const uint32_t sbase = tc::smem_u32(smem);
+    const int nph = 3 * nin;
+    // thread 0's copy issue for phase ph of tile into stage s
+    auto issue = [&](int tile, int ph, int s) {
+        const ConvIn in = ph >= 3 ? in1 : in0;
+        const int nch = in.cin / 8, dxi = ph % 3;
+        const uint32_t st = sbase + (uint32_t)s * stage_bytes, fb = tc::smem_u32(&full[s]);
+        tc::mbar_expect_tx(fb, 3u * nch * kSegBytes + 9u * nch * COUT * 16);
+        const long long base = (long long)tile * 128 + (dxi - 1) * (long long)g.Sx - g.Sy - 1;
+        for (int dyi = 0; dyi < 3; dyi++)
+            for (int q = 0; q < nch; q++)
+                tc::bulk_g2s(st + (uint32_t)(dyi * nch + q) * kSegBytes, in.x + act_off(g, q, base + dyi * g.Sy),
+                             kSegBytes, fb);
+        tc::bulk_g2s(st + wofs, reinterpret_cast<const uint4*>(in.w) + (size_t)dxi * 9 * nch * COUT,
+                     9u * nch * COUT * 16, fb);
+    };
+    uint32_t fpar[2] = {0, 0}, mpar[2] = {0, 0}, tpar = 0;
+    bool inflight[2] = {false, false};  // thread 0: a stage's copies not yet waited for
+    int n = 0;                          // thread 0: phases issued to the tensor cores so far
+    bool bad = false;
+    if (tid == 0 && (int)blockIdx.x < g.ntiles) {
+        issue(blockIdx.x, 0, 0);
+        inflight[0] = true;
+    }
+    for (int tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+        if (tid == 0) {
+            int nmma = 0;
+            for (int ph = 0; ph < nph; ph++, n++) {
+                const int s = nstage == 2 ? (n & 1) : 0;
+                if (!tc::mbar_wait(tc::smem_u32(&full[s]), fpar[s], kMaxPolls)) { s_bad = 1; break; }
+                fpar[s] ^= 1;
+                inflight[s] = false;
+                tc::fence_after_sync();
+                const int nch = (ph >= 3 ? in1.cin : in0.cin) / 8;
+                const uint32_t a0 = sbase + (uint32_t)s * stage_bytes, b0 = a0 + wofs;
+                for (int dyi = 0; dyi < 3; dyi++)
+                    for (int dzi = 0; dzi < 3; dzi++)
+                        for (int ks = 0; ks < nch / 2; ks++) {
+                            const uint64_t da =
+                                tc::sdesc(a0 + (uint32_t)((dyi * nch + 2 * ks) * kSegBytes + dzi * 16), kSegBytes, 128);
+                            const uint64_t db =
+                                tc::sdesc(b0 + (uint32_t)(((dyi * 3 + dzi) * nch + 2 * ks) * COUT * 16), COUT * 16, 128);
+                            tc::mma_bf16(tbase, da, db, idesc, nmma > 0 ? 1u : 0u);
+                            nmma++;
+                        }
+                tc::commit(tc::smem_u32(&mdone[s]));
+                if (ph == nph - 1) tc::commit(tc::smem_u32(&tdone));
+                // the next phase (of this tile, or the first of this block's next tile)
+                int nt = tile, np = ph + 1;
+                if (np == nph) { nt = tile + gridDim.x; np = 0; }
+                if (nt < g.ntiles) {
+                    const int s2 = nstage == 2 ? ((n + 1) & 1) : 0;
+                    // the stage was last read by phase n - 1 (two stages) or n (one)
+                    if (nstage == 1 || n >= 1) {
+                        if (!tc::mbar_wait(tc::smem_u32(&mdone[s2]), mpar[s2], kMaxPolls)) { s_bad = 1; break; }
+                        mpar[s2] ^= 1;
+                    }
+                    issue(nt, np, s2);
+                    inflight[s2] = true;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_bad) { bad = true; break; }
+        {
+            bool ok = tc::mbar_wait(tc::smem_u32(&tdone), tpar, kMaxPolls);
+            tpar ^= 1;
+            if (__syncthreads_or(!ok)) { bad = true; break; }
+        }
+        tc::fence_after_sync();
+        const int v0 = tile * 128;
+        const int v = v0 + 32 * warp + lane;
+        int x, yy, z;
+        const bool in_dom = interior(g, v, x, yy, z);
+#pragma unroll
+        for (int c0 = 0; c0 < COUT; c0 += 16) {
+            float acc[16];
+            tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                uint4* dst = reinterpret_cast<uint4*>(y + act_off(g, (c0 >> 3) + h, v));
+                float old[8] = {0, 0, 0, 0, 0, 0, 0, 0}, o[8];
+                if (flags & 2) unpack8(*dst, old);
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    float t = acc[8 * h + j] + (bias ? bias[c0 + 8 * h + j] : 0.0f);
+                    if (flags & 1) t = fmaxf(t, 0.0f);
+                    t += old[j];
+                    o[j] = in_dom ? t : 0.0f;
+                }
+                *dst = pack8(o);
+            }
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+    }
+    if (bad && tid == 0) {
+        atomicExch(err, 1);
+        // the copies still in flight land, and every MMA issued completes, before
+        // the block exits and frees its tensor memory (bounded waits)
+        for (int s = 0; s < 2; s++)
+            if (inflight[s]) tc::mbar_wait(tc::smem_u32(&full[s]), fpar[s], kMaxPolls);
+        tc::commit(tc::smem_u32(&fin));
+        tc::mbar_wait(tc::smem_u32(&fin), 0, kMaxPolls);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tbase, NCOLS);
+}
+
 // ===========================================================================
 // Tensor-core weight gradient
 // ===========================================================================
@@ -436,6 +585,11 @@ __global__ void __launch_bounds__(256) k_conv_first(Geo g, const float* __restri
                                                     __nv_bfloat16* __restrict__ y) {
     const int n = g.X * g.Y * g.Z;
     const float s = *scale;
+    // the weights tap-major in shared memory: one tap's 16 outputs are four
+    // broadcast 16-byte loads
+    __shared__ __align__(16) float ws[27 * 16];
+    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e] = w[(e % 16) * 27 + e / 16];
+    __syncthreads();
     GSTRIDE(t, n) {
         const int z = (int)(t % g.Z), yy = (int)((t / g.Z) % g.Y), x = (int)(t / ((long long)g.Y * g.Z));
         float acc[16];
@@ -446,8 +600,15 @@ __global__ void __launch_bounds__(256) k_conv_first(Geo g, const float* __restri
             const int a = x + tap / 9 - 1, b = yy + (tap / 3) % 3 - 1, c = z + tap % 3 - 1;
             const bool ok = a >= 0 && a < g.X && b >= 0 && b < g.Y && c >= 0 && c < g.Z;
             const float in = ok ? r[((size_t)a * g.Y + b) * g.Z + c] * s : 0.0f;
+            const float4* wt = reinterpret_cast<const float4*>(ws + tap * 16);
 #pragma unroll
-            for (int co = 0; co < 16; co++) acc[co] = fmaf(__ldg(w + co * 27 + tap), in, acc[co]);
+            for (int c4 = 0; c4 < 4; c4++) {
+                const float4 wv = wt[c4];
+                acc[4 * c4 + 0] = fmaf(wv.x, in, acc[4 * c4 + 0]);
+                acc[4 * c4 + 1] = fmaf(wv.y, in, acc[4 * c4 + 1]);
+                acc[4 * c4 + 2] = fmaf(wv.z, in, acc[4 * c4 + 2]);
+                acc[4 * c4 + 3] = fmaf(wv.w, in, acc[4 * c4 + 3]);
+            }
         }
         const int v = pvox(g, x, yy, z);
 #pragma unroll
@@ -467,6 +628,9 @@ __global__ void __launch_bounds__(256) k_conv_last(Geo g, const __nv_bfloat16* _
                                                    const float* __restrict__ scale, float* __restrict__ z) {
     const int n = g.X * g.Y * g.Z;
     const float inv = 1.0f / *scale;
+    __shared__ __align__(16) float ws[27 * 16];  // tap-major, as in k_conv_first
+    for (int e = threadIdx.x; e < 27 * 16; e += blockDim.x) ws[e] = w[(e % 16) * 27 + e / 16];
+    __syncthreads();
     GSTRIDE(t, n) {
         const int zz = (int)(t % g.Z), yy = (int)((t / g.Z) % g.Y), x = (int)(t / ((long long)g.Y * g.Z));
         const int v = pvox(g, x, yy, zz);
@@ -474,12 +638,15 @@ __global__ void __launch_bounds__(256) k_conv_last(Geo g, const __nv_bfloat16* _
 #pragma unroll 1
         for (int tap = 0; tap < 27; tap++) {
             const int off = tap_off(g, tap);
+            const float4* wt = reinterpret_cast<const float4*>(ws + tap * 16);
 #pragma unroll
             for (int q = 0; q < 2; q++) {
                 float h[8];
                 unpack8(*reinterpret_cast<const uint4*>(f + act_off(g, q, v + off)), h);
+                const float4 wa = wt[2 * q], wb = wt[2 * q + 1];
+                const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc = fmaf(__ldg(w + (8 * q + j) * 27 + tap), h[j], acc);
+                for (int j = 0; j < 8; j++) acc = fmaf(wv[j], h[j], acc);
             }
         }
         z[t] = (acc + bias[0]) * inv;
@@ -830,12 +997,40 @@ inline int rc_last() {
     return e == cudaSuccess ? EDGE_OK : (int)e;
 }
 
+// Kernel choice per layer.  By default every layer takes the bulk-copy kernel
+// with one stage: the smaller shared-memory footprint lets two to four times
+// more blocks share an SM, which measured faster on every layer than two
+// stages (U-Net forward at 256x128x128: 3.03 ms against 3.52 ms).  For
+// comparison EDGE_CONV_STAGED=1 forces the thread-staged k_conv_tc and =3 two
+// stages wherever they fit; all choices give bit-identical outputs.
+static int g_conv_mode() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("EDGE_CONV_STAGED");
+        v = e ? e[0] - '0' : 0;
+    }
+    return v;
+}
+
 template <int COUT>
 int launch_conv(const Geo& g, ConvIn a, ConvIn b, int nin, const float* bias, int flags, __nv_bfloat16* y, int* err,
                 cudaStream_t st) {
     const int nchmax = std::max(a.cin, nin > 1 ? b.cin : 0) / 8;
     const size_t smem = (size_t)3 * nchmax * kSegBytes + (size_t)9 * nchmax * COUT * 16;
     if (smem > 200 * 1024) return EDGE_EINVAL;
+    const int mode = g_conv_mode();
+    if (mode != 1) {
+        const uint32_t stage = (uint32_t)((smem + 127) / 128 * 128);
+        const bool two = mode == 3 && 2 * (size_t)stage <= 200 * 1024;
+        const int nstage = two ? 2 : 1;
+        const size_t total = (size_t)nstage * stage;
+        cudaError_t e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
+        if (e != cudaSuccess) return (int)e;
+        int per_sm = (int)std::max<size_t>(1, std::min<size_t>(200 * 1024 / total, 512 / (COUT < 32 ? 32 : COUT)));
+        int grid = std::min(g.ntiles, g_sms() * per_sm);
+        k_conv_bulk<COUT><<<grid, 128, total, st>>>(g, a, b, nin, bias, flags, y, err, nstage, stage);
+        return rc_last();
+    }
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
     int per_sm = (int)std::max<size_t>(1, std::min<size_t>(200 * 1024 / smem, 512 / (COUT < 32 ? 32 : COUT)));
