@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <vector>
 
@@ -1999,11 +2000,41 @@ int prepare_coarse_kernels(const Ctx& c) {
     return EDGE_OK;
 }
 
-// launch with the programmatic-dependent-launch attribute (see pdl_enter)
+// Blocks of kernel k (block threads, smem bytes of dynamic shared memory)
+// resident on the whole current device at once; cached per (device, kernel,
+// shape).  The solver's kernels loop over their slots, so a grid of at most
+// this many blocks runs in one wave with no block waiting for a free SM (the
+// CG kernels, 3-4 blocks per SM by their registers, measured 10-20% faster
+// than with 8 blocks per SM in 2-3 waves).
+static int wave_blocks(const void* k, int block, size_t smem) {
+    static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return kMaxBlocks;
+    }
+    const auto key = std::make_tuple(dev, k, block, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return kMaxBlocks;
+    }
+    const int n = std::max(1, per_sm * sms);
+    cache[key] = n;
+    return n;
+}
+
+// launch with the programmatic-dependent-launch attribute (see pdl_enter),
+// at most one wave of blocks
 template <class... KArgs, class... Args>
 static void launch_pdl(void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
+    cfg.gridDim = dim3(std::min(grid, wave_blocks(reinterpret_cast<const void*>(k), block, smem)));
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
