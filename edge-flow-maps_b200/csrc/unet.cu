@@ -997,6 +997,20 @@ inline int rc_last() {
     return e == cudaSuccess ? EDGE_OK : (int)e;
 }
 
+// Blocks of a 128-thread convolution kernel with `smem` bytes of dynamic
+// shared memory resident on one SM at once, with the kernel's carveout set to
+// the maximum (228 KB per SM, of which each block also takes 1 KB reserved
+// and a little static memory), at most the blocks whose tensor-memory
+// columns fit in the SM's 512.  The kernels loop over tiles, so a grid of
+// exactly this many blocks per SM runs in one wave (one block more per SM
+// than fits would run as a nearly empty second wave).
+static int resident_blocks(size_t smem, int cout) {
+    const size_t per_block = smem + 1024 + 128;
+    const int by_smem = (int)((size_t)228 * 1024 / per_block);
+    const int by_tmem = 512 / (cout < 32 ? 32 : cout);
+    return std::max(1, std::min(by_smem, by_tmem));
+}
+
 // Kernel choice per layer.  By default every layer takes the bulk-copy kernel
 // with one stage: the smaller shared-memory footprint lets two to four times
 // more blocks share an SM, which measured faster on every layer than two
@@ -1026,15 +1040,19 @@ int launch_conv(const Geo& g, ConvIn a, ConvIn b, int nin, const float* bias, in
         const size_t total = (size_t)nstage * stage;
         cudaError_t e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
         if (e != cudaSuccess) return (int)e;
-        int per_sm = (int)std::max<size_t>(1, std::min<size_t>(200 * 1024 / total, 512 / (COUT < 32 ? 32 : COUT)));
-        int grid = std::min(g.ntiles, g_sms() * per_sm);
+        e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return (int)e;
+        const int grid = std::min(g.ntiles, g_sms() * resident_blocks(total, COUT));
         k_conv_bulk<COUT><<<grid, 128, total, st>>>(g, a, b, nin, bias, flags, y, err, nstage, stage);
         return rc_last();
     }
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
-    int per_sm = (int)std::max<size_t>(1, std::min<size_t>(200 * 1024 / smem, 512 / (COUT < 32 ? 32 : COUT)));
-    int grid = std::min(g.ntiles, g_sms() * per_sm);
+    e = cudaFuncSetAttribute(k_conv_tc<COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return (int)e;
+    const int grid = std::min(g.ntiles, g_sms() * resident_blocks(smem, COUT));
     k_conv_tc<COUT><<<grid, 128, smem, st>>>(g, a, b, nin, bias, flags, y, err);
     return rc_last();
 }
