@@ -839,6 +839,14 @@ EDGE_D void st4(float* p, const float (&v)[4]) { *reinterpret_cast<float4*>(p) =
 struct Quad {
     int i, j, kk0, t0;
 };
+// p ? b : a for p in {0, 1} on the bits, so that the choice between two
+// array elements at constant indices is not turned back into one load at a
+// run-time index (which puts the array in local memory)
+EDGE_D float bsel(int p, float a, float b) {
+    const unsigned mask = 0u - (unsigned)p;
+    return __uint_as_float((__float_as_uint(a) & ~mask) | (__float_as_uint(b) & mask));
+}
+
 template <class LV>
 EDGE_D Quad quad_of(const LV& L, int t) {
     int row = fdiv(t, L.dQ);
@@ -881,7 +889,8 @@ EDGE_D void quad_nbr_sum(const LV& L, const Quad& q, int p, const unsigned (&cod
     for (int m = 0; m < 4; m++) {
         const unsigned c = code[m];
         const int k = 2 * (q.kk0 + m) + p;
-        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = o[m + 1 + p], vzm = o[m + p];
+        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = bsel(p, o[m + 1], o[m + 2]),
+              vzm = bsel(p, o[m], o[m + 1]);
         if (PRO) {
             if (c & NB_XP) vxp = vxp + pz(q.i + 1, q.j, k);
             if (c & NB_XM) vxm = vxm + pz(q.i - 1, q.j, k);
@@ -948,8 +957,8 @@ EDGE_D void quad_parents(const LV& F, const CV& C, int i, int j, int kk0, int p,
     const float e6[6] = {lo, c[0], c[1], c[2], c[3], hi};                               // K = kk0 - 1 .. kk0 + 4
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-        o.zp[m] = e6[m + 1 + p];
-        o.zm[m] = e6[m + p];
+        o.zp[m] = bsel(p, e6[m + 1], e6[m + 2]);
+        o.zm[m] = bsel(p, e6[m], e6[m + 1]);
     }
 }
 
@@ -971,7 +980,8 @@ EDGE_D void quad_nbr_sum_pro(const LV& L, const Quad& q, int p, const unsigned (
 #pragma unroll
     for (int m = 0; m < 4; m++) {
         const unsigned c = code[m];
-        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = o[m + 1 + p], vzm = o[m + p];
+        float vxp = xp[m], vxm = xm[m], vyp = yp[m], vym = ym[m], vzp = bsel(p, o[m + 1], o[m + 2]),
+              vzm = bsel(p, o[m], o[m + 1]);
         if (c & NB_XP) vxp = vxp + P.xp[m];
         if (c & NB_XM) vxm = vxm + P.xm[m];
         if (c & NB_YP) vyp = vyp + P.yp[m];
@@ -1041,11 +1051,25 @@ EDGE_D void coarse_body(const G& g, const Lvl* lvs, int L, int lc, float* sh, CL
     unsigned short* codes = reinterpret_cast<unsigned short*>(sh);
     const float mean = lc == 0 ? g.st->mean : 0.0f;
     {
+        // kLoadBatch loads in flight per thread before their shared-memory
+        // stores (one at a time, each would wait for the L2 round trip)
+        constexpr int kLoadBatch = 8;
         const CLvl& q = cl[lc];
-        for (int e = threadIdx.x; e < 2 * q.P; e += blockDim.x) {
-            const float* src = e < q.P ? lvs[lc].r[0] : lvs[lc].r[1];
-            const int ee = e < q.P ? e : e - q.P;
-            sh[q.roff + e] = (COH ? Zc<ZT>::ld(src, ee) : rld<ZT>(src, ee, lc == 0)) - mean;
+        for (int e0 = threadIdx.x; e0 < 2 * q.P; e0 += kLoadBatch * blockDim.x) {
+            float v[kLoadBatch];
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; u++) {
+                const int e = e0 + u * blockDim.x;
+                v[u] = 0.0f;
+                if (e < 2 * q.P) {
+                    const float* src = e < q.P ? lvs[lc].r[0] : lvs[lc].r[1];
+                    const int ee = e < q.P ? e : e - q.P;
+                    v[u] = (COH ? Zc<ZT>::ld(src, ee) : rld<ZT>(src, ee, lc == 0)) - mean;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kLoadBatch; u++)
+                if (e0 + u * blockDim.x < 2 * q.P) sh[q.roff + e0 + u * blockDim.x] = v[u];
         }
         if (SOLID)
             for (int l = lc; l < L; l++) {
