@@ -492,9 +492,21 @@ def c2_measure(steps=5, warm=3, per_cell=8):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     it, rtr, st = sim.proj.result()
+    # per-step solve results over a few more (untimed) steps: the solid
+    # projection stops at r.r < 1e-12 or 100 iterations (mgpcg_solid.py:413-416),
+    # which is at the float32 floor of this grid, so an occasional solve
+    # stagnates just above it and runs to the cap, as the reference's would;
+    # which one varies from run to run with the order of the particle
+    # scatter-adds (float atomics)
+    hist = []
+    for _ in range(steps):
+        sim.step()
+        hist.append(sim.proj.result())
     out = {"workload": "solid wedge + laden particles 256x128x128, EDGE, MGPCG_Solid_3", "ms_per_step": ms,
            "steps_per_s": 1e3 / ms, "particles": int(pos.shape[0]), "solid_cells": int((mask > 0).sum()),
-           "last_solve_iters": it, "last_solve_status": st}
+           "last_solve_iters": it, "last_solve_status": st,
+           "solve_iters_next_steps": [h[0] for h in hist], "solve_rtr_next_steps": [h[1] for h in hist],
+           "solve_tolerance": "r.r < 1e-12 absolute, at most 100 iterations (the reference's)"}
     del sim
     torch.cuda.empty_cache()
     return out
