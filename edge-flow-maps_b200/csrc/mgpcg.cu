@@ -1324,6 +1324,9 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
     const float* __restrict__ zo = pick(L.z, oc);
     float* __restrict__ zs = pick(L.z, color);
     double v[1] = {0.0};
+    // two slots' loads in flight per thread (the pointers are restrict-qualified,
+    // so the second iteration's loads may move above the first one's stores)
+#pragma unroll 2
     GRID_STRIDE(t, L.n0 * L.n1 * (L.H >> 2)) {
         const Quad q = quad_of(L, t);
         const int p = (q.i + q.j + color) & 1;
