@@ -89,6 +89,9 @@ struct G {  // what every solver kernel needs
     double* partials;
     cudaGraphConditionalHandle cond;
     int use_cond;  // 0: kernels run outside a graph (eager mode), no loop condition
+    cudaGraphConditionalHandle vcond;  // the CG loop body's "still running" IF node
+    int use_vcond;
+    int nochk;     // 1: launched inside that IF node, the loop is known to be running
     int bt[6];
     int walls;     // bit b set when bt[b] == 2 (device code tests bits: a pointer
                    // into or a run-time index of a kernel-parameter array makes
@@ -134,6 +137,17 @@ EDGE_D void set_cond(const G& g, unsigned v) {
 }
 
 EDGE_D bool running(const G& g) { return *((volatile int*)&g.st->status) == ST_RUNNING; }
+
+// In the graph-captured CG loop the V-cycle sits in an IF node whose
+// condition the iteration's CG kernels set (k_cg_ap4 clears it, k_cg_xr4
+// sets it while the loop runs), so its kernels skip the status load, an L2
+// round trip at the head of every launch; launched outside that node they
+// read the status and return once the loop has finished.
+EDGE_D bool stopped(const G& g) { return !g.nochk && !running(g); }
+
+EDGE_D void set_vcond(const G& g, unsigned v) {
+    if (g.use_vcond) cudaGraphSetConditional(g.vcond, v);
+}
 
 // every solver kernel counts itself once (block 0, thread 0), including the
 // ones that return early once the loop has finished
@@ -610,6 +624,7 @@ __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
     // reduction and asks to continue: a lost reduction can never spin.
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         set_cond(g, 0);
+        set_vcond(g, 0);
         if (g.st->it > g.st->max_iters + 8) g.st->status = ST_NOCONV;  // hard cap
     }
     if (!running(g)) return;
@@ -704,6 +719,7 @@ __global__ void __launch_bounds__(256) k_cg_xr(G g, Lvl L, Fine f) {
             st->mean = st->all_neumann ? (float)(s[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
             if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
             else if (rTr < st->tol) st->status = ST_CONVERGED;
+            set_vcond(g, st->status == ST_RUNNING ? 1u : 0u);
         }
     }
 }
@@ -727,7 +743,7 @@ template <int MODE, bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, int color) {
     pdl_enter();
     count_launch(g.st);
-    if (!running(g)) {
+    if (stopped(g)) {
         if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
@@ -785,7 +801,7 @@ template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0, int first) {
     pdl_enter();
     count_launch(g.st);
-    if (!running(g)) return;
+    if (stopped(g)) return;
     const float mean = level0 ? g.st->mean : 0.0f;
     GRID_STRIDE(t, C.n0 * C.n1 * C.n2) {
         const int rowc = fdiv(t, C.d2);
@@ -1301,7 +1317,7 @@ __global__ void __launch_bounds__(1024) k_coarse(G g, Levels a) {
     __shared__ CLvl cl[16];
     __shared__ Lvl sl[16];
     count_launch(g.st);
-    if (!running(g)) {
+    if (stopped(g)) {
         if (ZR && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
@@ -1314,7 +1330,7 @@ template <int MODE, bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, int color) {
     pdl_enter();
     count_launch(g.st);
-    if (!running(g)) {
+    if (stopped(g)) {
         if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
@@ -1383,6 +1399,7 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
     count_launch(g.st);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         set_cond(g, 0);
+        set_vcond(g, 0);
         if (g.st->it > g.st->max_iters + 8) g.st->status = ST_NOCONV;  // hard cap
     }
     if (!running(g)) return;
@@ -1494,6 +1511,7 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
             st->mean = st->all_neumann ? (float)(s[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
             if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
             else if (rTr < st->tol) st->status = ST_CONVERGED;
+            set_vcond(g, st->status == ST_RUNNING ? 1u : 0u);
         }
     }
 }
@@ -1504,7 +1522,7 @@ template <bool SOLID, class ZT>
 __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0, int first) {
     pdl_enter();
     count_launch(g.st);
-    if (!running(g)) return;
+    if (stopped(g)) return;
     const float mean = level0 ? g.st->mean : 0.0f;
     const int nq = F.H >> 2;  // == C.n2 / 4
     GRID_STRIDE(t, C.n0 * C.n1 * nq) {
@@ -1697,7 +1715,7 @@ __global__ void __launch_bounds__(kMidThreads) k_mid(G g, Levels a, int lm, int 
     count_launch(g.st);
     copy_levels(a, sl);
     __syncthreads();
-    if (!running(g)) return;  // the same in every block: the status only changes between launches
+    if (stopped(g)) return;  // the same in every block: the status only changes between launches
     const int rank = (int)cluster_rank();
     const int t0 = rank * blockDim.x + threadIdx.x, stride = (int)cluster_size() * blockDim.x;
     for (int l = lm; l < lcc; l++) {
@@ -2169,7 +2187,7 @@ void cg_kernels(const Ctx& c, cudaStream_t stream) {
 }
 
 // The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
-void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
+void enqueue_cg(const Ctx& c, bool solid, cudaStream_t stream) {
     if (c.zbf16) {
         if (solid) cg_kernels<true, __nv_bfloat16>(c, stream);
         else cg_kernels<false, __nv_bfloat16>(c, stream);
@@ -2177,6 +2195,10 @@ void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
         if (solid) cg_kernels<true, float>(c, stream);
         else cg_kernels<false, float>(c, stream);
     }
+}
+
+void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
+    enqueue_cg(c, solid, stream);
     enqueue_vcycle(c, solid, stream, true);
 }
 
@@ -2262,10 +2284,39 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     cudaGraphNode_t cnode;
     CK(cudaGraphAddNode(&cnode, graph, &leaf, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
+    //    the CG kernels, then if (still running) { V-cycle }: the V-cycle's
+    //    kernels are captured with nochk (see stopped())
+    cudaGraphConditionalHandle vh;
+    CK(cudaGraphConditionalHandleCreate(&vh, body, 0, 0));
+    s->ctx.g.vcond = vh;
+    s->ctx.g.use_vcond = 1;
     CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_iteration(s->ctx, s->solid, cs);
+    enqueue_cg(s->ctx, s->solid, cs);
     cudaGraph_t b2;
     CK(cudaStreamEndCapture(cs, &b2));
+    CK(cudaGraphGetNodes(body, nullptr, &nn));
+    nodes.resize(nn);
+    CK(cudaGraphGetNodes(body, nodes.data(), &nn));
+    cudaGraphNode_t bleaf = nullptr;
+    for (auto nd : nodes) {
+        size_t nout = 0;
+        CK(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+        if (nout == 0) bleaf = nd;
+    }
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = vh;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    CK(cudaGraphAddNode(&inode, body, &bleaf, 1, &ip));
+    Ctx vc = s->ctx;
+    vc.g.nochk = 1;
+    CK(cudaStreamBeginCaptureToGraph(cs, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    enqueue_vcycle(vc, s->solid, cs, true);
+    CK(cudaStreamEndCapture(cs, &b2));
+    s->ctx.g.use_vcond = 0;  // launches outside this graph set no IF condition
     // 3) finish
     CK(cudaStreamBeginCaptureToGraph(cs, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     enqueue_finish(s, U, rhs, xout, cs);
@@ -2282,6 +2333,7 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
 int run_solve_eager(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol, double rel_tol, int max_iters,
                     cudaStream_t cs) {
     s->ctx.g.use_cond = 0;
+    s->ctx.g.use_vcond = 0;
     enqueue_setup(s, U, rhs, abs_tol, rel_tol, max_iters, cs);
     for (int it = 0; it <= max_iters + 8; it++) {
         CK(cudaMemcpyAsync(&s->st_host->status, &s->ctx.g.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
