@@ -194,7 +194,25 @@ __global__ void __launch_bounds__(128) k_march_edge(Mac mac, MapF m, float dt, f
 
 // EDGE march on the packed layout (same algorithm as k_march_edge); output
 // planes 0-6 of `out` (n cells per plane).
-template <bool IDENT>
+// T = T_old @ T_step (interp_psi_hermite_garm_fd_unroll_func,
+// hermite.py:960-980) with T_step[a][d] = C[d][a]: float32 products and sums
+// as the reference forms them, or (F64) each entry accumulated in float64 and
+// rounded once
+template <bool F64>
+EDGE_D void compose_jac(const float (&G)[3][3], const float (&C)[3][3], float (&T)[3][3]) {
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (F64)
+                T[r][d] = (float)fma((double)G[r][2], (double)C[d][2],
+                                     fma((double)G[r][1], (double)C[d][1], (double)G[r][0] * (double)C[d][0]));
+            else
+                T[r][d] = G[r][0] * C[d][0] + G[r][1] * C[d][1] + G[r][2] * C[d][2];
+        }
+}
+
+template <bool IDENT, bool F64 = false>
 __global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
@@ -223,8 +241,7 @@ __global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float 
         } else {
             float val[3], G[3][3];
             hermite3p<HV_GARM_P, true>(m, P, val, G);
-            for (int r = 0; r < 3; r++)
-                for (int d = 0; d < 3; d++) T[r][d] = G[r][0] * C[d][0] + G[r][1] * C[d][1] + G[r][2] * C[d][2];
+            compose_jac<F64>(G, C, T);
             for (int c = 0; c < 3; c++) P[c] = val[c];
         }
         if (q == 0) {
@@ -325,8 +342,8 @@ __global__ void __launch_bounds__(128) k_march_ed8_p(Mac mac, MapP m, float dt, 
 EDGE_D void herm_full(const MapF& m, const float p[3], float v[3], float g[3][3]) { hermite3<HV_FULL, true>(m, p, v, g); }
 EDGE_D void herm_full(const MapP& m, const float p[3], float v[3], float g[3][3]) { hermite3p<HV_FULL, true>(m, p, v, g); }
 
-template <class M>
-EDGE_D void ge_center(const Mac& mac, const M& m, int e, float dt, float P[3], float T[3][3]) {
+template <class M, bool F64 = false>
+EDGE_D void ge_center(const Mac& mac, const M& m, int e, float dt, float P[3], float (&T)[3][3]) {
     int k = e % m.nz, j = (e / m.nz) % m.ny, i = e / (m.ny * m.nz);
     cell_pos(i, j, k, m.dx, P);
     float C[3][3];
@@ -335,9 +352,7 @@ EDGE_D void ge_center(const Mac& mac, const M& m, int e, float dt, float P[3], f
     rk4_jac<3>(mac, P, C, -dt);
     float val[3], G[3][3];
     herm_full(m, P, val, G);
-    // T = T_old @ T_step with T_step[a][d] = C[d][a]
-    for (int r = 0; r < 3; r++)
-        for (int d = 0; d < 3; d++) T[r][d] = G[r][0] * C[d][0] + G[r][1] * C[d][1] + G[r][2] * C[d][2];
+    compose_jac<F64>(G, C, T);  // T = T_old @ T_step
     for (int c = 0; c < 3; c++) P[c] = val[c];
 }
 
@@ -356,12 +371,13 @@ __global__ void __launch_bounds__(128) k_march_ge(Mac mac, MapF m, float dt, flo
 }
 
 // packed layout: planes 0-3 of `out`
+template <bool F64 = false>
 __global__ void __launch_bounds__(128) k_march_ge_p(Mac mac, MapP m, float dt, float4* __restrict__ out) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
     if (e >= n) return;
     float P[3], T[3][3];
-    ge_center(mac, m, e, dt, P, T);
+    ge_center<MapP, F64>(mac, m, e, dt, P, T);
     out[e] = make_float4(P[0], P[1], P[2], 0.f);
 #pragma unroll
     for (int d = 0; d < 3; d++) out[(size_t)(1 + d) * n + e] = make_float4(T[0][d], T[1][d], T[2][d], 0.f);
@@ -987,6 +1003,48 @@ __global__ void k_split_central(int nx, int ny, int nz, const float* __restrict_
     o[f.e] = 0.5f * (r + l);
 }
 
+// get_central_vector (taichi_utils.py:95-100): the face average per cell
+__global__ void k_get_central(int nx, int ny, int nz, const float* __restrict__ ux, const float* __restrict__ uy,
+                              const float* __restrict__ uz, float* __restrict__ vc) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)nx * ny * nz) return;
+    int k = (int)(e % nz), j = (int)((e / nz) % ny), i = (int)(e / ((long long)ny * nz));
+    float x = 0.5f * (ux[idx3(i + 1, j, k, ny, nz)] + ux[idx3(i, j, k, ny, nz)]);
+    float y = 0.5f * (uy[idx3(i, j + 1, k, ny + 1, nz)] + uy[idx3(i, j, k, ny + 1, nz)]);
+    float z = 0.5f * (uz[idx3(i, j, k + 1, ny, nz + 1)] + uz[idx3(i, j, k, ny, nz + 1)]);
+    vc[3 * e] = x;
+    vc[3 * e + 1] = y;
+    vc[3 * e + 2] = z;
+}
+
+// curl (taichi_utils.py:69-92): central differences of a cell vec3 field with
+// the neighbour index clamped to the grid (sample, taichi_utils.py:61-66);
+// products by 1/(2dx) rounded before the difference, as the reference's
+// separate statements round them
+__global__ void k_curl(int nx, int ny, int nz, float dx, const float* __restrict__ vf, float* __restrict__ cf) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)nx * ny * nz) return;
+    int k = (int)(e % nz), j = (int)((e / nz) % ny), i = (int)(e / ((long long)ny * nz));
+    const float inv = 1.0f / (2.0f * dx);
+    auto at = [&](int a, int b, int c) {
+        a = max(0, min(a, nx - 1));
+        b = max(0, min(b, ny - 1));
+        c = max(0, min(c, nz - 1));
+        return vf + 3 * (long long)idx3(a, b, c, ny, nz);
+    };
+    const float *vr = at(i + 1, j, k), *vl = at(i - 1, j, k), *vt = at(i, j + 1, k), *vb = at(i, j - 1, k),
+                *vc = at(i, j, k + 1), *va = at(i, j, k - 1);
+    float dvx_dz = __fmul_rn(inv, __fsub_rn(vc[0], va[0]));
+    float dvx_dy = __fmul_rn(inv, __fsub_rn(vt[0], vb[0]));
+    float dvy_dx = __fmul_rn(inv, __fsub_rn(vr[1], vl[1]));
+    float dvy_dz = __fmul_rn(inv, __fsub_rn(vc[1], va[1]));
+    float dvz_dx = __fmul_rn(inv, __fsub_rn(vr[2], vl[2]));
+    float dvz_dy = __fmul_rn(inv, __fsub_rn(vt[2], vb[2]));
+    cf[3 * e] = __fsub_rn(dvz_dy, dvy_dz);
+    cf[3 * e + 1] = __fsub_rn(dvx_dz, dvz_dx);
+    cf[3 * e + 2] = __fsub_rn(dvy_dx, dvx_dy);
+}
+
 // emit_smoke_delta (init_conditions.py:177-232): cells whose centre lies
 // within `radius` of an emitter take its colour; later emitters win, as the
 // reference's sequence of ifs does.
@@ -1035,6 +1093,7 @@ const char* edge_error_string(int code) {
         case EDGE_ENAN: return "non-finite residual";
         case EDGE_ESTALL: return "residual stalled";
         case EDGE_ESTATE: return "invalid call order or handle state";
+        case EDGE_ETIMEOUT: return "a bounded wait inside a solver launch ran out of time";
         default: return code > 0 ? cudaGetErrorString((cudaError_t)code) : "unknown error";
     }
 }
@@ -1188,7 +1247,7 @@ int edge_march_ge_packed(int nx, int ny, int nz, float dx, float dt, const float
     MapP m = make_mapp(in_packed, nx, ny, nz, dx);
     int n = nx * ny * nz;
     float4* o = (float4*)out_packed;
-    k_march_ge_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, o);
+    k_march_ge_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, o);
     k_fd3_dT_p<<<grid_for(n), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, o);
     k_fd3_d2T_p<<<grid_for(n), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, o);
     return launch_status();
@@ -1238,9 +1297,11 @@ int edge_map_unpack(int variant, int nx, int ny, int nz, const float* packed, fl
 }
 
 int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, float epsilon, const float* ux,
-                      const float* uy, const float* uz, const float* in_packed, float* out_packed, int identity,
+                      const float* uy, const float* uz, const float* in_packed, float* out_packed, int flags,
                       void* stream) {
     int pl = planes_of(variant);
+    if (flags & ~(EDGE_MARCH_IDENTITY | EDGE_MARCH_F64_COMPOSE)) return EDGE_EINVAL;
+    const int identity = flags & EDGE_MARCH_IDENTITY, f64 = (flags & EDGE_MARCH_F64_COMPOSE) != 0;
     if (!dims_ok(nx, ny, nz) || pl < 0 || !ux || !uy || !uz || !out_packed) return EDGE_EINVAL;
     if (!identity && !in_packed) return EDGE_EINVAL;
     if (identity && variant != HV_GARM) return EDGE_EINVAL;
@@ -1252,6 +1313,7 @@ int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, f
     float4* o = (float4*)out_packed;
     if (variant == HV_GARM) {
         if (identity) k_march_edge_p<true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        else if (f64) k_march_edge_p<false, true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
         else k_march_edge_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
     } else if (variant == HV_FD) {
         k_march_ed4_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
@@ -1492,6 +1554,19 @@ int edge_split_central_vector(int nx, int ny, int nz, const float* vc, float* ux
                               void* stream) {
     if (!dims_ok(nx, ny, nz) || !vc || !ux || !uy || !uz) return EDGE_EINVAL;
     k_split_central<<<grid_for(n_faces(nx, ny, nz)), kBlock, 0, S(stream)>>>(nx, ny, nz, vc, ux, uy, uz);
+    return launch_status();
+}
+
+int edge_get_central_vector(int nx, int ny, int nz, const float* ux, const float* uy, const float* uz, float* vc,
+                            void* stream) {
+    if (!dims_ok(nx, ny, nz) || !vc || !ux || !uy || !uz) return EDGE_EINVAL;
+    k_get_central<<<grid_for((long long)nx * ny * nz), kBlock, 0, S(stream)>>>(nx, ny, nz, ux, uy, uz, vc);
+    return launch_status();
+}
+
+int edge_curl(int nx, int ny, int nz, float dx, const float* vf, float* cf, void* stream) {
+    if (!dims_ok(nx, ny, nz) || !vf || !cf || vf == cf) return EDGE_EINVAL;
+    k_curl<<<grid_for((long long)nx * ny * nz), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, vf, cf);
     return launch_status();
 }
 

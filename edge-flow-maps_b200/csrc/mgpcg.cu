@@ -20,10 +20,12 @@
 // `mean` that every reader of r[0] subtracts and that the r update folds into
 // the stored residual.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -38,14 +40,20 @@ using namespace edge;
 
 namespace {
 
-enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_NOCONV = 2, ST_NAN = 3 };
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_NOCONV = 2, ST_NAN = 3, ST_TIMEOUT = 4 };
 
 struct SolveState {
     double zTr, pAp, rTr, rsum, tol, abs_tol, rel_tol, div_sum;
-    float alpha, beta, mean, pad0;
+    float alpha, beta, mean, zsc;
+    float zinv;   // 1 / zsc
+    int zscaled;  // FP16 level storage: zsc follows the residual's RMS (set_zscale)
+    int pad1, pad2;
     int it, max_iters, status, setup;
     int pcur, all_neumann, n_fluid, x_valid;
     unsigned int counter[8];
+    // grid barrier of the cooperative iteration kernel: arrivals, generation,
+    // and the flag a block sets when a wait ran out of time
+    unsigned int bar_count, bar_gen, bar_abort, bar_pad;
     unsigned long long kernels;  // kernels of this solver run so far (launch accounting)
 };
 
@@ -125,11 +133,10 @@ struct Ctx {
     G g;
     Fine f;
     int csmem;  // dynamic shared memory of k_coarse (bytes)
-    int zbf16;  // 1: the V-cycle's level arrays are BF16 (mixed-precision solver)
-    // k_mid: levels lm..lcc-1 on a cluster of cmid thread blocks, lcc..L-1 in
-    // block 0's shared memory (csmem_mid bytes); cmid == 0: per-level kernels
-    // down to lc and k_coarse
-    int lm = 0, lcc = 0, cmid = 0, csmem_mid = 0;
+    int ztype;  // storage of the V-cycle's level arrays: 0 FP32, 1 BF16, 2 FP16 (mixed-precision solvers)
+    // 1: the CG loop runs k_coarse + k_coop(ITER) per iteration on a grid of
+    // coop_grid co-resident blocks (plan_coop); 0: the per-level kernels
+    int coop = 0, coop_grid = 0;
 };
 
 EDGE_D void set_cond(const G& g, unsigned v) {
@@ -277,6 +284,33 @@ struct Zs<__nv_bfloat16> {
         return make_float2(__low2float(v), __high2float(v));
     }
 };
+template <>
+struct Zs<__half> {
+    static EDGE_D const __half* h(const float* b) { return reinterpret_cast<const __half*>(b); }
+    static EDGE_D __half* h(float* b) { return reinterpret_cast<__half*>(b); }
+    static EDGE_D float ld(const float* b, int e) { return __half2float(h(b)[e]); }
+    static EDGE_D void st(float* b, int e, float v) { h(b)[e] = __float2half_rn(v); }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        const uint2 u = *reinterpret_cast<const uint2*>(h(b) + e);
+        const __half2 a = *reinterpret_cast<const __half2*>(&u.x);
+        const __half2 c = *reinterpret_cast<const __half2*>(&u.y);
+        v[0] = __low2float(a); v[1] = __high2float(a); v[2] = __low2float(c); v[3] = __high2float(c);
+    }
+    static EDGE_D void st4(float* b, int e, const float (&v)[4]) {
+        __half2 a = __floats2half2_rn(v[0], v[1]), c = __floats2half2_rn(v[2], v[3]);
+        uint2 u;
+        u.x = *reinterpret_cast<unsigned*>(&a);
+        u.y = *reinterpret_cast<unsigned*>(&c);
+        *reinterpret_cast<uint2*>(h(b) + e) = u;
+    }
+    static EDGE_D void st2(float* b, int e, float x, float y) {
+        *reinterpret_cast<__half2*>(h(b) + e) = __floats2half2_rn(x, y);
+    }
+    static EDGE_D float2 ld2(const float* b, int e) {
+        const __half2 v = *reinterpret_cast<const __half2*>(h(b) + e);
+        return make_float2(__low2float(v), __high2float(v));
+    }
+};
 // r of a level: FP32 at level 0, else the level storage type
 template <class ZT>
 EDGE_D float rld(const float* b, int e, int level0) { return level0 ? __ldg(b + e) : Zs<ZT>::ld(b, e); }
@@ -309,6 +343,24 @@ struct Zc<__nv_bfloat16> {
         const uint2 u = __ldcg(reinterpret_cast<const uint2*>(reinterpret_cast<const __nv_bfloat16*>(b) + e));
         const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&u.x);
         const __nv_bfloat162 c = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
+        v[0] = __low2float(a); v[1] = __high2float(a); v[2] = __low2float(c); v[3] = __high2float(c);
+    }
+};
+template <>
+struct Zc<__half> {
+    static EDGE_D float ld(const float* b, int e) {
+        unsigned short u = __ldcg(reinterpret_cast<const unsigned short*>(b) + e);
+        return __half2float(__ushort_as_half(u));
+    }
+    static EDGE_D float2 ld2(const float* b, int e) {
+        unsigned u = __ldcg(reinterpret_cast<const unsigned*>(reinterpret_cast<const unsigned short*>(b) + e));
+        const __half2 v = *reinterpret_cast<const __half2*>(&u);
+        return make_float2(__low2float(v), __high2float(v));
+    }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        const uint2 u = __ldcg(reinterpret_cast<const uint2*>(reinterpret_cast<const __half*>(b) + e));
+        const __half2 a = *reinterpret_cast<const __half2*>(&u.x);
+        const __half2 c = *reinterpret_cast<const __half2*>(&u.y);
         v[0] = __low2float(a); v[1] = __high2float(a); v[2] = __low2float(c); v[3] = __high2float(c);
     }
 };
@@ -395,7 +447,8 @@ EDGE_D void final_sum(const G& g, int slot, double (&out)[N]) {
 // the loop condition (mgpcg.py:221-226, 263-277); thread 0 only
 EDGE_D void zr_epilogue(const G& g, double zr) {
     SolveState* st = g.st;
-    double zTr = (double)(float)zr;
+    const double zi = (double)st->zinv;  // z and r of the V-cycle carry the scale zsc each
+    double zTr = (double)(float)(zr * zi * zi);
     if (st->setup) {
         st->setup = 0;
         st->zTr = zTr;
@@ -409,6 +462,20 @@ EDGE_D void zr_epilogue(const G& g, double zr) {
         if (st->it >= st->max_iters) st->status = ST_NOCONV;
     }
     set_cond(g, st->status == ST_RUNNING ? 1u : 0u);
+}
+
+// FP16 level storage: the V-cycle runs on the level-0 residual times a power
+// of two zsc that brings its RMS near 1 (FP16 keeps 10 bits of mantissa but
+// only 5 of exponent); every product and quotient by zsc or zinv is exact, so
+// the FP32 and BF16 solvers, whose zsc stays 1, are unaffected.  rr = sum of
+// r^2 over n cells.
+EDGE_D void set_zscale(SolveState* st, double rr, double n) {
+    if (!st->zscaled) return;
+    const double rms = sqrt(rr / n);
+    int e = 0;
+    if (rms > 0.0 && rms < 1e300) e = max(-120, min(120, -(int)lround(log2(rms))));
+    st->zsc = ldexpf(1.0f, e);
+    st->zinv = ldexpf(1.0f, -e);
 }
 
 #define GRID_STRIDE(t, n) for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (n); t += gridDim.x * blockDim.x)
@@ -466,7 +533,7 @@ __global__ void __launch_bounds__(256) k_setup_rhs(G g, Lvl L, Fine f, Faces U, 
                                                    double rel_tol, int max_iters) {
     count_launch(g.st);
     const int ny = L.n1, nz = L.n2;
-    double v[3] = {0.0, 0.0, 0.0};  // sum div (fluid), fluid count, sum r
+    double v[4] = {0.0, 0.0, 0.0, 0.0};  // sum div (fluid), fluid count, sum r, sum r^2
     GRID_STRIDE(t, L.P) {
         Slot s = slot_of(L, t);
         const int c0 = (s.i + s.j) & 1;
@@ -496,11 +563,12 @@ __global__ void __launch_bounds__(256) k_setup_rhs(G g, Lvl L, Fine f, Faces U, 
                 v[1] += 1.0;
             }
             v[2] += r;
+            v[3] += (double)r * (double)r;
         }
     }
-    if (last_block<3>(g, 0, v)) {
-        double s[3];
-        final_sum<3>(g, 0, s);
+    if (last_block<4>(g, 0, v)) {
+        double s[4];
+        final_sum<4>(g, 0, s);
         if (threadIdx.x == 0) {
             SolveState* st = g.st;
             st->div_sum = (double)(float)s[0];
@@ -517,6 +585,7 @@ __global__ void __launch_bounds__(256) k_setup_rhs(G g, Lvl L, Fine f, Faces U, 
             st->pcur = 0;
             st->x_valid = 0;
             st->mean = st->all_neumann ? (float)(s[2] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
+            set_zscale(st, s[3], (double)L.n0 * L.n1 * L.n2);
         }
     }
 }
@@ -631,7 +700,7 @@ __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
     SolveState* st = g.st;
     const int pc = st->pcur;
     const bool first = st->it == 0;  // p = 0 before the first update_p (mgpcg.py:61-66)
-    const float beta = st->beta;
+    const float beta = st->beta, zinv = st->zinv;
     double v[1] = {0.0};
     GRID_STRIDE(t, L.P) {
         Slot s = slot_of(L, t);
@@ -645,10 +714,10 @@ __global__ void __launch_bounds__(256) k_cg_ap(G g, Lvl L, Fine f) {
             if (code & CELL_FLUID) {
                 const float* __restrict__ zo = pick(L.z, pl ^ 1);
                 const float* __restrict__ po = pick2(f.p, pc, pl ^ 1);
-                const float zt = Zs<ZT>::ld(pick(L.z, pl), t);
+                const float zt = Zs<ZT>::ld(pick(L.z, pl), t) * zinv;
                 pe = first ? zt : __fadd_rn(zt, __fmul_rn(beta, __ldg(pick2(f.p, pc, pl) + t)));
                 float ns = nbr_sum(L, code, t, k, [&](int e, int) {
-                    const float ze = Zs<ZT>::ld(zo, e);
+                    const float ze = Zs<ZT>::ld(zo, e) * zinv;
                     return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e)));
                 });
                 float ape = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.walls, L, code, s.i, s.j, k), pe), ns);
@@ -717,6 +786,7 @@ __global__ void __launch_bounds__(256) k_cg_xr(G g, Lvl L, Fine f) {
             st->rsum = s[1];
             st->x_valid = 1;
             st->mean = st->all_neumann ? (float)(s[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
+            set_zscale(st, rTr, (double)L.n0 * L.n1 * L.n2);
             if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
             else if (rTr < st->tol) st->status = ST_CONVERGED;
             set_vcond(g, st->status == ST_RUNNING ? 1u : 0u);
@@ -747,7 +817,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
         if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
-    const float mean = level0 ? g.st->mean : 0.0f;
+    const float mean = level0 ? g.st->mean : 0.0f, zsc = level0 ? g.st->zsc : 1.0f;
     const int oc = color ^ 1;
     const float* __restrict__ rs = pick(L.r, color);
     const float* __restrict__ zo = pick(L.z, oc);
@@ -759,7 +829,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
         if (k < L.n2) {
             const unsigned code = code_at<SOLID>(L, color, t, s.i, s.j, k);
             if (code & CELL_FLUID) {
-                const float rv = rld<ZT>(rs, t, level0) - mean;
+                const float rv = (rld<ZT>(rs, t, level0) - mean) * zsc;
                 float ns = 0.0f;
                 if (MODE == HS_PROLONG) {
                     ns = nbr_sum(L, code, t, k, [&](int e, int d) {
@@ -779,7 +849,7 @@ __global__ void __launch_bounds__(256) k_hsweep(G g, Lvl L, Lvl C, int level0, i
             // the other cell of the slot (final from the previous half sweep)
             const int ko = 2 * s.kk + ((s.i + s.j + oc) & 1);
             if (ko < L.n2 && (code_at<SOLID>(L, oc, t, s.i, s.j, ko) & CELL_FLUID))
-                v[0] += (double)Zs<ZT>::ld(zo, t) * (double)(rld<ZT>(pick(L.r, oc), t, level0) - mean);
+                v[0] += (double)Zs<ZT>::ld(zo, t) * (double)((rld<ZT>(pick(L.r, oc), t, level0) - mean) * zsc);
         }
     }
     if (MODE == HS_ZR) {
@@ -802,7 +872,7 @@ __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0,
     pdl_enter();
     count_launch(g.st);
     if (stopped(g)) return;
-    const float mean = level0 ? g.st->mean : 0.0f;
+    const float mean = level0 ? g.st->mean : 0.0f, zsc = level0 ? g.st->zsc : 1.0f;
     GRID_STRIDE(t, C.n0 * C.n1 * C.n2) {
         const int rowc = fdiv(t, C.d2);
         const int K = t - rowc * C.n2;
@@ -823,7 +893,7 @@ __global__ void __launch_bounds__(256) k_restrict(G g, Lvl F, Lvl C, int level0,
                     const float* __restrict__ zo = pick(F.z, pl ^ 1);
                     float ns = nbr_sum(F, code, e, k, [&](int ee, int) { return Zs<ZT>::ld(zo, ee); });
                     float az = __fsub_rn(__fmul_rn(nf_of<SOLID>(g.walls, F, code, i, j, k), Zs<ZT>::ld(pick(F.z, pl), e)), ns);
-                    float res = (rld<ZT>(pick(F.r, pl), e, level0) - mean) - az;
+                    float res = (rld<ZT>(pick(F.r, pl), e, level0) - mean) * zsc - az;
                     acc += res * 0.5f;
                 }
         const int pc = (I + J + K) & 1;
@@ -1065,7 +1135,7 @@ EDGE_D void coarse_body(const G& g, const Lvl* lvs, int L, int lc, float* sh, CL
     }
     __syncthreads();
     unsigned short* codes = reinterpret_cast<unsigned short*>(sh);
-    const float mean = lc == 0 ? g.st->mean : 0.0f;
+    const float mean = lc == 0 ? g.st->mean : 0.0f, zsc = lc == 0 ? g.st->zsc : 1.0f;
     {
         // kLoadBatch loads in flight per thread before their shared-memory
         // stores (one at a time, each would wait for the L2 round trip)
@@ -1080,7 +1150,7 @@ EDGE_D void coarse_body(const G& g, const Lvl* lvs, int L, int lc, float* sh, CL
                 if (e < 2 * q.P) {
                     const float* src = e < q.P ? lvs[lc].r[0] : lvs[lc].r[1];
                     const int ee = e < q.P ? e : e - q.P;
-                    v[u] = (COH ? Zc<ZT>::ld(src, ee) : rld<ZT>(src, ee, lc == 0)) - mean;
+                    v[u] = ((COH ? Zc<ZT>::ld(src, ee) : rld<ZT>(src, ee, lc == 0)) - mean) * zsc;
                 }
             }
 #pragma unroll
@@ -1334,7 +1404,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
         if (MODE == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
         return;
     }
-    const float mean = level0 ? g.st->mean : 0.0f;
+    const float mean = level0 ? g.st->mean : 0.0f, zsc = level0 ? g.st->zsc : 1.0f;
     const int oc = color ^ 1;
     const float* __restrict__ rs = pick(L.r, color);
     const float* __restrict__ zo = pick(L.z, oc);
@@ -1366,7 +1436,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
         }
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            rv[m] = rv[m] - mean;
+            rv[m] = (rv[m] - mean) * zsc;
             zn[m] = (code[m] & CELL_FLUID) ? (rv[m] + ns[m]) / nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
                                            : 0.0f;
             if (MODE == HS_ZR && (code[m] & CELL_FLUID)) v[0] += (double)zn[m] * (double)rv[m];
@@ -1381,7 +1451,7 @@ __global__ void __launch_bounds__(256) k_hsweep4(G g, Lvl L, Lvl C, int level0, 
             Zs<ZT>::ld4(zo, q.t0, zz);
 #pragma unroll
             for (int m = 0; m < 4; m++)
-                if (co[m] & CELL_FLUID) v[0] += (double)zz[m] * (double)(ro[m] - mean);
+                if (co[m] & CELL_FLUID) v[0] += (double)zz[m] * (double)((ro[m] - mean) * zsc);
         }
     }
     if (MODE == HS_ZR) {
@@ -1406,7 +1476,7 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
     SolveState* st = g.st;
     const int pc = st->pcur;
     const bool first = st->it == 0;
-    const float beta = st->beta;
+    const float beta = st->beta, zinv = st->zinv;
     double v[1] = {0.0};
     GRID_STRIDE(t, L.n0 * L.n1 * (L.H >> 2)) {
         const Quad q = quad_of(L, t);
@@ -1420,6 +1490,8 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
             const float* __restrict__ po = pick2(f.p, pc, pl ^ 1);
             auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
                 Zs<ZT>::ld4(zz, e, o);
+#pragma unroll
+                for (int m = 0; m < 4; m++) o[m] = o[m] * zinv;
                 if (!first) {
                     float b[4];
                     ld4(pp + e, b);
@@ -1431,7 +1503,10 @@ __global__ void __launch_bounds__(256) k_cg_ap4(G g, Lvl L, Fine f) {
             pn4(pick(L.z, pl), pick2(f.p, pc, pl), q.t0, pe);
             quad_nbr_sum<false>(
                 L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
-                [&](int e) { const float ze = Zs<ZT>::ld(zo, e); return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e))); },
+                [&](int e) {
+                    const float ze = Zs<ZT>::ld(zo, e) * zinv;
+                    return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldg(po + e)));
+                },
                 NoParent(), ns);
 #pragma unroll
             for (int m = 0; m < 4; m++) {
@@ -1509,6 +1584,7 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
             st->rsum = s[1];
             st->x_valid = 1;
             st->mean = st->all_neumann ? (float)(s[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
+            set_zscale(st, rTr, (double)L.n0 * L.n1 * L.n2);
             if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
             else if (rTr < st->tol) st->status = ST_CONVERGED;
             set_vcond(g, st->status == ST_RUNNING ? 1u : 0u);
@@ -1523,7 +1599,7 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
     pdl_enter();
     count_launch(g.st);
     if (stopped(g)) return;
-    const float mean = level0 ? g.st->mean : 0.0f;
+    const float mean = level0 ? g.st->mean : 0.0f, zsc = level0 ? g.st->zsc : 1.0f;
     const int nq = F.H >> 2;  // == C.n2 / 4
     GRID_STRIDE(t, C.n0 * C.n1 * nq) {
         const int rowc = fdiv(t, F.dQ);
@@ -1555,7 +1631,7 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
                         if (!(code[m] & CELL_FLUID)) continue;
                         float nf = nf_of<SOLID>(g.walls, F, code[m], i, j, 2 * (K0 + m) + h);
                         float az = __fsub_rn(__fmul_rn(nf, zc[m]), ns[m]);
-                        float res = (rc[m] - mean) - az;
+                        float res = (rc[m] - mean) * zsc - az;
                         acc[m] += res * 0.5f;
                     }
                 }
@@ -1581,29 +1657,7 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
     }
 }
 
-// ---------------------------------------------------------------------------
-// The middle of the V-cycle in one thread-block cluster (k_mid): levels
-// lm..lcc-1 (small enough to live in L2, too small to fill the GPU) run the
-// four-slot half sweeps and restrictions of k_hsweep4 / k_restrict4 spread
-// over the cluster's threads, a cluster barrier between phases instead of a
-// kernel boundary; block 0 then runs the shared-memory coarse group
-// (levels lcc..L-1) and the cluster runs the up sweeps.  Data written in the
-// launch is read through L2 (Zc).  Same arithmetic as the per-level kernels.
-// ---------------------------------------------------------------------------
-EDGE_D void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-EDGE_D unsigned cluster_rank() {
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-EDGE_D unsigned cluster_size() {
-    unsigned r;
-    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-    return r;
-}
-
+// z of the coarse level at the parent of fine cell (i, j, k), read through L2
 template <class ZT>
 EDGE_D float parent_zc(const Lvl& C, int i, int j, int k) {
     int I = i >> 1, J = j >> 1, K = k >> 1;
@@ -1611,9 +1665,138 @@ EDGE_D float parent_zc(const Lvl& C, int i, int j, int k) {
     return Zc<ZT>::ld(pick(C.z, (I + J + K) & 1), e);
 }
 
-// k_hsweep4 (HS_PLAIN / HS_PROLONG) on a level >= 1, threads t0, t0+stride, ...
+// ---------------------------------------------------------------------------
+// Cooperative CG iteration (k_coop): the levels that run per-level kernels
+// (0..lc-1) and the CG vector updates of one iteration in ONE launch over a
+// grid of co-resident blocks (cooperative launch), phases separated by a grid
+// barrier instead of a kernel boundary.  An iteration of the graph's loop is
+// then two launches: k_coarse (the shared-memory coarse group, one block) and
+//   k_coop(ITER): up sweeps lc-1..0 (the fine level's last one forms z.r and
+//                 beta), p = z + beta p with A p and p.Ap, the x and r updates
+//                 with r.r and the convergence test, then - while running -
+//                 the down sweeps and restrictions 0..lc-1 of the next
+//                 V-cycle;
+// the set-up ends with k_coop(DOWN), the down half alone.  Each phase runs
+// the same per-cell arithmetic, in the same order, as the per-level kernels
+// (k_hsweep4, k_restrict4, k_cg_ap4, k_cg_xr4); the reductions' per-block
+// partials are summed in block order by the last block to arrive at the
+// barrier, which publishes the scalars before it releases the others.
+// Data written inside the launch is read through L2 (ld.global.cg).  Every
+// wait is bounded: a block whose wait runs out of time sets an abort flag that
+// every other waiting block sees, the solve ends with ST_TIMEOUT, and all
+// blocks return.
+// ---------------------------------------------------------------------------
+enum { COOP_DOWN = 0, COOP_ITER = 1 };
+constexpr unsigned long long kCoopWaitNs = 2000000000ull;  // 2 s
+
+EDGE_D unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+EDGE_D void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+EDGE_D unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct CoopBar {
+    unsigned gen;  // generation this block expects next (thread 0)
+    int ok;        // 0 once the launch is aborted (shared)
+};
+
+// Thread 0: wait until the barrier's generation reaches `target`; false when
+// the launch was aborted or this wait ran out of time (which aborts it).
+EDGE_D bool coop_wait(SolveState* st, unsigned target) {
+    const unsigned long long t0 = global_ns();
+    unsigned n = 0;
+    while (ld_acquire_u32(&st->bar_gen) != target) {
+        if (*((volatile unsigned*)&st->bar_abort)) return false;
+        if ((++n & 63u) == 0 && global_ns() - t0 > kCoopWaitNs) {
+            atomicExch(&st->bar_abort, 1u);
+            st->status = ST_TIMEOUT;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Grid barrier; returns false in every thread of the block once the launch
+// is aborted.
+EDGE_D bool coop_sync(SolveState* st, CoopBar& b) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned target = b.gen + 1;
+        __threadfence();
+        bool ok = true;
+        if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+            atomicExch(&st->bar_count, 0u);  // no block arrives again before the release below
+            st_release_u32(&st->bar_gen, target);
+        } else {
+            ok = coop_wait(st, target);
+        }
+        b.gen = target;
+        b.ok = ok;
+    }
+    __syncthreads();
+    return b.ok;
+}
+
+// Grid barrier with a reduction: the block's partials v (summed over the
+// block) are published, the last block to arrive sums all blocks' partials
+// in block order and runs epi(sums) in its thread 0 before releasing the
+// others, so every block reads epi's results after the barrier.
+template <int N, class EPI>
+EDGE_D bool coop_reduce(const G& g, CoopBar& b, double (&v)[N], EPI epi) {
+    __shared__ int last;
+    SolveState* st = g.st;
+    block_sum<N>(v);
+    const int nblk = gridDim.x;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < N; q++) g.partials[q * nblk + blockIdx.x] = v[q];
+        __threadfence();
+        last = atomicAdd(&st->bar_count, 1u) == (unsigned)nblk - 1;
+    }
+    __syncthreads();
+    const unsigned target = b.gen + 1;
+    if (last) {
+        __threadfence();
+        double w[N];
+#pragma unroll
+        for (int q = 0; q < N; q++) {
+            double s = 0.0;
+            for (int k = threadIdx.x; k < nblk; k += blockDim.x) s += __ldcg(g.partials + q * nblk + k);
+            w[q] = s;
+        }
+        block_sum<N>(w);
+        if (threadIdx.x == 0) {
+            epi(w);
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            st_release_u32(&st->bar_gen, target);
+            b.ok = 1;
+        }
+    } else if (threadIdx.x == 0) {
+        b.ok = coop_wait(st, target);
+    }
+    if (threadIdx.x == 0) b.gen = target;
+    __syncthreads();
+    return b.ok;
+}
+
+EDGE_D float st_ldf(const float* p) { return *((const volatile float*)p); }
+EDGE_D int st_ldi(const int* p) { return *((const volatile int*)p); }
+
+// one half sweep of colour `color` on a four-slot level (k_hsweep4's
+// arithmetic), slots t0, t0 + stride, ...; HS_ZR adds z.r over both colours
+// to zr
 template <int MODE, bool SOLID, class ZT>
-EDGE_D void cl_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int t0, int stride) {
+EDGE_D void co_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int level0, float mean, float zsc, int t0,
+                     int stride, double& zr) {
     const int oc = color ^ 1;
     const float* rs = pick(L.r, color);
     const float* zo = pick(L.z, oc);
@@ -1625,31 +1808,49 @@ EDGE_D void cl_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int t0, 
         unsigned code[4];
         quad_codes<SOLID>(L, color, q, p, code);
         float rv[4], ns[4] = {0.0f, 0.0f, 0.0f, 0.0f}, zn[4];
-        Zc<ZT>::ld4(rs, q.t0, rv);
-        auto v4 = [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); };
-        auto v1 = [&](int e) { return Zc<ZT>::ld(zo, e); };
-        if (MODE == HS_PROLONG && L.n2 % 8 == 0) {
-            QParents P;
-            quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return Zc<ZT>::ld2(pick(C.z, pl), e); },
-                         [&](int pl, int e) { return Zc<ZT>::ld(pick(C.z, pl), e); }, P);
-            quad_nbr_sum_pro(L, q, p, code, v4, v1, P, ns);
-        } else if (MODE == HS_PROLONG)
-            quad_nbr_sum<true>(L, q, p, code, v4, v1, [&](int i, int j, int k) { return parent_zc<ZT>(C, i, j, k); },
-                               ns);
-        else
-            quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
+        if (level0) Zc<float>::ld4(rs, q.t0, rv);
+        else Zc<ZT>::ld4(rs, q.t0, rv);
+        if (MODE != HS_FIRST) {
+            auto v4 = [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); };
+            auto v1 = [&](int e) { return Zc<ZT>::ld(zo, e); };
+            if (MODE == HS_PROLONG && L.n2 % 8 == 0) {
+                QParents P;
+                quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return Zc<ZT>::ld2(pick(C.z, pl), e); },
+                             [&](int pl, int e) { return Zc<ZT>::ld(pick(C.z, pl), e); }, P);
+                quad_nbr_sum_pro(L, q, p, code, v4, v1, P, ns);
+            } else if (MODE == HS_PROLONG)
+                quad_nbr_sum<true>(L, q, p, code, v4, v1,
+                                   [&](int i, int j, int k) { return parent_zc<ZT>(C, i, j, k); }, ns);
+            else
+                quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
+        }
 #pragma unroll
-        for (int m = 0; m < 4; m++)
+        for (int m = 0; m < 4; m++) {
+            rv[m] = (rv[m] - mean) * zsc;
             zn[m] = (code[m] & CELL_FLUID)
-                        ? ((rv[m] - 0.0f) + ns[m]) / nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
+                        ? (rv[m] + ns[m]) / nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
                         : 0.0f;
+            if (MODE == HS_ZR && (code[m] & CELL_FLUID)) zr += (double)zn[m] * (double)rv[m];
+        }
         Zs<ZT>::st4(zs, q.t0, zn);
+        if (MODE == HS_ZR) {
+            unsigned co[4];
+            quad_codes<SOLID>(L, oc, q, p ^ 1, co);
+            float ro[4], zz[4];
+            if (level0) Zc<float>::ld4(pick(L.r, oc), q.t0, ro);
+            else Zc<ZT>::ld4(pick(L.r, oc), q.t0, ro);
+            Zc<ZT>::ld4(zo, q.t0, zz);
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (co[m] & CELL_FLUID) zr += (double)zz[m] * (double)((ro[m] - mean) * zsc);
+        }
     }
 }
 
-// k_restrict4 on a level >= 1
+// k_restrict4's arithmetic on slots t0, t0 + stride, ...
 template <bool SOLID, class ZT>
-EDGE_D void cl_restrict(const G& g, const Lvl& F, const Lvl& C, bool first, int t0, int stride) {
+EDGE_D void co_restrict(const G& g, const Lvl& F, const Lvl& C, int level0, float mean, float zsc, bool first,
+                        int t0, int stride) {
     const int nq = F.H >> 2;
     for (int t = t0; t < C.n0 * C.n1 * nq; t += stride) {
         const int rowc = fdiv(t, F.dQ);
@@ -1669,19 +1870,20 @@ EDGE_D void cl_restrict(const G& g, const Lvl& F, const Lvl& C, bool first, int 
                     const int pl = c0 ^ h;
                     unsigned code[4];
                     quad_codes<SOLID>(F, pl, q, h, code);
-                    const float* __restrict__ zo = pick(F.z, pl ^ 1);
+                    const float* zo = pick(F.z, pl ^ 1);
                     float ns[4], zc[4], rc[4];
                     quad_nbr_sum<false>(
                         F, q, h, code, [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); },
                         [&](int e) { return Zc<ZT>::ld(zo, e); }, NoParent(), ns);
                     Zc<ZT>::ld4(pick(F.z, pl), q.t0, zc);
-                    Zc<ZT>::ld4(pick(F.r, pl), q.t0, rc);
+                    if (level0) Zc<float>::ld4(pick(F.r, pl), q.t0, rc);
+                    else Zc<ZT>::ld4(pick(F.r, pl), q.t0, rc);
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         if (!(code[m] & CELL_FLUID)) continue;
                         float nf = nf_of<SOLID>(g.walls, F, code[m], i, j, 2 * (K0 + m) + h);
                         float az = __fsub_rn(__fmul_rn(nf, zc[m]), ns[m]);
-                        float res = (rc[m] - 0.0f) - az;
+                        float res = (rc[m] - mean) * zsc - az;
                         acc[m] += res * 0.5f;
                     }
                 }
@@ -1704,42 +1906,210 @@ EDGE_D void cl_restrict(const G& g, const Lvl& F, const Lvl& C, bool first, int 
     }
 }
 
-constexpr int kMidThreads = 512;
+// k_cg_ap4's arithmetic (p = z + beta p, A p, p.Ap) on slots t0, t0 + stride, ...
+template <bool SOLID, class ZT>
+EDGE_D void co_ap(const G& g, const Lvl& L, const Fine& f, int pc, bool first, float beta, float zinv, int t0,
+                  int stride, double& pap) {
+    const int nq = L.n0 * L.n1 * (L.H >> 2);
+    for (int t = t0; t < nq; t += stride) {
+        const Quad q = quad_of(L, t);
+        const int c0 = (q.i + q.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int pl = c0 ^ h;
+            unsigned code[4];
+            quad_codes<SOLID>(L, pl, q, h, code);
+            const float* zo = pick(L.z, pl ^ 1);
+            const float* po = pick2(f.p, pc, pl ^ 1);
+            auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
+                Zc<ZT>::ld4(zz, e, o);
+#pragma unroll
+                for (int m = 0; m < 4; m++) o[m] = o[m] * zinv;
+                if (!first) {
+                    float b[4];
+                    Zc<float>::ld4(pp, e, b);
+#pragma unroll
+                    for (int m = 0; m < 4; m++) o[m] = __fadd_rn(o[m], __fmul_rn(beta, b[m]));
+                }
+            };
+            float pe[4], ns[4];
+            pn4(pick(L.z, pl), pick2(f.p, pc, pl), q.t0, pe);
+            quad_nbr_sum<false>(
+                L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
+                [&](int e) {
+                    const float ze = Zc<ZT>::ld(zo, e) * zinv;
+                    return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldcg(po + e)));
+                },
+                NoParent(), ns);
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                if (code[m] & CELL_FLUID) {
+                    float nf = nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
+                    float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
+                    pap += (double)pe[m] * (double)ape;
+                } else {
+                    pe[m] = 0.0f;
+                }
+            }
+            st4(pick2(f.p, pc ^ 1, pl) + q.t0, pe);
+        }
+    }
+}
+
+// k_cg_xr4's arithmetic (x += alpha p, r -= alpha A p, r.r, sum r)
+template <bool SOLID>
+EDGE_D void co_xr(const G& g, const Lvl& L, const Fine& f, int pc, bool first, float alpha, float mean, int t0,
+                  int stride, double (&v)[2]) {
+    const int nq = L.n0 * L.n1 * (L.H >> 2);
+    for (int t = t0; t < nq; t += stride) {
+        const Quad q = quad_of(L, t);
+        const int c0 = (q.i + q.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int pl = c0 ^ h;
+            unsigned code[4];
+            quad_codes<SOLID>(L, pl, q, h, code);
+            const float* po = pick2(f.p, pc, pl ^ 1);
+            float pe[4], ns[4], r[4], x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            Zc<float>::ld4(pick2(f.p, pc, pl), q.t0, pe);
+            ld4c(pick(L.r, pl) + q.t0, r);
+            if (!first) ld4c(pick(f.x, pl) + q.t0, x);
+            quad_nbr_sum<false>(
+                L, q, h, code, [&](int e, float(&o)[4]) { Zc<float>::ld4(po, e, o); },
+                [&](int e) { return __ldcg(po + e); }, NoParent(), ns);
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                r[m] = r[m] - mean;
+                if (code[m] & CELL_FLUID) {
+                    x[m] = first ? __fmul_rn(alpha, pe[m]) : __fadd_rn(x[m], __fmul_rn(alpha, pe[m]));
+                    float nf = nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
+                    float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
+                    r[m] = __fsub_rn(r[m], __fmul_rn(alpha, ape));
+                    v[0] += (double)r[m] * (double)r[m];
+                }
+                v[1] += r[m];
+            }
+            st4(pick(f.x, pl) + q.t0, x);
+            st4(pick(L.r, pl) + q.t0, r);
+        }
+    }
+}
+
+constexpr int kCoopThreads = 256;
+
+// a phase boundary; an aborted launch ends the loop and returns
+#define COOP_SYNC(expr)                                  \
+    do {                                                 \
+        if (!(expr)) {                                   \
+            if (threadIdx.x == 0) set_cond(g, 0);        \
+            return;                                      \
+        }                                                \
+    } while (0)
 
 template <bool SOLID, class ZT>
-__global__ void __launch_bounds__(kMidThreads) k_mid(G g, Levels a, int lm, int lcc) {
-    pdl_enter();
-    extern __shared__ float sh[];
-    __shared__ CLvl cl[16];
+__global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f, int mode) {
     __shared__ Lvl sl[16];
+    __shared__ CoopBar bar;
     count_launch(g.st);
     copy_levels(a, sl);
+    SolveState* st = g.st;
+    if (threadIdx.x == 0) {
+        bar.gen = ld_acquire_u32(&st->bar_gen);
+        bar.ok = *((volatile unsigned*)&st->bar_abort) == 0;
+    }
     __syncthreads();
-    if (stopped(g)) return;  // the same in every block: the status only changes between launches
-    const int rank = (int)cluster_rank();
-    const int t0 = rank * blockDim.x + threadIdx.x, stride = (int)cluster_size() * blockDim.x;
-    for (int l = lm; l < lcc; l++) {
-        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
-        cluster_sync();
-        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 0, t0, stride);
-        cluster_sync();
-        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
-        cluster_sync();
-        cl_restrict<SOLID, ZT>(g, sl[l], sl[l + 1], l + 1 < lcc, t0, stride);
-        cluster_sync();
+    COOP_SYNC(bar.ok);
+    const int lc = a.lc;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    G gq = g;
+    gq.use_cond = 0;  // the loop condition is set once, below
+    if (mode == COOP_ITER) {
+        // up sweeps of the V-cycle whose coarse group k_coarse just ran
+        for (int l = lc - 1; l >= 0; l--) {
+            const Lvl& L = sl[l];
+            const Lvl& C = sl[l + 1];
+            const int l0 = l == 0;
+            const float mean = l0 ? st_ldf(&st->mean) : 0.0f, zsc = l0 ? st_ldf(&st->zsc) : 1.0f;
+            double zr = 0.0;
+            co_sweep<HS_PROLONG, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+            COOP_SYNC(coop_sync(st, bar));
+            co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+            COOP_SYNC(coop_sync(st, bar));
+            co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+            COOP_SYNC(coop_sync(st, bar));
+            if (l > 0) {
+                co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+                COOP_SYNC(coop_sync(st, bar));
+            } else {
+                co_sweep<HS_ZR, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+                double v[1] = {zr};
+                COOP_SYNC(coop_reduce<1>(g, bar, v, [&](double (&w)[1]) {
+                    zr_epilogue(gq, w[0]);
+                    if (st->it > st->max_iters + 8) st->status = ST_NOCONV;
+                }));
+            }
+        }
+        if (st_ldi(&st->status) != ST_RUNNING) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
+            return;
+        }
+        const Lvl& L = sl[0];
+        {
+            const int pc = st_ldi(&st->pcur);
+            const bool first = st_ldi(&st->it) == 0;
+            const float beta = st_ldf(&st->beta), zinv = st_ldf(&st->zinv);
+            double v[1] = {0.0};
+            co_ap<SOLID, ZT>(g, L, f, pc, first, beta, zinv, t0, stride, v[0]);
+            COOP_SYNC(coop_reduce<1>(g, bar, v, [&](double (&w)[1]) {
+                double pAp = (double)(float)w[0];
+                st->pAp = pAp;
+                st->alpha = (float)(st->zTr / (pAp + 1e-12));
+                st->pcur = pc ^ 1;
+            }));
+        }
+        {
+            const int pc = st_ldi(&st->pcur);
+            const bool first = st_ldi(&st->it) == 0;
+            const float alpha = st_ldf(&st->alpha), mean = st_ldf(&st->mean);
+            double v[2] = {0.0, 0.0};
+            co_xr<SOLID>(g, L, f, pc, first, alpha, mean, t0, stride, v);
+            COOP_SYNC(coop_reduce<2>(g, bar, v, [&](double (&w)[2]) {
+                double rTr = (double)(float)w[0];
+                st->rTr = rTr;
+                st->rsum = w[1];
+                st->x_valid = 1;
+                st->mean = st->all_neumann ? (float)(w[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
+                set_zscale(st, rTr, (double)L.n0 * L.n1 * L.n2);
+                if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
+                else if (rTr < st->tol) st->status = ST_CONVERGED;
+            }));
+        }
+        if (st_ldi(&st->status) != ST_RUNNING) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
+            return;
+        }
     }
-    if (rank == 0) coarse_body<false, SOLID, ZT, true>(g, sl, a.L, lcc, sh, cl);
-    cluster_sync();
-    for (int l = lcc - 1; l >= lm; l--) {
-        cl_sweep<HS_PROLONG, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
-        cluster_sync();
-        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 0, t0, stride);
-        cluster_sync();
-        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 1, t0, stride);
-        cluster_sync();
-        cl_sweep<HS_PLAIN, SOLID, ZT>(g, sl[l], sl[l + 1], 0, t0, stride);
-        if (l > lm) cluster_sync();
+    // down sweeps and restrictions of the next V-cycle, levels 0..lc-1
+    for (int l = 0; l < lc; l++) {
+        const Lvl& L = sl[l];
+        const Lvl& C = sl[l + 1];
+        const int l0 = l == 0;
+        const float mean = l0 ? st_ldf(&st->mean) : 0.0f, zsc = l0 ? st_ldf(&st->zsc) : 1.0f;
+        double zr = 0.0;
+        if (l0) {
+            co_sweep<HS_FIRST, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+            COOP_SYNC(coop_sync(st, bar));
+        }
+        co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+        COOP_SYNC(coop_sync(st, bar));
+        co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+        COOP_SYNC(coop_sync(st, bar));
+        co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+        COOP_SYNC(coop_sync(st, bar));
+        co_restrict<SOLID, ZT>(g, L, C, l0, mean, zsc, l + 1 < lc, t0, stride);
+        if (l + 1 < lc) COOP_SYNC(coop_sync(st, bar));
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 1);
 }
 
 // mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
@@ -1783,8 +2153,28 @@ __global__ void __launch_bounds__(256) k_grad_p(G g, Lvl L, Fine f, Faces U) {
 
 // red-black planes <-> lexicographic field of one level; `valid` (may be
 // NULL) gates the planes' content (x before the first update reads as 0)
+// zsc of an FP16 solver from the RMS of level 0's r planes (V-cycle calls)
+__global__ void __launch_bounds__(256) k_zscale(G g, Lvl L) {
+    double v[1] = {0.0};
+    GRID_STRIDE(t, L.P) {
+        const Slot sl = slot_of(L, t);
+        const int c0 = (sl.i + sl.j) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            if (2 * sl.kk + h >= L.n2) break;
+            const float r = pick(L.r, c0 ^ h)[t];
+            v[0] += (double)r * (double)r;
+        }
+    }
+    if (last_block<1>(g, 5, v)) {
+        double sm[1];
+        final_sum<1>(g, 5, sm);
+        if (threadIdx.x == 0) set_zscale(g.st, sm[0], (double)L.n0 * L.n1 * L.n2);
+    }
+}
+
 __global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p1, float* dst, const int* valid,
-                          int bf16) {
+                          int ztype, const float* scale) {
     if (st) count_launch(st);
     const bool ok = valid == nullptr || *valid != 0;
     GRID_STRIDE(t, L.n0 * L.n1 * L.n2) {
@@ -1794,7 +2184,8 @@ __global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p
         int j = row - i * L.n1;
         const float* p = ((i + j + k) & 1) ? p1 : p0;
         const int e = row * L.H + (k >> 1);
-        dst[t] = ok ? (bf16 ? Zs<__nv_bfloat16>::ld(p, e) : p[e]) : 0.0f;
+        const float v = ztype == 1 ? Zs<__nv_bfloat16>::ld(p, e) : (ztype == 2 ? Zs<__half>::ld(p, e) : p[e]);
+        dst[t] = ok ? (scale ? v * *scale : v) : 0.0f;
     }
 }
 
@@ -1868,6 +2259,48 @@ __global__ void k_apply_A64(G g, Lvl L, const double* p, double* Ap) {
         if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += p[e - stride[a]];
     }
     Ap[e] = (double)n_fluid_lex(g.walls, L, i, j, k) * p[e] - ns;
+}
+
+// Iterative refinement (mixed-precision solves): r = b - A x with b, x and
+// the arithmetic in float64, r stored as the float32 right-hand side of the
+// next inner solve, and sums of r^2 and b^2 (fluid cells) into out[0..1]
+// (last block, block order); then x += d for the inner solve's correction d.
+__global__ void __launch_bounds__(256) k_refine_residual(G g, Lvl L, const double* b, const double* x, float* r32,
+                                                         double* out, int slot) {
+    const int n = L.n0 * L.n1 * L.n2;
+    double v[2] = {0.0, 0.0};
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        double r = 0.0;
+        if (is_fluid(L.bm, e)) {
+            const int k = e % L.n2, j = (e / L.n2) % L.n1, i = e / (L.n1 * L.n2);
+            const int I[3] = {i, j, k}, D[3] = {L.n0, L.n1, L.n2};
+            const int stride[3] = {L.n1 * L.n2, L.n2, 1};
+            double ns = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                if (I[a] < D[a] - 1 && is_fluid(L.bm, e + stride[a])) ns += x[e + stride[a]];
+                if (I[a] > 0 && is_fluid(L.bm, e - stride[a])) ns += x[e - stride[a]];
+            }
+            const double be = b[e];
+            r = be - ((double)n_fluid_lex(g.walls, L, i, j, k) * x[e] - ns);
+            v[0] += r * r;
+            v[1] += be * be;
+        }
+        r32[e] = (float)r;
+    }
+    if (last_block<2>(g, slot, v)) {
+        double sm[2];
+        final_sum<2>(g, slot, sm);
+        if (threadIdx.x == 0) {
+            out[0] = sm[0];
+            out[1] = sm[1];
+        }
+    }
+}
+
+__global__ void k_refine_update(long long n, double* x, const float* d) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        x[e] += (double)d[e];
 }
 
 // ---------------------------------------------------------------------------
@@ -1948,99 +2381,22 @@ void plan_coarse(Ctx& c, bool solid) {
     }
 }
 
-// shared memory of the coarse group lc..L-1 (see k_coarse)
-static size_t coarse_bytes(const Levels& V, int lc, bool solid) {
-    size_t floats = 0, codes = 0;
-    for (int l = lc; l < V.L; l++) {
-        floats += 4 * (size_t)V.lv[l].P;
-        codes += 2 * (size_t)V.lv[l].P;
-    }
-    return floats * sizeof(float) + (solid ? codes * sizeof(unsigned short) : 0) + 16;
-}
-
-// k_mid takes the levels with at most 65536 slots per plane (the per-level
-// kernels of those run a few microseconds each, mostly launch and ramp) down
-// to the first level of at most 1024 slots, which starts block 0's
-// shared-memory group.  Opt-in with EDGE_MGPCG_CLUSTER=1: measured at
-// 256x128x128 it takes 80 us per V-cycle against 66 us for the per-level
-// kernels and k_coarse it replaces (the phases wait on block 0's coarse
-// group and on a cluster barrier each); off when a level in between is not
-// four-slot or the grid has too few levels.
-void plan_mid(Ctx& c, bool solid) {
-    c.cmid = 0;
-    const char* env = getenv("EDGE_MGPCG_CLUSTER");
-    if (!env || env[0] != '1') return;
-    const Levels& V = c.lv;
-    int lm = -1, lcc = -1;
-    for (int l = 1; l < V.L - 1; l++)
-        if (V.lv[l].P <= 65536) { lm = l; break; }
-    if (lm < 1) return;
-    for (int l = lm + 1; l < V.L; l++)
-        if (V.lv[l].P <= 1024) { lcc = l; break; }
-    if (lcc < 0) return;
-    for (int l = lm; l < lcc; l++)
-        if (!V.lv[l].vec) return;
-    size_t bytes = coarse_bytes(V, lcc, solid);
-    if (bytes > kCoarseSmem) return;
-    c.lm = lm;
-    c.lcc = lcc;
-    c.csmem_mid = (int)bytes;
-}
-
-// cluster size for k_mid: 16 blocks (non-portable) if the device schedules
-// such clusters with this shared memory, else 8, else the per-level path
-template <bool S, class ZT>
-static int mid_attrs(int smem) {
-    if (cudaFuncSetAttribute(k_mid<S, ZT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 1;
-    if (cudaFuncSetAttribute(k_mid<S, ZT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 1;
-    return 0;
-}
-void prepare_mid_kernels(Ctx& c) {
-    if (c.lm < 1) return;
-    int bad = mid_attrs<false, float>(c.csmem_mid) | mid_attrs<true, float>(c.csmem_mid) |
-              mid_attrs<false, __nv_bfloat16>(c.csmem_mid) | mid_attrs<true, __nv_bfloat16>(c.csmem_mid);
-    if (bad) {
-        cudaGetLastError();
-        c.cmid = 0;
-        return;
-    }
-    for (int size : {16, 8}) {
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = size;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.gridDim = dim3(size);
-        cfg.blockDim = dim3(kMidThreads);
-        cfg.dynamicSmemBytes = c.csmem_mid;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        int n = 0;
-        if (cudaOccupancyMaxActiveClusters(&n, k_mid<false, float>, &cfg) == cudaSuccess && n >= 1) {
-            c.cmid = size;
-            return;
-        }
-        cudaGetLastError();
-    }
-    c.cmid = 0;
+template <class ZT>
+static int coarse_smem_attrs(int bytes) {
+    CK(cudaFuncSetAttribute(k_coarse<true, false, ZT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_coarse<false, false, ZT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_coarse<true, true, ZT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaFuncSetAttribute(k_coarse<false, true, ZT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return EDGE_OK;
 }
 
 int prepare_coarse_kernels(const Ctx& c) {
     if ((size_t)c.csmem > kCoarseSmem) return EDGE_EINVAL;  // the coarsest level alone must fit
     if (c.csmem > 48 * 1024) {
-        CK(cudaFuncSetAttribute(k_coarse<true, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false, false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<true, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false, true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<true, false, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false, false, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<true, true, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                c.csmem));
-        CK(cudaFuncSetAttribute(k_coarse<false, true, __nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                c.csmem));
+        int r = coarse_smem_attrs<float>(c.csmem);
+        if (r == EDGE_OK) r = coarse_smem_attrs<__nv_bfloat16>(c.csmem);
+        if (r == EDGE_OK) r = coarse_smem_attrs<__half>(c.csmem);
+        if (r != EDGE_OK) return r;
     }
     return EDGE_OK;
 }
@@ -2096,9 +2452,8 @@ static void launch_pdl(void (*k)(KArgs...), int grid, int block, size_t smem, cu
 template <bool S, class ZT>
 void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
     const Levels& V = c.lv;
-    const bool mid = c.cmid > 0;
-    const int lc = mid ? c.lm : V.lc;         // levels 0..lc-1 run per-level kernels
-    const int lgroup = mid ? c.lcc : V.lc;    // first level of the shared-memory group
+    const int lc = V.lc;  // levels 0..lc-1 run per-level kernels, lc..L-1 the shared-memory group
+    const int lgroup = V.lc;
     for (int l = 0; l < lc; l++) {
         const Lvl& L = V.lv[l];
         const Lvl& C = V.lv[l + 1];
@@ -2119,23 +2474,7 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
             launch_pdl(k_restrict<S, ZT>, rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream, c.g, L, C, l0, first);
         }
     }
-    if (mid) {
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute at[2];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = c.cmid;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[1].val.programmaticStreamSerializationAllowed = 1;
-        cfg.gridDim = dim3(c.cmid);
-        cfg.blockDim = dim3(kMidThreads);
-        cfg.dynamicSmemBytes = c.csmem_mid;
-        cfg.stream = stream;
-        cfg.attrs = at;
-        cfg.numAttrs = 2;
-        cudaLaunchKernelEx(&cfg, k_mid<S, ZT>, c.g, V, c.lm, c.lcc);
-    } else if (final_zr && lc == 0) {
+    if (final_zr && lc == 0) {
         launch_pdl(k_coarse<true, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
     } else {
         launch_pdl(k_coarse<false, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
@@ -2164,9 +2503,12 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
 }
 
 void enqueue_vcycle(const Ctx& c, bool solid, cudaStream_t stream, bool final_zr) {
-    if (c.zbf16) {
+    if (c.ztype == 1) {
         if (solid) vcycle_t<true, __nv_bfloat16>(c, stream, final_zr);
         else vcycle_t<false, __nv_bfloat16>(c, stream, final_zr);
+    } else if (c.ztype == 2) {
+        if (solid) vcycle_t<true, __half>(c, stream, final_zr);
+        else vcycle_t<false, __half>(c, stream, final_zr);
     } else {
         if (solid) vcycle_t<true, float>(c, stream, final_zr);
         else vcycle_t<false, float>(c, stream, final_zr);
@@ -2188,9 +2530,12 @@ void cg_kernels(const Ctx& c, cudaStream_t stream) {
 
 // The body of one CG iteration (mgpcg.py:236-277), enqueued on `stream`.
 void enqueue_cg(const Ctx& c, bool solid, cudaStream_t stream) {
-    if (c.zbf16) {
+    if (c.ztype == 1) {
         if (solid) cg_kernels<true, __nv_bfloat16>(c, stream);
         else cg_kernels<false, __nv_bfloat16>(c, stream);
+    } else if (c.ztype == 2) {
+        if (solid) cg_kernels<true, __half>(c, stream);
+        else cg_kernels<false, __half>(c, stream);
     } else {
         if (solid) cg_kernels<true, float>(c, stream);
         else cg_kernels<false, float>(c, stream);
@@ -2200,6 +2545,90 @@ void enqueue_cg(const Ctx& c, bool solid, cudaStream_t stream) {
 void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
     enqueue_cg(c, solid, stream);
     enqueue_vcycle(c, solid, stream, true);
+}
+
+// The cooperative path (k_coop): taken when levels 0..lc-1 all run the
+// four-slot kernels and the device launches a cooperative grid of at least
+// one block per SM; EDGE_MGPCG_COOP=0 selects the per-level kernels.  The
+// grid is every block the device holds at once (occupancy x SMs, at most
+// kMaxBlocks, the capacity of the reduction partials).
+template <bool S, class ZT>
+static int coop_grid_of() {
+    int dev = 0, sms = 0, per_sm = 0, coop_ok = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+        cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop<S, ZT>, kCoopThreads, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    if (!coop_ok || per_sm < 1) return 0;
+    return std::min(per_sm * sms, kMaxBlocks);
+}
+
+void plan_coop(Ctx& c, bool solid) {
+    c.coop = 0;
+    c.coop_grid = 0;
+    const char* env = getenv("EDGE_MGPCG_COOP");
+    if (env && env[0] == '0') return;
+    const Levels& V = c.lv;
+    if (V.lc < 1) return;
+    for (int l = 0; l < V.lc; l++)
+        if (!V.lv[l].vec) return;
+    int grid = 0;
+    if (c.ztype == 1) grid = solid ? coop_grid_of<true, __nv_bfloat16>() : coop_grid_of<false, __nv_bfloat16>();
+    else if (c.ztype == 2) grid = solid ? coop_grid_of<true, __half>() : coop_grid_of<false, __half>();
+    else grid = solid ? coop_grid_of<true, float>() : coop_grid_of<false, float>();
+    if (grid < 1) return;
+    c.coop = 1;
+    c.coop_grid = grid;
+}
+
+template <bool S, class ZT>
+static void launch_coop(const Ctx& c, cudaStream_t stream, int mode) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c.coop_grid);
+    cfg.blockDim = dim3(kCoopThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_coop<S, ZT>, c.g, c.lv, c.f, mode);
+}
+
+template <bool S, class ZT>
+static void coop_t(const Ctx& c, cudaStream_t stream, int mode) {
+    if (mode == COOP_ITER) {
+        // the coarse group of the V-cycle whose down half the previous
+        // launch ran; inside the loop the solve is known to be running
+        G gc = c.g;
+        gc.nochk = 1;
+        launch_pdl(k_coarse<false, S, ZT>, 1, 1024, c.csmem, stream, gc, c.lv);
+    }
+    launch_coop<S, ZT>(c, stream, mode);
+}
+
+// k_coop(DOWN) at the end of the set-up, or one loop iteration
+// (k_coarse + k_coop(ITER))
+void enqueue_coop(const Ctx& c, bool solid, cudaStream_t stream, int mode) {
+    if (c.ztype == 1) {
+        if (solid) coop_t<true, __nv_bfloat16>(c, stream, mode);
+        else coop_t<false, __nv_bfloat16>(c, stream, mode);
+    } else if (c.ztype == 2) {
+        if (solid) coop_t<true, __half>(c, stream, mode);
+        else coop_t<false, __half>(c, stream, mode);
+    } else {
+        if (solid) coop_t<true, float>(c, stream, mode);
+        else coop_t<false, float>(c, stream, mode);
+    }
+}
+
+// one iteration of the CG loop on either path
+void enqueue_loop_body(const Ctx& c, bool solid, cudaStream_t stream) {
+    if (c.coop) enqueue_coop(c, solid, stream, COOP_ITER);
+    else enqueue_iteration(c, solid, stream);
 }
 
 // set-up kernels of Poisson / solve (everything before the CG loop)
@@ -2226,11 +2655,13 @@ void enqueue_setup(Solver* s, Faces U, const float* rhs, double abs_tol, double 
             k_codes<<<rgrid((long long)V.n0 * V.n1 * V.n2), 256, 0, cs>>>(c.g, V);
         }
     }
-    cudaMemsetAsync(c.g.st->counter, 0, sizeof(c.g.st->counter), cs);  // fresh reduction counters
+    // fresh reduction counters and grid barrier
+    cudaMemsetAsync(c.g.st->counter, 0, offsetof(SolveState, kernels) - offsetof(SolveState, counter), cs);
     if (s->solid) k_setup_rhs<true><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
     else k_setup_rhs<false><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
     if (s->solid && !rhs) k_solid_fix<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f);
-    enqueue_vcycle(c, s->solid, cs, true);  // first preconditioner application + z.r + tol
+    if (c.coop) enqueue_coop(c, s->solid, cs, COOP_DOWN);  // the first V-cycle's down half
+    else enqueue_vcycle(c, s->solid, cs, true);           // first preconditioner application + z.r + tol
 }
 
 // gradient update (Poisson) or the solution copy (solve)
@@ -2243,7 +2674,7 @@ void enqueue_finish(Solver* s, Faces U, const float* rhs, float* xout, cudaStrea
         k_grad_p<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U);
         if (s->solid) k_apply_solid<<<grid_for(n), 256, 0, cs>>>(c.g.st, nx, ny, nz, L0.bm, s->bvel, U);
     } else {
-        k_from_rb<<<rgrid(n), 256, 0, cs>>>(c.g.st, L0, c.f.x[0], c.f.x[1], xout, &c.g.st->x_valid, 0);
+        k_from_rb<<<rgrid(n), 256, 0, cs>>>(c.g.st, L0, c.f.x[0], c.f.x[1], xout, &c.g.st->x_valid, 0, nullptr);
     }
 }
 
@@ -2284,6 +2715,13 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     cudaGraphNode_t cnode;
     CK(cudaGraphAddNode(&cnode, graph, &leaf, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaGraph_t b2;
+    if (s->ctx.coop) {
+        //    k_coarse + k_coop(ITER), which sets the loop condition itself
+        CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        enqueue_coop(s->ctx, s->solid, cs, COOP_ITER);
+        CK(cudaStreamEndCapture(cs, &b2));
+    } else {
     //    the CG kernels, then if (still running) { V-cycle }: the V-cycle's
     //    kernels are captured with nochk (see stopped())
     cudaGraphConditionalHandle vh;
@@ -2292,7 +2730,6 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     s->ctx.g.use_vcond = 1;
     CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     enqueue_cg(s->ctx, s->solid, cs);
-    cudaGraph_t b2;
     CK(cudaStreamEndCapture(cs, &b2));
     CK(cudaGraphGetNodes(body, nullptr, &nn));
     nodes.resize(nn);
@@ -2317,6 +2754,7 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     enqueue_vcycle(vc, s->solid, cs, true);
     CK(cudaStreamEndCapture(cs, &b2));
     s->ctx.g.use_vcond = 0;  // launches outside this graph set no IF condition
+    }
     // 3) finish
     CK(cudaStreamBeginCaptureToGraph(cs, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     enqueue_finish(s, U, rhs, xout, cs);
@@ -2339,7 +2777,7 @@ int run_solve_eager(Solver* s, Faces U, const float* rhs, float* xout, double ab
         CK(cudaMemcpyAsync(&s->st_host->status, &s->ctx.g.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
         CK(cudaStreamSynchronize(cs));
         if (s->st_host->status != ST_RUNNING) break;
-        enqueue_iteration(s->ctx, s->solid, cs);
+        enqueue_loop_body(s->ctx, s->solid, cs);
     }
     enqueue_finish(s, U, rhs, xout, cs);
     return cu(cudaPeekAtLastError());
@@ -2367,6 +2805,16 @@ int run_solve(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol,
     return cu(cudaGraphLaunch(exec, stream));
 }
 
+// the C-ABI code of a solve status
+int status_code(int st) {
+    switch (st) {
+        case ST_CONVERGED: return EDGE_OK;
+        case ST_NAN: return EDGE_ENAN;
+        case ST_TIMEOUT: return EDGE_ETIMEOUT;
+        default: return EDGE_ENOCONV;
+    }
+}
+
 // levels of a grid (mgpcg.py:34); EDGE_EINVAL when a level would not halve
 int level_count(int nx, int ny, int nz, int base_level, int* L) {
     int mn = std::min(nx, std::min(ny, nz));
@@ -2390,7 +2838,7 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
                       const float* bvel, int precision) {
     if (!handle || !bt || nx < 2 || ny < 2 || nz < 2) return EDGE_EINVAL;
     if ((mask == nullptr) != (bvel == nullptr)) return EDGE_EINVAL;
-    if (precision != 0 && precision != 1) return EDGE_EINVAL;
+    if (precision < 0 || precision > 2) return EDGE_EINVAL;
     long long n = (long long)nx * ny * nz;
     if (n * 3 >= (1LL << 31)) return EDGE_EINVAL;
     int L = 0;
@@ -2403,7 +2851,7 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     Ctx& c = s->ctx;
     memset(&c, 0, sizeof(c));
     c.lv.L = L;
-    c.zbf16 = precision == 1;
+    c.ztype = precision;
     for (int q = 0; q < 6; q++) c.g.bt[q] = bt[q];
     c.g.walls = 0;
     for (int q = 0; q < 6; q++) c.g.walls |= (bt[q] == 2) << q;
@@ -2414,7 +2862,7 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
         size_t pa = plane_alloc(V.P);
         // level 0's r is the FP32 CG residual; the other level arrays are
         // BF16 in the mixed-precision solver
-        const size_t esz = precision == 1 ? 2 : 4, esr = l == 0 ? 4 : esz;
+        const size_t esz = precision != 0 ? 2 : 4, esr = l == 0 ? 4 : esz;
         r = alloc(s, (void**)&V.r[0], 2 * pa * esr);
         if (r == EDGE_OK) r = alloc(s, (void**)&V.z[0], 2 * pa * esz);
         if (r == EDGE_OK) r = cu(cudaMemset(V.z[0], 0, 2 * pa * esz));
@@ -2429,10 +2877,7 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     }
     plan_coarse(c, s->solid);
     if (r == EDGE_OK) r = prepare_coarse_kernels(c);
-    if (r == EDGE_OK) {
-        plan_mid(c, s->solid);
-        prepare_mid_kernels(c);
-    }
+    if (r == EDGE_OK) plan_coop(c, s->solid);
     const size_t pa0 = plane_alloc(c.lv.lv[0].P);
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.x[0], 2 * pa0 * sizeof(float));
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.p[0][0], 4 * pa0 * sizeof(float));
@@ -2444,12 +2889,14 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
         c.f.p[1][0] = c.f.p[0][0] + 2 * pa0;
         c.f.p[1][1] = c.f.p[0][0] + 3 * pa0;
     }
-    if (r == EDGE_OK) r = alloc(s, (void**)&c.g.partials, 3 * (size_t)(kMaxBlocks + 64) * sizeof(double));
+    if (r == EDGE_OK) r = alloc(s, (void**)&c.g.partials, 4 * (size_t)(kMaxBlocks + 64) * sizeof(double));
     if (r == EDGE_OK) r = alloc(s, (void**)&c.g.st, sizeof(SolveState));
     if (r == EDGE_OK) {
         SolveState st;
         memset(&st, 0, sizeof(st));
         st.all_neumann = (bt[0] + bt[1] + bt[2] + bt[3] + bt[4] + bt[5]) == 12;
+        st.zsc = st.zinv = 1.0f;
+        st.zscaled = precision == 2;
         r = cu(cudaMemcpy(c.g.st, &st, sizeof(st), cudaMemcpyHostToDevice));
     }
     if (r == EDGE_OK) r = cu(cudaMallocHost((void**)&s->st_host, sizeof(SolveState)));
@@ -2513,7 +2960,7 @@ int edge_mgpcg_result(void* handle, int* iters, double* rTr, int* status, void* 
     if (iters) *iters = st.it;
     if (rTr) *rTr = st.rTr;
     if (status)
-        *status = st.status == ST_CONVERGED ? EDGE_OK : (st.status == ST_NAN ? EDGE_ENAN : EDGE_ENOCONV);
+        *status = status_code(st.status);
     return EDGE_OK;
 }
 
@@ -2548,10 +2995,11 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
         }
     }
     k_to_rb<<<rgrid(n), 256, 0, st>>>(L0, r, L0.r[0], L0.r[1]);
+    if (c.ztype == 2) k_zscale<<<rgrid(L0.P), 256, 0, st>>>(c.g, L0);  // the input's scale
     // outside a graph there is no loop condition to set
     c.g.use_cond = 0;
     enqueue_vcycle(c, s->solid, st, false);
-    k_from_rb<<<rgrid(n), 256, 0, st>>>(nullptr, L0, L0.z[0], L0.z[1], z, nullptr, c.zbf16);
+    k_from_rb<<<rgrid(n), 256, 0, st>>>(nullptr, L0, L0.z[0], L0.z[1], z, nullptr, c.ztype, &c.g.st->zinv);
     return cu(cudaPeekAtLastError());
 }
 
@@ -2560,6 +3008,25 @@ int edge_mgpcg_apply_A_f64(void* handle, const double* p, double* Ap, void* stre
     Solver* s = (Solver*)handle;
     const Lvl& L = s->ctx.lv.lv[0];
     k_apply_A64<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx.g, L, p, Ap);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_refine_residual(void* handle, const double* b, const double* x, float* r, double* sums,
+                               void* stream) {
+    if (!handle || !b || !x || !r || !sums) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& L = s->ctx.lv.lv[0];
+    k_refine_residual<<<rgrid((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx.g, L, b, x, r,
+                                                                                            sums, 6);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_refine_update(void* handle, double* x, const float* d, void* stream) {
+    if (!handle || !x || !d) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& L = s->ctx.lv.lv[0];
+    const long long n = (long long)L.n0 * L.n1 * L.n2;
+    k_refine_update<<<rgrid(n), 256, 0, (cudaStream_t)stream>>>(n, x, d);
     return cu(cudaPeekAtLastError());
 }
 
@@ -2580,7 +3047,7 @@ int edge_mgpcg_get(void* handle, int which, float* dst, void* stream) {
     if (which == 0) return cu(cudaMemcpyAsync(dst, s->ctx.f.div, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     if (which == 1) {
         k_from_rb<<<rgrid((long long)n), 256, 0, st>>>(nullptr, L, s->ctx.f.x[0], s->ctx.f.x[1], dst,
-                                                      &s->ctx.g.st->x_valid, 0);
+                                                      &s->ctx.g.st->x_valid, 0, nullptr);
         return cu(cudaPeekAtLastError());
     }
     return EDGE_EINVAL;
@@ -2606,7 +3073,7 @@ constexpr long long kNoAllocMaxCells = 262144;  // 64^3 cells
 constexpr long long kNoAllocFloats = 8 * kNoAllocMaxCells + 4096;
 
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
-static __device__ __align__(256) double g_noalloc_partials[3 * (kMaxBlocks + 64)];
+static __device__ __align__(256) double g_noalloc_partials[4 * (kMaxBlocks + 64)];
 static __device__ __align__(256) SolveState g_noalloc_state;
 
 struct NoAllocAddrs {
@@ -2619,11 +3086,14 @@ constexpr int kMaxDevices = 64;
 NoAllocAddrs g_noalloc_addrs[kMaxDevices];
 
 // Host code may not use the arrays' names as device addresses: resolve them
-// once per device (with that device current).
+// once per device (with that device current).  The lookup is serialised, so
+// host threads whose first calls on a device coincide fill the entry once.
 int noalloc_addrs(NoAllocAddrs** out) {
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return EDGE_EINVAL;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
     NoAllocAddrs& a = g_noalloc_addrs[dev];
     if (!a.ready) {
         CK(cudaGetSymbolAddress((void**)&a.scratch, g_noalloc_scratch));
@@ -2686,16 +3156,13 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     c.g.use_cond = 0;
     plan_coarse(c, false);
     r = prepare_coarse_kernels(c);
-    if (r == EDGE_OK) {
-        plan_mid(c, false);
-        prepare_mid_kernels(c);
-    }
     if (r != EDGE_OK) return r;
     // the loop state starts clean on every call (the arrays keep the last
     // call's contents; the set-up and the first iteration overwrite what is read)
     SolveState init;
     memset(&init, 0, sizeof(init));
     init.all_neumann = (bt[0] + bt[1] + bt[2] + bt[3] + bt[4] + bt[5]) == 12;
+    init.zsc = init.zinv = 1.0f;
     CK(cudaMemcpyAsync(c.g.st, &init, sizeof(init), cudaMemcpyHostToDevice, cs));
     Faces U = {{ux, uy, uz}, {nullptr, nullptr, nullptr}};
     enqueue_setup(&s, U, nullptr, abs_tol, rel_tol, max_iters, cs);
@@ -2713,6 +3180,6 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     CK(cudaStreamSynchronize(cs));
     if (iters) *iters = fin.it;
     if (rTr) *rTr = fin.rTr;
-    if (status) *status = fin.status == ST_CONVERGED ? EDGE_OK : (fin.status == ST_NAN ? EDGE_ENAN : EDGE_ENOCONV);
+    if (status) *status = status_code(fin.status);
     return EDGE_OK;
 }

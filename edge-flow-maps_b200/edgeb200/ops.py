@@ -127,10 +127,12 @@ def map_unpack(variant, packed, psi, T, dT, d2T):
     _call("edge_map_unpack", variant, nx, ny, nz, ptr(packed), ptr(psi), *_p3(T), *_p3(dT), *_p3(d2T), stream())
 
 
-def march_packed(variant, u, dx, dt, eps, packed_in, packed_out, res, identity=False):
+def march_packed(variant, u, dx, dt, eps, packed_in, packed_out, res, identity=False, f64_compose=False):
+    """f64_compose: accumulate the composed Jacobian in float64 (EDGE)."""
     _check_packed(variant, packed_out, res)
+    flags = (1 if identity else 0) | (2 if f64_compose else 0)
     _call("edge_march_packed", variant, *res, F(dx), F(dt), F(eps), *_p3(u), ptr(packed_in), ptr(packed_out),
-          int(bool(identity)), stream())
+          flags, stream())
     _launched[0] += variant != 2
 
 
@@ -236,6 +238,16 @@ def clamp_max(x, hi):
 def split_central_vector(vc, u):
     nx, ny, nz = cell_dims(vc)
     _call("edge_split_central_vector", nx, ny, nz, ptr(vc), *_p3(u), stream())
+
+
+def get_central_vector(u, vc):
+    nx, ny, nz = cell_dims(vc)
+    _call("edge_get_central_vector", nx, ny, nz, *_p3(u), ptr(vc), stream())
+
+
+def curl(vf, cf, dx):
+    nx, ny, nz = cell_dims(vf)
+    _call("edge_curl", nx, ny, nz, F(dx), ptr(vf), ptr(cf), stream())
 
 
 # ---- particles ----------------------------------------------------------------

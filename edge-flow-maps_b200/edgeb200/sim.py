@@ -33,9 +33,17 @@ VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL, 
 class EdgeSim:
     def __init__(self, res, dx, variant="edge", cfl=0.5, reinit_every=12, ed_eps=None, base_level=3,
                  bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda", solid=None,
-                 emitters=None, packed=True):
+                 emitters=None, packed=True, precision=0):
+        """precision: 0 runs the reference's float32 arithmetic; 1 (BF16) and
+        2 (FP16) store the projection's V-cycle levels in 16 bits (float32
+        residuals and arithmetic, float64 dot products, as in
+        Projection(precision=...)) and accumulate the EDGE march's composed
+        Jacobian in float64."""
         if variant not in VARIANTS:
             raise ValueError(f"variant must be one of {sorted(VARIANTS)}")
+        if precision not in (0, 1, 2):
+            raise ValueError("precision must be 0 (float32), 1 (BF16 V-cycle) or 2 (FP16 V-cycle)")
+        self.precision = int(precision)
         N.load()
         self.res = tuple(int(n) for n in res)
         self.dx = float(dx)
@@ -87,10 +95,10 @@ class EdgeSim:
         self.solid = solid is not None
         if self.solid:
             mask, bvel = solid
-            self.proj = Projection(r, base_level=base_level, mask=mask, bvel=bvel)
+            self.proj = Projection(r, base_level=base_level, mask=mask, bvel=bvel, precision=self.precision)
             self.abs_tol, self.rel_tol, self.max_iters = 1e-12, 0.0, 100  # mgpcg_solid.py:413-416
         else:
-            self.proj = Projection(r, base_level=base_level)
+            self.proj = Projection(r, base_level=base_level, precision=self.precision)
             self.max_iters = 400  # mgpcg.py:434-438
         self.emitters = emitters
         self.side_stream = torch.cuda.Stream(device=device)
@@ -389,7 +397,7 @@ class EdgeSim:
                 ops.march_ge_packed(self.u, dx, dt, src, dst, self.res)
             else:
                 ops.march_packed(self.hv, self.u, dx, dt, eps, src, dst, self.res,
-                                 identity=reinit and self.variant == "edge")
+                                 identity=reinit and self.variant == "edge", f64_compose=self.precision > 0)
             self.cur ^= 1
             return
         src, dst = self.maps[self.cur], self.maps[self.cur ^ 1]
@@ -486,6 +494,43 @@ def leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.03, circulation=1.0, x_st
     u = zeros_faces(res, None, device)
     ops.split_central_vector(u_c, u)
     return u, smoke
+
+
+def random_potential_init(res, dx, kmax=8, slope=-17.0 / 6.0, seed=0, u_max=1.0, device="cuda"):
+    """Divergence-free-in-the-continuum initial velocity u = curl A of a seeded
+    random vector potential: every Fourier mode of the grid's periodic box
+    with integer index vector m, 1 <= |m| <= kmax, gets an independent
+    complex normal amplitude per component scaled by |m|^slope (numpy
+    default_rng(seed), modes in lexicographic order of (m0, m1, m2) with
+    m2 >= 0); A is evaluated at the cell centres by an inverse real FFT,
+    u_c = curl(A) by the reference's clamped central differences
+    (taichi_utils.py:69-92), split to the faces (taichi_utils.py:103-116) and
+    scaled so that max |u| = u_max.  No reference counterpart (the
+    512x256x256 mixed-precision workload)."""
+    import numpy as np
+    nx, ny, nz = res
+    rng = np.random.default_rng(seed)
+    r = np.arange(-kmax, kmax + 1)
+    m0, m1, m2 = np.meshgrid(r, r, np.arange(0, kmax + 1), indexing="ij")
+    k2 = m0 ** 2 + m1 ** 2 + m2 ** 2
+    sel = (k2 >= 1) & (k2 <= kmax * kmax)
+    m0, m1, m2, k2 = m0[sel], m1[sel], m2[sel], k2[sel]
+    amp = np.power(k2.astype(np.float64), slope / 2.0)
+    coef = (rng.standard_normal((3, m0.size)) + 1j * rng.standard_normal((3, m0.size))) * amp
+    spec = torch.zeros((3, nx, ny, nz // 2 + 1), dtype=torch.complex128, device=device)
+    idx = (torch.from_numpy(m0 % nx).to(device), torch.from_numpy(m1 % ny).to(device),
+           torch.from_numpy(m2).to(device))
+    for c in range(3):
+        spec[c][idx] = torch.from_numpy(coef[c]).to(device)
+    A = torch.fft.irfftn(spec, s=(nx, ny, nz), dim=(1, 2, 3), norm="forward")
+    A = A.permute(1, 2, 3, 0).contiguous().float()
+    u_c = zeros_cells(res, 3, device)
+    ops.curl(A, u_c, dx)
+    del A, spec
+    u_c.mul_(float(u_max) / float(u_c.norm(dim=-1).max()))
+    u = zeros_faces(res, None, device)
+    ops.split_central_vector(u_c, u)
+    return u
 
 
 def wedge_mask(res, dx, apex=(0.1, 0.5, 0.2), chord=1.0, half_angle_deg=15.0, aoa_deg=0.0, thickness_cells=4,

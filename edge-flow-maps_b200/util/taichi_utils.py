@@ -52,17 +52,9 @@ def split_central_vector(vc, vx, vy, vz):
 
 def get_central_vector(vx, vy, vz, vc):
     """taichi_utils.py:95-100 (output helper)."""
-    vc[..., 0] = 0.5 * (vx[1:] + vx[:-1])
-    vc[..., 1] = 0.5 * (vy[:, 1:] + vy[:, :-1])
-    vc[..., 2] = 0.5 * (vz[:, :, 1:] + vz[:, :, :-1])
+    ops.get_central_vector((vx, vy, vz), vc)
 
 
 def curl(vf, cf, dx):
-    """taichi_utils.py:70-92 (output helper; clamped central differences)."""
-    p = torch.nn.functional.pad(vf.permute(3, 0, 1, 2)[None], (1, 1, 1, 1, 1, 1), mode="replicate")[0]
-    inv = 1.0 / (2 * dx)
-    d = lambda c, a: (p[c].narrow(a, 2, vf.shape[a]) - p[c].narrow(a, 0, vf.shape[a])).narrow(  # noqa: E731
-        (a + 1) % 3, 1, vf.shape[(a + 1) % 3]).narrow((a + 2) % 3, 1, vf.shape[(a + 2) % 3]) * inv
-    cf[..., 0] = d(2, 1) - d(1, 2)
-    cf[..., 1] = d(0, 2) - d(2, 0)
-    cf[..., 2] = d(1, 0) - d(0, 1)
+    """taichi_utils.py:69-92 (output helper; clamped central differences)."""
+    ops.curl(vf, cf, dx)

@@ -37,6 +37,7 @@ extern "C" {
 #define EDGE_ENAN (-4)       /* non-finite residual */
 #define EDGE_ESTALL (-5)     /* residual stalled (flexible PCG fallback taken) */
 #define EDGE_ESTATE (-6)     /* call order / handle state error */
+#define EDGE_ETIMEOUT (-7)   /* a bounded wait inside a solver launch ran out of time */
 
 /* Hermite variants (sim/hermite.py) */
 #define EDGE_HERMITE_FD 0    /* interp_(grad_)hermite_fd_unroll, hermite.py:65-295 (ED4) */
@@ -142,10 +143,16 @@ int edge_map_unpack(int variant, int nx, int ny, int nz, const float *packed, fl
                     void *stream);
 /* The EDGE / ED4 / ED8 marches (hermite.py:1426-1521, 1375-1395, 1290-1338)
  * on packed maps: in_packed is the accumulated map, out_packed receives the
- * new one (must not alias).  identity (EDGE only): compose with the identity
- * map, in_packed is not read. */
+ * new one (must not alias).  flags (EDGE only):
+ *   EDGE_MARCH_IDENTITY     compose with the identity map, in_packed is not
+ *                           read (the step right after a reinitialisation);
+ *   EDGE_MARCH_F64_COMPOSE  accumulate each entry of the composed Jacobian
+ *                           T_old(psi_step) T_step (hermite.py:960-980, float32
+ *                           in the reference) in float64, rounded once. */
+#define EDGE_MARCH_IDENTITY 1
+#define EDGE_MARCH_F64_COMPOSE 2
 int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, float epsilon, const float *ux,
-                      const float *uy, const float *uz, const float *in_packed, float *out_packed, int identity,
+                      const float *uy, const float *uz, const float *in_packed, float *out_packed, int flags,
                       void *stream);
 /* edge_march_ge on packed maps (the ED8 planes 0-7); out_packed must not
  * alias in_packed. */
@@ -234,7 +241,10 @@ int edge_copy(long long n, const float *src, float *dst, void *stream);
  * bt: boundary_types as int[6] = {x-, x+, y-, y+, z-, z+} (2 = wall).
  * mask / bvel (device, int32 cells / vec3 cells) select the solid solver;
  * both NULL for the plain one.  precision: 0 = float32 V-cycle (the
- * reference), 1 = mixed (bf16 smoother storage, float32 residuals). */
+ * reference), 1 = mixed with bf16 smoother storage, 2 = mixed with fp16
+ * smoother storage (the V-cycle runs on the residual times a power of two
+ * that brings its RMS near 1); both keep float32 residuals and arithmetic
+ * and float64 dot products. */
 int edge_mgpcg_create(void **handle, int nx, int ny, int nz, int base_level, const int *bt, const int *mask,
                       const float *bvel, int precision);
 int edge_mgpcg_destroy(void *handle);
@@ -259,6 +269,14 @@ int edge_mgpcg_apply_A(void *handle, const float *p, float *Ap, void *stream);
 /* The same operator in float64 (no reference counterpart): the FP64
  * reference solve that the precision study measures errors against. */
 int edge_mgpcg_apply_A_f64(void *handle, const double *p, double *Ap, void *stream);
+/* Iterative refinement of a mixed-precision solve (no reference counterpart):
+ * r = b - A x with b, x (device float64, cell layout) and the arithmetic in
+ * float64, r written as float32 (the right-hand side of the next inner solve),
+ * and sums[0] = sum r^2, sums[1] = sum b^2 over fluid cells (device float64,
+ * block-ordered sums); then x += d for the inner solve's correction d. */
+int edge_mgpcg_refine_residual(void *handle, const double *b, const double *x, float *r, double *sums,
+                               void *stream);
+int edge_mgpcg_refine_update(void *handle, double *x, const float *d, void *stream);
 /* Copy the divergence (u_div) or pressure (p) of the last Poisson call. */
 int edge_mgpcg_get(void *handle, int which, float *dst, void *stream);
 /* Number of multigrid levels (mgpcg.py:34). */
@@ -400,6 +418,12 @@ int edge_clamp_max(long long n, float hi, float *x, void *stream);
 /* split_central_vector, taichi_utils.py:103-116 */
 int edge_split_central_vector(int nx, int ny, int nz, const float *vc, float *ux, float *uy, float *uz,
                               void *stream);
+/* get_central_vector, taichi_utils.py:95-100: vc (nx,ny,nz,3) = face averages */
+int edge_get_central_vector(int nx, int ny, int nz, const float *ux, const float *uy, const float *uz, float *vc,
+                            void *stream);
+/* curl, taichi_utils.py:69-92: cf = curl of the cell vec3 field vf (both
+ * (nx,ny,nz,3)), central differences with clamped neighbour indices */
+int edge_curl(int nx, int ny, int nz, float dx, const float *vf, float *cf, void *stream);
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _SO = os.path.join(_HERE, "_build", "libedge_oracle.so")
-_lib = None
+_SO_FMA = os.path.join(_HERE, "_build", "libedge_oracle_fma.so")
+_libs = {}
+_variant = ["plain"]
 
 F32 = np.float32
 
@@ -28,19 +30,36 @@ def build():
 
 
 def lib():
-    global _lib
-    if _lib is None:
+    v = _variant[0]
+    if v not in _libs:
         # spinning OpenMP barriers collapse when any core is busy (a torch or
         # driver thread); the multigrid's many short parallel loops need
         # blocking waits unless the caller chose otherwise
         os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
-        if not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(os.path.join(_HERE, "edge_oracle.c")):
+        so = _SO_FMA if v == "fma" else _SO
+        if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(os.path.join(_HERE, "edge_oracle.c")):
             build()
-        _lib = ctypes.CDLL(_SO)
-        _lib.orc_calc_max_speed.restype = ctypes.c_float
+        L = ctypes.CDLL(so)
+        L.orc_calc_max_speed.restype = ctypes.c_float
         for name in ("orc_poisson", "orc_poisson_solid", "orc_vcycle"):
-            getattr(_lib, name).restype = ctypes.c_int
-    return _lib
+            getattr(L, name).restype = ctypes.c_int
+        _libs[v] = L
+    return _libs[v]
+
+
+class fma_twin:
+    """Context manager: oracle calls inside it run the fused-multiply-add
+    build of the same source (libedge_oracle_fma.so), a second float32
+    evaluation of the reference arithmetic that differs only in rounding."""
+
+    def __enter__(self):
+        self._prev = _variant[0]
+        _variant[0] = "fma"
+        return self
+
+    def __exit__(self, *exc):
+        _variant[0] = self._prev
+        return False
 
 
 def _p(a):
@@ -412,6 +431,37 @@ def split_central_vector(vc):
     return out
 
 
+def get_central_vector(u):
+    """taichi_utils.py:95-100: the face average per cell (float32)."""
+    ux, uy, uz = (np.asarray(a, F32) for a in u)
+    vc = np.empty((ux.shape[0] - 1,) + ux.shape[1:] + (3,), F32)
+    vc[..., 0] = F32(0.5) * (ux[1:] + ux[:-1])
+    vc[..., 1] = F32(0.5) * (uy[:, 1:] + uy[:, :-1])
+    vc[..., 2] = F32(0.5) * (uz[:, :, 1:] + uz[:, :, :-1])
+    return vc
+
+
+def curl(vf, dx):
+    """taichi_utils.py:69-92: central differences with the neighbour index
+    clamped to the grid (sample, taichi_utils.py:61-66), float32."""
+    vf = np.asarray(vf, F32)
+    inv = F32(1.0) / (F32(2.0) * F32(dx))
+    p = np.pad(vf, ((1, 1), (1, 1), (1, 1), (0, 0)), mode="edge")
+    n0, n1, n2 = vf.shape[:3]
+
+    def d(c, axis):
+        sl_hi = [slice(1, 1 + n0), slice(1, 1 + n1), slice(1, 1 + n2), c]
+        sl_lo = list(sl_hi)
+        sl_hi[axis] = slice(2, 2 + vf.shape[axis])
+        sl_lo[axis] = slice(0, vf.shape[axis])
+        return inv * (p[tuple(sl_hi)] - p[tuple(sl_lo)])
+    cf = np.empty_like(vf)
+    cf[..., 0] = d(2, 1) - d(1, 2)
+    cf[..., 1] = d(0, 2) - d(2, 0)
+    cf[..., 2] = d(1, 0) - d(0, 1)
+    return cf
+
+
 # ----------------------------------------------------------------------------
 # the EDGE substep (run_edge.py:588-712), non-particle, non-solid path
 # ----------------------------------------------------------------------------
@@ -442,16 +492,24 @@ def emit_smoke(res, dx, centers, colors, radius, smoke):
 
 
 def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_clamp=True, dt=None,
-                 abs_tol=1e-12, rel_tol=1e-12, variant="edge", solid=None, emitters=None, particles=None):
+                 abs_tol=1e-12, rel_tol=1e-12, variant="edge", solid=None, emitters=None, particles=None,
+                 max_iters=400, project=None):
     """One iteration of run_edge.py:588-712 (variant "edge"), run_ed4.py:
     402-484 ("ed4"), run_ed8.py:365-451 ("ed8"), run_ge.py:363-448 ("ge",
     the ED8 substep with the GE march) or run_efm.py:319-406 ("efm", the ED8
-    substep with the face map backtracked through the cached velocities); no
-    particles, no solids,
+    substep with the face map backtracked through the cached velocities);
     no frame bookkeeping: dt = CFL*dx/max_speed unless given.  Returns
-    (dt, iters)."""
+    (dt, iters).
+
+    max_iters bounds the plain projection's CG loop (mgpcg.py:440-445 fixes
+    it at 400).  `project`, when given, replaces both projections of the
+    substep: it is called as project(u, force) with the face velocity list
+    (and the Poisson_with_buffer force list or None), must update u in place
+    and return an iteration count; the parity tests use it to hand both
+    implementations the same projected velocity."""
     if variant != "edge":
-        return _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_tol, rel_tol, variant)
+        return _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_tol, rel_tol, variant,
+                           max_iters, project)
     dx = float(st.dx)
     eps = F32(ed_eps if ed_eps is not None else 0.025 * dx)
     st.i += 1
@@ -465,10 +523,14 @@ def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_
         dt = cfl * dx / ms  # run_edge.py:595-614 (Python double)
     dt32 = F32(dt)
 
-    def project(u, force=None):
+    hook = project
+
+    def _project(u, force=None):
+        if hook is not None:
+            return hook(u, force)
         if solid is not None:
             return poisson_solid(u, solid[0], solid[1], base_level)[0]
-        return poisson(u, base_level, abs_tol=abs_tol, rel_tol=rel_tol, force=force)[0]
+        return poisson(u, base_level, abs_tol=abs_tol, rel_tol=rel_tol, max_iters=max_iters, force=force)[0]
     if j == 0:
         # run_edge.py:616-625
         for a in range(3):
@@ -500,7 +562,7 @@ def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_
         err = map_smoke(st.smoke, st.phi, dx)
         st.init_smoke = np.minimum(st.init_smoke + F32(1.0) * err, F32(1.0))
     st.u = advect_u_semi_lagrangian(st.u, dx, F32(0.5 * dt))
-    it1 = project(st.u)
+    it1 = _project(st.u)
     st.psi, st.T, st.dT = march_edge(st.u, st.psi, st.T, st.dT, dx, dt32, eps)
     for a in range(3):
         advance_map(st.u, st.phi[a], st.F[a], a, dx, dt32)
@@ -528,13 +590,19 @@ def edge_substep(st, cfl=0.5, reinit_every=12, ed_eps=None, base_level=3, bfecc_
     st.smoke = smoke_new
     if vis is not None:
         particles["vis"] = [np.zeros_like(a) for a in st.u]
-        it2 = project(st.u, force=particles["vis"])
+        it2 = _project(st.u, force=particles["vis"])
     else:
-        it2 = project(st.u)
+        it2 = _project(st.u)
     return dt, (it1, it2)
 
 
-def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_tol, rel_tol, variant):
+def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_tol, rel_tol, variant, max_iters,
+                project):
+    def _project(u):
+        if project is not None:
+            return project(u, None)
+        return poisson(u, base_level, abs_tol=abs_tol, rel_tol=rel_tol, max_iters=max_iters)[0]
+
     dx = float(st.dx)
     eps = F32(ed_eps if ed_eps is not None else 0.025 * dx)
     st.i += 1
@@ -556,7 +624,7 @@ def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_
         st.init_u = [a.copy() for a in st.u]
         st.init_smoke = st.smoke.copy()
     st.u = advect_u_semi_lagrangian(st.u, dx, F32(0.5 * dt))
-    it1 = poisson(st.u, base_level, abs_tol=abs_tol, rel_tol=rel_tol)[0]
+    it1 = _project(st.u)
     if variant == "efm":
         # run_efm.py:360-365: cache the projected velocity, backtrack the faces
         if not hasattr(st, "u_cache"):
@@ -600,5 +668,5 @@ def _ed_substep(st, cfl, reinit_every, ed_eps, base_level, bfecc_clamp, dt, abs_
         clamp_smoke(st.init_smoke, smoke_new, pf, dx)
     st.u = [clamp_u(e, a) for e, a in zip(err_u, u_new)] if bfecc_clamp else err_u
     st.smoke = smoke_new
-    it2 = poisson(st.u, base_level, abs_tol=abs_tol, rel_tol=rel_tol)[0]
+    it2 = _project(st.u)
     return dt, (it1, it2)

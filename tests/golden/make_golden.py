@@ -672,6 +672,24 @@ def init_rings():
 
 
 @fixture
+def output_fields():
+    """The output helpers get_central_vector (taichi_utils.py:95-100) and
+    curl (taichi_utils.py:69-92) on a seeded velocity."""
+    res = (12, 8, 10)
+    g = Grid(res, 1.0 / 8.0)
+    rng = np.random.default_rng(21)
+    faces = [sfield(s) for s in g.faces()]
+    for f, s in zip(faces, g.faces()):
+        f.from_numpy(rng.standard_normal(s).astype(F32))
+    vc = vfield(res)
+    tu.get_central_vector(*faces, vc)
+    w = vfield(res)
+    tu.curl(vc, w, g.dx)
+    save("output_fields", res=np.array(res), meta_dx=g.dx, u_x=faces[0], u_y=faces[1], u_z=faces[2],
+         u_center=vc, curl=w)
+
+
+@fixture
 def edge_steps():
     """Two substeps of the EDGE driver loop (run_edge.py:588-712: reinit at
     j == 0, SL pre-advection, projection, EDGE and forward-map marches,

@@ -61,6 +61,10 @@ def test_argument_validation_without_device():
     bt = (ctypes.c_int * 6)(2, 2, 2, 2, 2, 2)
     assert lib.edge_mgpcg_create(ctypes.byref(h), 10, 8, 8, 1, bt, null, null, 0) == N.EDGE_EINVAL
     assert lib.edge_mgpcg_create(ctypes.byref(h), 16, 8, 8, 1, bt, null, null, 7) == N.EDGE_EINVAL
+    # the allocation-free projection refuses grids beyond its static scratch
+    # (64^3 cells) before any CUDA call
+    assert lib.edge_mgpcg_poisson_noalloc(128, 64, 64, 2, bt, p, p, p, ctypes.c_double(1e-12),
+                                          ctypes.c_double(1e-12), 400, null, null, null, null) == N.EDGE_EINVAL
 
 
 def test_python_side_has_no_fallback(monkeypatch):

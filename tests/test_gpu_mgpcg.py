@@ -100,10 +100,15 @@ def test_poisson_vs_oracle(res, base_level, bt):
     assert abs(it - it_o) <= 1
     for i in range(3):
         assert rel_l2(N_(ug[i]), uo[i]) < 1e-4
-    # divergence left by the projection is the CG residual: below the
-    # absolute tolerance the reference uses (r.r < 1e-12 on the recursion)
-    d = div_of([N_(t).astype(np.float64) for t in ug])
-    assert np.sqrt((d ** 2).sum()) < 1e-3 * np.sqrt((div_of([a.astype(np.float64) for a in u]) ** 2).sum())
+    # the divergence left by the projection is the CG residual (stopped
+    # below the solver's tolerance on the recursion) plus one float32
+    # rounding of each stored face value
+    got = [N_(t).astype(np.float64) for t in ug]
+    d = np.sqrt((div_of(got) ** 2).sum())
+    a = [np.abs(t) for t in got]
+    floor = 2.0 ** -24 * np.sqrt(((a[0][1:] + a[0][:-1] + a[1][:, 1:] + a[1][:, :-1] + a[2][:, :, 1:]
+                                   + a[2][:, :, :-1]) ** 2).sum())
+    assert d <= np.sqrt(rtr) + 4 * floor, (d, rtr, floor)
 
 
 @pytest.mark.parametrize("res,base_level", [((128, 64, 64), 2), ((48, 24, 24), 1)])
@@ -216,22 +221,26 @@ def test_poisson_with_buffer():
         assert rel_l2(N_(u[i]), uo[i]) < 1e-4
 
 
-def test_mixed_precision_vs_fp64():
-    """BF16 V-cycle storage (precision=1): one V-cycle within bf16 rounding of
-    the float32 one, and solves to 1e-6 whose error against an FP64 solve is
-    of the float32 solver's size."""
+@pytest.mark.parametrize("precision,vtol", [(1, 3e-2), (2, 4e-3)])
+@pytest.mark.parametrize("amp", [1.0, 1e-7])
+def test_mixed_precision_vs_fp64(precision, vtol, amp):
+    """BF16 (precision=1) or FP16 (precision=2, scaled by a power of two)
+    V-cycle storage: one V-cycle within the storage format's rounding of the
+    float32 one, and solves to 1e-6 whose error against an FP64 solve is of
+    the float32 solver's size.  The tiny amplitude would underflow FP16
+    without the scaling."""
     from edgeb200.precision import fp64_solve, rel_error
     from edgeb200.projection import Projection
     res = (128, 64, 64)
     g = torch.Generator().manual_seed(21)
-    b = torch.randn(res, generator=g)
+    b = torch.randn(res, generator=g) * amp
     b = (b - b.mean()).cuda()
     P32 = Projection(res, base_level=1)
-    P16 = Projection(res, base_level=1, precision=1)
+    P16 = Projection(res, base_level=1, precision=precision)
     z32, z16 = torch.empty_like(b), torch.empty_like(b)
     P32.vcycle(b, z32)
     P16.vcycle(b, z16)
-    assert rel_l2(N_(z16), N_(z32)) < 3e-2
+    assert rel_l2(N_(z16), N_(z32)) < vtol
     ref = fp64_solve(P32, b)
     bb = float((b.double() ** 2).sum())
     errs, its = [], []
@@ -246,31 +255,116 @@ def test_mixed_precision_vs_fp64():
     assert errs[0] < 1e-3 and errs[1] < 3 * errs[0] + 1e-6, errs
 
 
-@pytest.mark.parametrize("res,base_level,solid", [((256, 128, 128), 2, False), ((128, 64, 64), 1, False),
-                                                  ((128, 64, 64), 1, True)])
-def test_cluster_vcycle_matches_per_level_kernels(res, base_level, solid, monkeypatch):
-    """The middle levels on one thread-block cluster (k_mid) run the same
-    arithmetic as the per-level kernels: solutions and iteration counts are
-    identical bit for bit."""
-    from edgeb200.projection import Projection
+def _coop_case(res, base_level, solid, precision, poisson):
     rng = np.random.default_rng(3)
-    b = rng.normal(size=res).astype(np.float32)
-    b -= b.mean()
     mask = bvel = None
     if solid:
         m = np.zeros(res, np.int32)
         m[res[0] // 3:res[0] // 3 + 6, res[1] // 3:2 * res[1] // 3, res[2] // 4:res[2] // 2] = 1
         mask, bvel = torch.from_numpy(m).cuda(), torch.zeros(res + (3,), device="cuda")
+        bvel[..., 0] = 0.25
+    if poisson:
+        u = [rng.normal(size=s).astype(np.float32) for s in O.face_shapes(res)]
+        return mask, bvel, u
+    b = rng.normal(size=res).astype(np.float32)
+    b -= b.mean()
+    return mask, bvel, b
+
+
+@pytest.mark.parametrize("res,base_level,solid,precision", [((256, 128, 128), 2, False, 0),
+                                                            ((128, 64, 64), 1, False, 0),
+                                                            ((128, 64, 64), 1, True, 0),
+                                                            ((64, 32, 32), 2, False, 1),
+                                                            ((128, 64, 64), 2, True, 1)])
+def test_cooperative_iteration_matches_per_level_kernels(res, base_level, solid, precision, monkeypatch):
+    """The cooperative iteration kernel (k_coarse + k_coop per CG iteration,
+    grid barriers between phases) runs the per-level kernels' arithmetic:
+    the projected velocity, the solution of a solve and the iteration counts
+    are identical bit for bit (the reductions' partials are summed in another
+    block order, in float64, and rounded to float32 before use)."""
+    from edgeb200.projection import Projection
+    mask, bvel, u = _coop_case(res, base_level, solid, precision, True)
+    _, _, b = _coop_case(res, base_level, solid, precision, False)
     out = []
     for flag in ("1", "0"):
-        monkeypatch.setenv("EDGE_MGPCG_CLUSTER", flag)
-        P = Projection(res, base_level=base_level, mask=mask, bvel=bvel)
+        monkeypatch.setenv("EDGE_MGPCG_COOP", flag)
+        P = Projection(res, base_level=base_level, mask=mask, bvel=bvel, precision=precision)
+        ug = [T_(a) for a in u]
+        P.poisson(*ug)
+        r1 = P.result()
         x = torch.zeros(res, device="cuda")
-        z = torch.empty(res, device="cuda")
-        P.vcycle(T_(b), z)
         P.solve(T_(b), x, abs_tol=0.0, rel_tol=1e-6)
-        out.append((N_(z), N_(x), P.result()))
+        out.append(([N_(t) for t in ug], N_(x), r1, P.result()))
         P.close()
-    np.testing.assert_array_equal(out[0][0], out[1][0])
+    assert out[0][2] == out[1][2] and out[0][3] == out[1][3]
+    assert out[0][2][2] == 0 and out[0][3][2] == 0
+    for a, c in zip(out[0][0], out[1][0]):
+        np.testing.assert_array_equal(a, c)
     np.testing.assert_array_equal(out[0][1], out[1][1])
-    assert out[0][2] == out[1][2]
+
+
+_EAGER_SCRIPT = r"""
+import sys
+import numpy as np, torch
+sys.path[:0] = [sys.argv[2], sys.argv[3]]
+from edgeb200.projection import Projection
+res = (128, 64, 64)
+rng = np.random.default_rng(3)
+u = [torch.from_numpy(rng.normal(size=s).astype(np.float32)).cuda()
+     for s in ((129, 64, 64), (128, 65, 64), (128, 64, 65))]
+P = Projection(res, base_level=2)
+P.poisson(*u)
+it, rtr, st = P.result()
+np.savez(sys.argv[1], ux=u[0].cpu().numpy(), uy=u[1].cpu().numpy(), uz=u[2].cpu().numpy(),
+         res=np.array([it, st]), rtr=np.array(rtr))
+"""
+
+
+def test_host_driven_loop_matches_graph(tmp_path):
+    """The host-driven CG loop (EDGE_MGPCG_EAGER=1: one status read per
+    iteration), on the cooperative and on the per-level path, gives the
+    graph-captured solve's result bit for bit.  The switch is read once per
+    process, so each runs in a child process."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pkg = os.path.join(root, "edge-flow-maps_b200")
+    outs = {}
+    for eager, coop in (("0", "1"), ("1", "1"), ("1", "0")):
+        path = str(tmp_path / f"e{eager}c{coop}.npz")
+        env = dict(os.environ, EDGE_MGPCG_EAGER=eager, EDGE_MGPCG_COOP=coop)
+        subprocess.run([sys.executable, "-c", _EAGER_SCRIPT, path, pkg, root], env=env, check=True, timeout=600)
+        outs[(eager, coop)] = np.load(path)
+    ref = outs[("0", "1")]
+    assert int(ref["res"][1]) == 0
+    for k, d in outs.items():
+        for f in ("ux", "uy", "uz", "res", "rtr"):
+            np.testing.assert_array_equal(d[f], ref[f], err_msg=f"{f} {k}")
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_refined_solve_reaches_true_tolerance(precision):
+    """Iterative refinement (float64 residual and iterate on the device,
+    float32/BF16/FP16 inner V-cycle-PCG solves) brings the TRUE relative
+    residual below 1e-6, where the float32 recursion alone stops above it,
+    and the result matches the FP64 solve."""
+    from edgeb200.precision import RefinedSolver, fp64_solve, rel_error
+    from edgeb200.projection import Projection
+    res = (128, 64, 64)
+    g = torch.Generator().manual_seed(5)
+    b = torch.randn(res, generator=g, dtype=torch.float64)
+    b = (b - b.mean()).cuda()
+    P = Projection(res, base_level=2, precision=precision)
+    R = RefinedSolver(P, inner_rel=1e-2)
+    x = R.solve(b, rel_tol=1e-6)
+    assert R.stats["true_rel_residual"] <= 1e-6, R.stats
+    assert 1 <= R.stats["outer"] <= 8, R.stats
+    # the float64 residual recomputed independently
+    Ax = torch.empty_like(x)
+    from edgeb200.precision import apply_A64
+    apply_A64(P, x, Ax)
+    true = float((b - Ax).norm() / b.norm())
+    assert true <= 1.01e-6, true
+    ref = fp64_solve(P, b.float())
+    assert rel_error(x.float(), ref) < 1e-4

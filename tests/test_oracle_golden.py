@@ -224,6 +224,14 @@ def test_init_rings():
         assert rel_l2(f[i], d["u_" + a]) < TOL
 
 
+def test_output_fields():
+    """get_central_vector and curl (taichi_utils.py:69-100), bit for bit."""
+    d = load_golden("output_fields")
+    vc = O.get_central_vector([d["u_x"], d["u_y"], d["u_z"]])
+    np.testing.assert_array_equal(vc, d["u_center"])
+    np.testing.assert_array_equal(O.curl(d["u_center"], float(d["meta_dx"])), d["curl"])
+
+
 def test_edge_steps():
     """Two full EDGE substeps of the driver loop (run_edge.py:588-712)."""
     d = load_golden("edge_steps")

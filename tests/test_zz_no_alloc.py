@@ -1,7 +1,13 @@
 """The allocation-free projection entry point (edge_mgpcg_poisson_noalloc),
 called through the C ABI, against the regular solver (edge_mgpcg_poisson) on
-the same input, twice in a row (the shared scratch keeps the previous call's
-contents, which must not leak into the next result).
+the same input.  Some callers cannot allocate device memory while they run
+(a host runtime that owns the whole device heap, an engine that forbids
+cudaMalloc after warm-up); this entry point serves them from static scratch.
+
+The calls come in a row on two shapes: the shared scratch keeps the previous
+call's contents, which must not leak into the next result, and the second
+shape (five levels down to an odd 3^3 grid, whose colour planes carry padding
+slots) places its levels at other offsets than the first.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test."""
@@ -24,20 +30,19 @@ def _rel(a, b):
     return float((a - b).norm() / b.norm().clamp_min(1e-30))
 
 
-def test_noalloc_matches_regular_solver_twice():
+@pytest.mark.parametrize("cases", [[((32, 32, 16), 2), ((32, 32, 16), 2), ((48, 48, 48), 1), ((32, 32, 16), 2)]])
+def test_noalloc_matches_regular_solver_in_a_row(cases):
     from edgeb200 import _native as N
     from edgeb200.projection import Projection
 
     lib = N.load()
     torch.cuda.set_device(0)
-    res = (32, 32, 16)
-    base_level = 2
     bt = (ctypes.c_int * 6)(2, 2, 2, 2, 2, 2)
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     rng = np.random.default_rng(123)
-    shapes = [(res[0] + 1, res[1], res[2]), (res[0], res[1] + 1, res[2]), (res[0], res[1], res[2] + 1)]
-    P = Projection(res, base_level=base_level)
-    for call in range(2):
+    for call, (res, base_level) in enumerate(cases):
+        shapes = [(res[0] + 1, res[1], res[2]), (res[0], res[1] + 1, res[2]), (res[0], res[1], res[2] + 1)]
+        P = Projection(res, base_level=base_level)
         u0 = [torch.from_numpy(rng.normal(size=s).astype(np.float32)).cuda() for s in shapes]
         ref = [t.clone() for t in u0]
         P.poisson(*ref)
@@ -52,17 +57,6 @@ def test_noalloc_matches_regular_solver_twice():
         torch.cuda.synchronize()
         assert rc == N.EDGE_OK
         assert st.value == N.EDGE_OK == st_ref
-        assert it.value == it_ref
+        assert it.value == it_ref, (call, res)
         for a, b in zip(got, ref):
-            assert _rel(a, b) < 1e-5, call
-
-
-def test_noalloc_rejects_grids_beyond_its_scratch():
-    from edgeb200 import _native as N
-    lib = N.load()
-    bt = (ctypes.c_int * 6)(2, 2, 2, 2, 2, 2)
-    p = ctypes.c_void_p(256)
-    null = ctypes.c_void_p(0)
-    rc = lib.edge_mgpcg_poisson_noalloc(128, 64, 64, 2, bt, p, p, p, ctypes.c_double(1e-12), ctypes.c_double(1e-12),
-                                        400, null, null, null, null)
-    assert rc == N.EDGE_EINVAL
+            assert _rel(a, b) < 1e-5, (call, res)
