@@ -314,60 +314,101 @@ PCG_REL = 1e-6
 PCG_TRAFFIC = 1379416320
 
 
-def pcg_measure(res, reps=5):
+def _event_ms(fn, reps):
     import torch
-    from edgeb200.projection import Projection
-    g = torch.Generator().manual_seed(1)
-    b = torch.randn(res, generator=g, dtype=torch.float64)
-    b -= b.mean()
-    bb = float((b * b).sum())
-    b = b.float().cuda()
-    x = torch.zeros(res, device="cuda")
-    P = Projection(res, base_level=BASE_LEVEL)
-    tol = PCG_REL * PCG_REL * bb
-    P.solve(b, x, abs_tol=tol, rel_tol=0.0)  # captures the solve graph
-    torch.cuda.synchronize()
     times = []
     for _ in range(reps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        P.solve(b, x, abs_tol=tol, rel_tol=0.0)
+        fn()
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    return statistics.median(times)
+
+
+def _solve_stats(res, b, bb, tol, precision, reps, ref):
+    """One Projection solving A x = b to r.r <= tol (graph-captured solve):
+    median CUDA-event time, iterations, the recursion's and the true relative
+    residual, and the error against the FP64 solve `ref`."""
+    import torch
+    from edgeb200.precision import rel_error
+    from edgeb200.projection import Projection
+    P = Projection(res, base_level=BASE_LEVEL, precision=precision)
+    x = torch.zeros(res, device="cuda")
+    P.solve(b, x, abs_tol=tol, rel_tol=0.0)  # captures the solve graph
+    torch.cuda.synchronize()
+    ms = _event_ms(lambda: P.solve(b, x, abs_tol=tol, rel_tol=0.0), reps)
     it, rtr, st = P.result()
     Ax = torch.empty_like(x)
     P.apply_A(x, Ax)
     true_rel = float((Ax.double() - b.double()).norm() / b.double().norm())
-    nc = res[0] * res[1] * res[2]
-    nbytes = 100 * nc + (it + 1) * 117 * nc  # set-up + one preconditioned CG iteration per iteration (+1: set-up V-cycle)
-    ms = statistics.median(times)
-    # errors against an FP64 solve of the same system, and the mixed-precision
-    # solver (BF16 V-cycle storage, FP32 residual, FP64 dots) on it
+    out = {"ms": ms, "iters": it, "status": st, "rel_residual": math.sqrt(rtr / bb), "true_rel_residual": true_rel,
+           "fp64_rel_error": rel_error(x, ref) if ref is not None else None}
+    return out, P
+
+
+def _refined_stats(P, b, reps, ref, inner_rel):
+    """Iterative refinement around P (float64 residual and iterate) to a
+    TRUE relative residual of 1e-6."""
+    from edgeb200.precision import RefinedSolver, rel_error
+    R = RefinedSolver(P, inner_rel=inner_rel)
+    b64 = b.double()
+    R.solve(b64, rel_tol=PCG_REL)
+    ms = _event_ms(lambda: R.solve(b64, rel_tol=PCG_REL), reps)
+    x = R.solve(b64, rel_tol=PCG_REL)
+    return {"ms": ms, "outer": R.stats["outer"], "inner_iters": R.stats["inner_iters"],
+            "true_rel_residual": R.stats["true_rel_residual"], "inner_rel": inner_rel,
+            "fp64_rel_error": rel_error(x.float(), ref) if ref is not None else None}
+
+
+def pcg_measure(res, reps=5, variants=True):
+    """Pressure solve to 1e-6 relative residual on a seeded N(0,1)
+    mean-removed right-hand side: the plain float32 solver (the roofline
+    line; cooperative iteration kernel, and the per-level kernels beside it),
+    the BF16 and FP16 mixed-precision solvers, and iterative refinement that
+    brings the TRUE residual to 1e-6 (float64 residual and iterate around
+    float32 or FP16 inner solves); errors against an FP64 solve."""
+    import torch
     from edgeb200.precision import fp64_solve, rel_error
+    g = torch.Generator().manual_seed(1)
+    b = torch.randn(res, generator=g, dtype=torch.float64)
+    b -= b.mean()
+    bb = float((b * b).sum())
+    b = b.float().cuda()
+    tol = PCG_REL * PCG_REL * bb
+    nc = res[0] * res[1] * res[2]
+    os.environ.pop("EDGE_MGPCG_COOP", None)
+    out, P = _solve_stats(res, b, bb, tol, 0, reps, None)
     ref = fp64_solve(P, b)
-    err32 = rel_error(x, ref)
-    P16 = Projection(res, base_level=BASE_LEVEL, precision=1)
-    x16 = torch.zeros(res, device="cuda")
-    P16.solve(b, x16, abs_tol=tol, rel_tol=0.0)
-    t16 = []
-    for _ in range(reps):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        P16.solve(b, x16, abs_tol=tol, rel_tol=0.0)
-        e1.record()
-        torch.cuda.synchronize()
-        t16.append(e0.elapsed_time(e1))
-    it16, rtr16, st16 = P16.result()
-    mixed = {"ms": statistics.median(t16), "iters": it16, "status": st16, "rel_residual": math.sqrt(rtr16 / bb),
-             "fp64_rel_error": rel_error(x16, ref), "speedup_vs_fp32": ms / statistics.median(t16)}
-    P16.close()
+    x = torch.zeros(res, device="cuda")
+    P.solve(b, x, abs_tol=tol, rel_tol=0.0)
+    out["fp64_rel_error"] = rel_error(x, ref)
+    it = out["iters"]
+    # set-up + one preconditioned iteration each (+1: the set-up V-cycle)
+    out["algorithmic_bytes"] = 100 * nc + (it + 1) * 117 * nc
+    out["res"] = list(res)
+    out["rhs"] = "N(0,1) seed 1, mean removed"
+    if not variants:
+        P.close()
+        return out
+    out["refined"] = {"fp32": _refined_stats(P, b, reps, ref, 1e-2)}
     P.close()
-    return {"ms": ms, "iters": it, "status": st, "rel_residual": math.sqrt(rtr / bb), "true_rel_residual": true_rel,
-            "fp64_rel_error": err32, "mixed": mixed,
-            "algorithmic_bytes": nbytes, "res": list(res), "rhs": "N(0,1) seed 1, mean removed"}
+    # the per-level kernels (no cooperative launch), same arithmetic
+    os.environ["EDGE_MGPCG_COOP"] = "0"
+    pl, Pp = _solve_stats(res, b, bb, tol, 0, reps, ref)
+    Pp.close()
+    os.environ.pop("EDGE_MGPCG_COOP", None)
+    out["per_level_kernels"] = {"ms": pl["ms"], "iters": pl["iters"]}
+    out["mixed"] = {}
+    for name, prec in (("bf16", 1), ("fp16", 2)):
+        m, Pm = _solve_stats(res, b, bb, tol, prec, reps, ref)
+        m["speedup_vs_fp32"] = out["ms"] / m["ms"]
+        m["refined"] = _refined_stats(Pm, b, reps, ref, 1e-2)
+        Pm.close()
+        out["mixed"][name] = m
+    return out
 
 
 # FLOPs per cell of the marches, counted from the reference's arithmetic
@@ -512,6 +553,103 @@ def c2_measure(steps=5, warm=3, per_cell=8):
     return out
 
 
+C4_RES = (512, 256, 256)
+
+
+def fp64_projection_error(P, u_pre, u_out):
+    """Relative L2 error over all faces of the projected velocity u_out
+    against the FP64 projection of the same pre-projection velocity u_pre
+    (MGPCG_3.Poisson's steps, mgpcg.py:440-445, in float64: walls zeroed,
+    divergence, A p = -div solved by float64 flexible CG, u - grad p)."""
+    from edgeb200.precision import fp64_solve
+    ux, uy, uz = (t.double().clone() for t in u_pre)
+    ux[0] = 0.0
+    ux[-1] = 0.0
+    uy[:, 0] = 0.0
+    uy[:, -1] = 0.0
+    uz[:, :, 0] = 0.0
+    uz[:, :, -1] = 0.0
+    div = (ux[1:] - ux[:-1]) + (uy[:, 1:] - uy[:, :-1]) + (uz[:, :, 1:] - uz[:, :, :-1])
+    p = fp64_solve(P, -div, rel_tol=1e-12)
+    del div
+    ux[1:-1] -= p[1:] - p[:-1]
+    uy[:, 1:-1] -= p[:, 1:] - p[:, :-1]
+    uz[:, :, 1:-1] -= p[:, :, 1:] - p[:, :, :-1]
+    num = sum(float(((o.double() - r) ** 2).sum()) for o, r in zip(u_out, (ux, uy, uz)))
+    den = sum(float((r ** 2).sum()) for r in (ux, uy, uz))
+    return math.sqrt(num / den)
+
+
+def c4_measure(steps=100, precision=2, warm=2):
+    """Configuration 4: 512x256x256, initial velocity = curl of a seeded
+    random vector potential (modes 1 <= |m| <= 8, amplitude |m|^(-17/6)),
+    EDGE with FP16 V-cycle storage and the float64 Jacobian composition.
+    Pass 1 times `steps` steps with CUDA events; pass 2 (untimed) repeats the
+    same deterministic steps from the same initial state and measures after
+    every step the error of its final projection against an FP64 projection
+    of the same velocity, and the step's MGPCG iterations."""
+    import torch
+    from edgeb200.sim import EdgeSim, random_potential_init
+    res = C4_RES
+    dx = 1.0 / res[1]
+
+    def fresh():
+        sim = EdgeSim(res, dx, variant="edge", cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * dx,
+                      base_level=BASE_LEVEL, bfecc_clamp=True, visualize_dt=1e9, packed=True, precision=precision)
+        sim.set_velocity(*random_potential_init(res, dx, seed=0))
+        sim.proj.poisson(*sim.u)  # run_edge.py:557
+        for _ in range(warm):
+            sim.step()
+        torch.cuda.synchronize()
+        return sim
+
+    torch.cuda.empty_cache()
+    torch.cuda.reset_peak_memory_stats()
+    sim = fresh()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sim.step()
+    e1.record()
+    torch.cuda.synchronize()
+    total_ms = e0.elapsed_time(e1)
+    peak = torch.cuda.max_memory_allocated()
+    levels = sim.proj.levels
+    del sim
+    torch.cuda.empty_cache()
+    sim = fresh()
+    rec = []
+    orig = sim.proj.poisson
+
+    def poisson(ux, uy, uz, **kw):
+        rec.append([t.clone() for t in (ux, uy, uz)])
+        orig(ux, uy, uz, **kw)
+    sim.proj.poisson = poisson
+    errs, iters = [], []
+    for _ in range(steps):
+        rec.clear()
+        sim.step()
+        iters.append(sim.proj.result()[0])
+        errs.append(fp64_projection_error(sim.proj, rec[-1], sim.u))
+    del sim, rec
+    torch.cuda.empty_cache()
+    return {"workload": f"curl of a seeded random vector potential (1 <= |m| <= 8, |m|^-17/6) 512x256x256, EDGE, "
+                        f"{'FP16' if precision == 2 else 'BF16'} V-cycle storage, float64 Jacobian composition, "
+                        f"reinit 12, {levels}-level MGPCG",
+            "steps": steps, "ms_per_step": total_ms / steps, "steps_per_s": 1e3 * steps / total_ms,
+            "peak_device_bytes": int(peak), "second_projection_iters": iters,
+            "fp64_projection_rel_error": [float(f"{e:.4g}") for e in errs],
+            "fp64_projection_rel_error_max": max(errs)}
+
+
+def run_c4_only(args):
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps({"c4_mixed": c4_measure(steps=args.c4_steps)}), flush=True)
+    return 0
+
+
 def run_pcg_only(args):
     import torch
     torch.cuda.set_device(0)
@@ -628,6 +766,10 @@ def run_ours(args, rank, world, local_rank):
     pcg = pcg_measure(RES) if not (args.res or args.no_extras) else None
     if pcg is not None:
         pcg["learned"] = learned_measure(RES)
+        # the same solves at 512x256x256, where the level arrays no longer fit
+        # in L2 and 16-bit storage halves their traffic
+        pcg["at_512x256x256"] = pcg_measure(C4_RES, reps=3)
+    c4 = c4_measure(steps=args.c4_steps) if not (args.res or args.no_extras) else None
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -666,6 +808,7 @@ def run_ours(args, rank, world, local_rank):
             "pcg": pcg,
             "variants": variants or None,
             "c2_solid_particles": c2,
+            "c4_mixed": c4,
             "mgpcg_iters": list(iters),
             "clocks": clk.summary(),
             "gpu_launches": launches,
@@ -695,6 +838,8 @@ def main():
     ap.add_argument("--pcg-only", action="store_true", help="only the PCG-to-1e-6 measurement (profiling)")
     ap.add_argument("--learned-only", action="store_true", help="only the learned-preconditioner measurement")
     ap.add_argument("--c2-only", action="store_true", help="only the solid + particle configuration")
+    ap.add_argument("--c4-only", action="store_true", help="only the 512x256x256 mixed-precision configuration")
+    ap.add_argument("--c4-steps", type=int, default=100)
     ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8/GE/EFM step timings")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the EDGE steps (no ED4/ED8, PCG or FP32-peak measurements; profiling)")
@@ -715,6 +860,8 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps({"c2_solid_particles": c2_measure()}), flush=True)
         return 0
+    if args.c4_only:
+        return run_c4_only(args)
     return run_ours(args, rank, world, local_rank)
 
 
