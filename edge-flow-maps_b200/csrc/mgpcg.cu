@@ -2024,6 +2024,12 @@ __global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f,
     G gq = g;
     gq.use_cond = 0;  // the loop condition is set once, below
     if (mode == COOP_ITER) {
+        // a launch after the loop ended (the stepwise solve) does nothing; no
+        // block writes the status before the first barrier of this launch
+        if (st_ldi(&st->status) != ST_RUNNING) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
+            return;
+        }
         // up sweeps of the V-cycle whose coarse group k_coarse just ran
         for (int l = lc - 1; l >= 0; l--) {
             const Lvl& L = sl[l];
@@ -2189,14 +2195,17 @@ __global__ void k_from_rb(SolveState* st, Lvl L, const float* p0, const float* p
     }
 }
 
-__global__ void k_to_rb(Lvl L, const float* src, float* p0, float* p1) {
+__global__ void k_to_rb(Lvl L, const float* src, float* p0, float* p1, int ztype) {
     GRID_STRIDE(t, L.n0 * L.n1 * L.n2) {
         int row = fdiv(t, L.d2);
         int k = t - row * L.n2;
         int i = fdiv(row, L.d1);
         int j = row - i * L.n1;
         float* p = ((i + j + k) & 1) ? p1 : p0;
-        p[row * L.H + (k >> 1)] = src[t];
+        const int e = row * L.H + (k >> 1);
+        if (ztype == 1) Zs<__nv_bfloat16>::st(p, e, src[t]);
+        else if (ztype == 2) Zs<__half>::st(p, e, src[t]);
+        else p[e] = src[t];
     }
 }
 
@@ -2964,6 +2973,17 @@ int edge_mgpcg_result(void* handle, int* iters, double* rTr, int* status, void* 
     return EDGE_OK;
 }
 
+int edge_mgpcg_progress(void* handle, int* iters, double* rTr, int* running, void* stream) {
+    if (!handle) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    CK(cudaMemcpyAsync(s->st_host, s->ctx.g.st, sizeof(SolveState), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaStreamSynchronize((cudaStream_t)stream));
+    if (iters) *iters = s->st_host->it;
+    if (rTr) *rTr = s->st_host->rTr;
+    if (running) *running = s->st_host->status == ST_RUNNING;
+    return EDGE_OK;
+}
+
 int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
     if (!handle || !r || !z) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
@@ -2994,7 +3014,7 @@ int edge_mgpcg_vcycle(void* handle, const float* r, float* z, void* stream) {
             k_codes<<<rgrid((long long)V.n0 * V.n1 * V.n2), 256, 0, st>>>(c.g, V);
         }
     }
-    k_to_rb<<<rgrid(n), 256, 0, st>>>(L0, r, L0.r[0], L0.r[1]);
+    k_to_rb<<<rgrid(n), 256, 0, st>>>(L0, r, L0.r[0], L0.r[1], 0);
     if (c.ztype == 2) k_zscale<<<rgrid(L0.P), 256, 0, st>>>(c.g, L0);  // the input's scale
     // outside a graph there is no loop condition to set
     c.g.use_cond = 0;
@@ -3008,6 +3028,100 @@ int edge_mgpcg_apply_A_f64(void* handle, const double* p, double* Ap, void* stre
     Solver* s = (Solver*)handle;
     const Lvl& L = s->ctx.lv.lv[0];
     k_apply_A64<<<grid_for((long long)L.n0 * L.n1 * L.n2), 256, 0, (cudaStream_t)stream>>>(s->ctx.g, L, p, Ap);
+    return cu(cudaPeekAtLastError());
+}
+
+// ---- stepwise solve with a replaceable coarse solver -------------------------
+int edge_mgpcg_coarse_shape(void* handle, int* level, int* dims) {
+    if (!handle || !level || !dims) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Levels& V = s->ctx.lv;
+    *level = V.lc;
+    dims[0] = V.lv[V.lc].n0;
+    dims[1] = V.lv[V.lc].n1;
+    dims[2] = V.lv[V.lc].n2;
+    return s->ctx.coop ? EDGE_OK : EDGE_ESTATE;
+}
+
+int edge_mgpcg_coarse_get_r(void* handle, float* dense, void* stream) {
+    if (!handle || !dense) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& C = s->ctx.lv.lv[s->ctx.lv.lc];
+    const long long n = (long long)C.n0 * C.n1 * C.n2;
+    k_from_rb<<<rgrid(n), 256, 0, (cudaStream_t)stream>>>(nullptr, C, C.r[0], C.r[1], dense, nullptr, s->ctx.ztype,
+                                                         nullptr);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_coarse_set_z(void* handle, const float* dense, void* stream) {
+    if (!handle || !dense) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    const Lvl& C = s->ctx.lv.lv[s->ctx.lv.lc];
+    const long long n = (long long)C.n0 * C.n1 * C.n2;
+    k_to_rb<<<rgrid(n), 256, 0, (cudaStream_t)stream>>>(C, dense, C.z[0], C.z[1], s->ctx.ztype);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_coarse_default(void* handle, void* stream) {
+    if (!handle) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    if (!s->ctx.coop) return EDGE_ESTATE;
+    Ctx c = s->ctx;
+    c.g.use_cond = 0;
+    const int t = c.ztype;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (t == 1) {
+        if (s->solid) launch_pdl(k_coarse<false, true, __nv_bfloat16>, 1, 1024, c.csmem, st, c.g, c.lv);
+        else launch_pdl(k_coarse<false, false, __nv_bfloat16>, 1, 1024, c.csmem, st, c.g, c.lv);
+    } else if (t == 2) {
+        if (s->solid) launch_pdl(k_coarse<false, true, __half>, 1, 1024, c.csmem, st, c.g, c.lv);
+        else launch_pdl(k_coarse<false, false, __half>, 1, 1024, c.csmem, st, c.g, c.lv);
+    } else {
+        if (s->solid) launch_pdl(k_coarse<false, true, float>, 1, 1024, c.csmem, st, c.g, c.lv);
+        else launch_pdl(k_coarse<false, false, float>, 1, 1024, c.csmem, st, c.g, c.lv);
+    }
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_solve_begin(void* handle, const float* b, double abs_tol, double rel_tol, int max_iters,
+                           void* stream) {
+    if (!handle || !b) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    if (!s->ctx.coop) return EDGE_ESTATE;
+    if (max_iters < 0) max_iters = s->solid ? 100 : 400;
+    Faces U = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    s->ctx.g.use_cond = 0;
+    s->ctx.g.use_vcond = 0;
+    enqueue_setup(s, U, b, abs_tol, rel_tol, max_iters, (cudaStream_t)stream);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_solve_iter(void* handle, void* stream) {
+    if (!handle) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    if (!s->ctx.coop) return EDGE_ESTATE;
+    Ctx c = s->ctx;
+    c.g.use_cond = 0;
+    const int t = c.ztype;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (t == 1) {
+        if (s->solid) launch_coop<true, __nv_bfloat16>(c, st, COOP_ITER);
+        else launch_coop<false, __nv_bfloat16>(c, st, COOP_ITER);
+    } else if (t == 2) {
+        if (s->solid) launch_coop<true, __half>(c, st, COOP_ITER);
+        else launch_coop<false, __half>(c, st, COOP_ITER);
+    } else {
+        if (s->solid) launch_coop<true, float>(c, st, COOP_ITER);
+        else launch_coop<false, float>(c, st, COOP_ITER);
+    }
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_solve_end(void* handle, const float* b, float* x, void* stream) {
+    if (!handle || !b || !x) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    Faces U = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    enqueue_finish(s, U, b, x, (cudaStream_t)stream);
     return cu(cudaPeekAtLastError());
 }
 

@@ -79,11 +79,48 @@ class Projection:
         N.call("edge_mgpcg_result", self._h, ctypes.byref(it), ctypes.byref(rtr), ctypes.byref(st), stream())
         return it.value, rtr.value, st.value
 
+    def progress(self):
+        """(iterations, r.r, whether the CG loop is still running);
+        synchronises the stream."""
+        it = ctypes.c_int()
+        rtr = ctypes.c_double()
+        run = ctypes.c_int()
+        N.call("edge_mgpcg_progress", self._h, ctypes.byref(it), ctypes.byref(rtr), ctypes.byref(run), stream())
+        return it.value, rtr.value, bool(run.value)
+
     def kernel_count(self):
         """Kernels this solver has run (counted on the device; synchronises)."""
         c = ctypes.c_longlong()
         N.call("edge_mgpcg_kernel_count", self._h, ctypes.byref(c), stream())
         return c.value
+
+    # -- stepwise solve with a replaceable coarse solver --------------------------
+    def coarse_shape(self):
+        """(level, (n0, n1, n2)) of the level whose residual equation the
+        coarse group solves; raises on the per-level kernel path."""
+        lvl = ctypes.c_int()
+        dims = (ctypes.c_int * 3)()
+        N.call("edge_mgpcg_coarse_shape", self._h, ctypes.byref(lvl), dims)
+        return lvl.value, tuple(int(v) for v in dims)
+
+    def solve_begin(self, b, abs_tol=1e-12, rel_tol=1e-12, max_iters=-1):
+        N.call("edge_mgpcg_solve_begin", self._h, ptr(b, "b"), ctypes.c_double(abs_tol), ctypes.c_double(rel_tol),
+               int(max_iters), stream())
+
+    def coarse_get_r(self, dense):
+        N.call("edge_mgpcg_coarse_get_r", self._h, ptr(dense), stream())
+
+    def coarse_set_z(self, dense):
+        N.call("edge_mgpcg_coarse_set_z", self._h, ptr(dense), stream())
+
+    def coarse_default(self):
+        N.call("edge_mgpcg_coarse_default", self._h, stream())
+
+    def solve_iter(self):
+        N.call("edge_mgpcg_solve_iter", self._h, stream())
+
+    def solve_end(self, b, x):
+        N.call("edge_mgpcg_solve_end", self._h, ptr(b, "b"), ptr(x, "x"), stream())
 
     def vcycle(self, r, z):
         N.call("edge_mgpcg_vcycle", self._h, ptr(r), ptr(z), stream())

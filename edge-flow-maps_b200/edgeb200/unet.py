@@ -408,3 +408,83 @@ def mgpcg_pairs(sim, steps, every=1):
             x = sim.proj.get("p")
             out.append(((-div).contiguous(), x.contiguous()))
     return out
+
+
+# ---- learned coarse-grid solver inside MGPCG -----------------------------------
+class LearnedCoarsePCG:
+    """MGPCG whose coarse group is the U-Net.  The V-cycle's coarsest levels
+    (lc..L-1, which the solver otherwise runs in one shared-memory block) solve
+    the level-lc residual equation A_lc z = r_lc approximately; here the
+    network, trained on exact solutions of that equation, supplies z_lc, and
+    everything else (the finer levels' sweeps, restrictions and
+    prolongations, the CG updates with their device-side scalars) is the
+    plain solver's cooperative iteration kernel.  The network works at the
+    coarse level's size (32x16x16 for the 128x64x64 and 256x128x128 grids),
+    a few hundred times fewer voxels than the fine grid.
+
+    Fallback: when an iteration reduces |r| by less than `stall`, the rest of
+    the solve takes the built-in coarse group (plain MGPCG).  One iteration
+    (coarse step + CG iteration) is a CUDA graph replayed per iteration; the
+    host reads the status (and r.r for the stall test) between iterations."""
+
+    def __init__(self, proj, params, stall=0.5, graphs=True):
+        self.P = proj
+        self.level, self.dims = proj.coarse_shape()
+        self.net = UNet(self.dims, params=params)
+        self.r = torch.zeros(self.dims, device="cuda")
+        self.z = torch.zeros(self.dims, device="cuda")
+        self.stall = float(stall)
+        self.graphs = {}
+        self.use_graphs = bool(graphs)
+
+    def _step(self, mode):
+        if mode == "net":
+            self.P.coarse_get_r(self.r)
+            self.net.forward(self.r, self.z)
+            self.P.coarse_set_z(self.z)
+        else:
+            self.P.coarse_default()
+        self.P.solve_iter()
+
+    def _run(self, mode):
+        if not self.use_graphs:
+            self._step(mode)
+            return
+        g = self.graphs.get(mode)
+        if g is None:
+            # capture after the buffers exist; a launch that cannot be captured
+            # leaves the eager path in place
+            try:
+                g = torch.cuda.CUDAGraph()
+                s = torch.cuda.Stream()
+                s.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(s):
+                    g.capture_begin()
+                    self._step(mode)
+                    g.capture_end()
+                torch.cuda.current_stream().wait_stream(s)
+                self.graphs[mode] = g
+            except RuntimeError:
+                self.use_graphs = False
+                self._step(mode)
+                return
+        g.replay()
+
+    def solve(self, b, x, abs_tol=1e-12, rel_tol=1e-12, max_iters=400, mode="net"):
+        """x solves A x = b (the solver's tolerance semantics, mgpcg.py:224).
+        Returns (iterations, r.r, status, fell_back)."""
+        P = self.P
+        P.solve_begin(b, abs_tol=abs_tol, rel_tol=rel_tol, max_iters=max_iters)
+        fell_back = False
+        prev = None
+        while True:
+            self._run(mode)
+            it, rtr, running = P.progress()
+            if not running:
+                break
+            if mode == "net" and prev is not None and rtr > self.stall * self.stall * prev:
+                mode, fell_back = "vcycle", True
+            prev = rtr
+        P.solve_end(b, x)
+        it, rtr, st = P.result()
+        return it, rtr, st, fell_back

@@ -269,6 +269,33 @@ int edge_mgpcg_apply_A(void *handle, const float *p, float *Ap, void *stream);
 /* The same operator in float64 (no reference counterpart): the FP64
  * reference solve that the precision study measures errors against. */
 int edge_mgpcg_apply_A_f64(void *handle, const double *p, double *Ap, void *stream);
+/* Stepwise solve with a replaceable coarse solver (no reference counterpart;
+ * the learned preconditioner's path).  The V-cycle's levels lc..L-1 normally
+ * run in one shared-memory block (the coarse group); these calls let the
+ * caller replace that group by its own solver of the level-lc residual
+ * equation.  Available on the cooperative path only (EDGE_ESTATE otherwise).
+ *   coarse_shape: lc and its cell dims (int[3]);
+ *   solve_begin:  set-up of solve(b) up to the first V-cycle's coarse level;
+ *   coarse_get_r: the level-lc residual as a float32 cell array;
+ *   coarse_set_z: the level-lc correction from a float32 cell array, or
+ *   coarse_default: the built-in coarse group;
+ *   solve_iter:   the rest of that V-cycle, one CG iteration and the next
+ *                 V-cycle's descent (nothing once the solve has ended);
+ *   solve_end:    the solution into x.
+ * edge_mgpcg_result reports the status between iterations.  One coarse step
+ * per solve_iter, starting after solve_begin: the V-cycles and CG updates are
+ * those of edge_mgpcg_solve. */
+int edge_mgpcg_coarse_shape(void *handle, int *level, int *dims);
+int edge_mgpcg_solve_begin(void *handle, const float *b, double abs_tol, double rel_tol, int max_iters,
+                           void *stream);
+int edge_mgpcg_coarse_get_r(void *handle, float *dense, void *stream);
+int edge_mgpcg_coarse_set_z(void *handle, const float *dense, void *stream);
+int edge_mgpcg_coarse_default(void *handle, void *stream);
+int edge_mgpcg_solve_iter(void *handle, void *stream);
+int edge_mgpcg_solve_end(void *handle, const float *b, float *x, void *stream);
+/* Iterations, r.r and whether the CG loop still runs (1) or has ended (0);
+ * synchronises the stream. */
+int edge_mgpcg_progress(void *handle, int *iters, double *rTr, int *running, void *stream);
 /* Iterative refinement of a mixed-precision solve (no reference counterpart):
  * r = b - A x with b, x (device float64, cell layout) and the arithmetic in
  * float64, r written as float32 (the right-hand side of the next inner solve),

@@ -244,3 +244,58 @@ def test_conv_kernel_choices_bit_identical(tmp_path):
     for mode in ("1", "3"):
         for k in outs["0"].files:
             np.testing.assert_array_equal(outs[mode][k], outs["0"][k], err_msg=f"{k} (EDGE_CONV_STAGED={mode})")
+
+
+@pytest.mark.parametrize("precision", [0, 2])
+def test_stepwise_solve_matches_graph_solve(precision):
+    """The stepwise solve with the built-in coarse group (the learned
+    solver's frame: set-up, then per iteration a coarse step and the
+    cooperative iteration kernel) gives the graph-captured solve's result
+    and iteration count bit for bit; the level-lc residual round-trips
+    through the cell-array I/O."""
+    from edgeb200.projection import Projection
+    from edgeb200.unet import LearnedCoarsePCG
+    res = (128, 64, 64)
+    g = torch.Generator().manual_seed(8)
+    b = torch.randn(res, generator=g)
+    b = (b - b.mean()).cuda()
+    bb = float((b.double() ** 2).sum())
+    P = Projection(res, base_level=2, precision=precision)
+    x0 = torch.zeros(res, device="cuda")
+    P.solve(b, x0, abs_tol=1e-12 * bb, rel_tol=0.0)
+    ref = P.result()
+    L = LearnedCoarsePCG(P, None)
+    assert L.dims == (32, 16, 16)
+    x1 = torch.zeros(res, device="cuda")
+    it, rtr, st, fell = L.solve(b, x1, abs_tol=1e-12 * bb, rel_tol=0.0, mode="vcycle")
+    assert (it, st) == (ref[0], ref[2]) and rtr == ref[1] and not fell
+    assert torch.equal(x0, x1)
+    # level-lc residual: cell array -> planes -> cell array is exact in float32
+    P.solve_begin(b, abs_tol=1e-12 * bb, rel_tol=0.0)
+    r = torch.empty(L.dims, device="cuda")
+    P.coarse_get_r(r)
+    P.coarse_set_z(r)
+    P.coarse_default()
+    torch.cuda.synchronize()
+    assert float(r.abs().max()) > 0
+
+
+def test_learned_coarse_solver_converges_with_fallback():
+    """With untrained weights the network is a poor coarse solver: the solve
+    still reaches the tolerance (the stall test hands it to the built-in
+    coarse group when needed) and reports the status of the plain solver."""
+    from edgeb200.projection import Projection
+    from edgeb200.unet import LearnedCoarsePCG, init_params
+    res = (128, 64, 64)
+    g = torch.Generator().manual_seed(9)
+    b = torch.randn(res, generator=g)
+    b = (b - b.mean()).cuda()
+    bb = float((b.double() ** 2).sum())
+    P = Projection(res, base_level=2)
+    L = LearnedCoarsePCG(P, init_params(3))
+    x = torch.zeros(res, device="cuda")
+    it, rtr, st, fell = L.solve(b, x, abs_tol=1e-12 * bb, rel_tol=0.0, mode="net")
+    assert st == 0 and rtr < 1e-12 * bb
+    Ax = torch.empty_like(x)
+    P.apply_A(x, Ax)
+    assert float((Ax - b).norm() / b.norm()) < 1e-5
