@@ -1733,6 +1733,7 @@ EDGE_D bool coop_sync(SolveState* st, CoopBar& b) {
         __threadfence();
         bool ok = true;
         if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+            __threadfence();  // acquire: the other blocks' writes before their arrivals
             atomicExch(&st->bar_count, 0u);  // no block arrives again before the release below
             st_release_u32(&st->bar_gen, target);
         } else {
@@ -1791,10 +1792,29 @@ EDGE_D bool coop_reduce(const G& g, CoopBar& b, double (&v)[N], EPI epi) {
 EDGE_D float st_ldf(const float* p) { return *((const volatile float*)p); }
 EDGE_D int st_ldi(const int* p) { return *((const volatile int*)p); }
 
+// Weak loads of data written earlier in the same launch (plain ld.global,
+// L1-cached): correct after the grid barrier, whose acquire and block
+// barrier order them after the other blocks' released writes.
+template <class ZT>
+struct Zw;
+template <>
+struct Zw<float> {
+    static EDGE_D float ld(const float* b, int e) { return b[e]; }
+    static EDGE_D float2 ld2(const float* b, int e) { return *reinterpret_cast<const float2*>(b + e); }
+    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
+        float4 t = *reinterpret_cast<const float4*>(b + e);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+};
+template <>
+struct Zw<__nv_bfloat16> : Zs<__nv_bfloat16> {};
+template <>
+struct Zw<__half> : Zs<__half> {};
+
 // one half sweep of colour `color` on a four-slot level (k_hsweep4's
 // arithmetic), slots t0, t0 + stride, ...; HS_ZR adds z.r over both colours
 // to zr
-template <int MODE, bool SOLID, class ZT>
+template <template <class> class LD, int MODE, bool SOLID, class ZT>
 EDGE_D void co_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int level0, float mean, float zsc, int t0,
                      int stride, double& zr) {
     const int oc = color ^ 1;
@@ -1808,19 +1828,22 @@ EDGE_D void co_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int leve
         unsigned code[4];
         quad_codes<SOLID>(L, color, q, p, code);
         float rv[4], ns[4] = {0.0f, 0.0f, 0.0f, 0.0f}, zn[4];
-        if (level0) Zc<float>::ld4(rs, q.t0, rv);
-        else Zc<ZT>::ld4(rs, q.t0, rv);
+        if (level0) LD<float>::ld4(rs, q.t0, rv);
+        else LD<ZT>::ld4(rs, q.t0, rv);
         if (MODE != HS_FIRST) {
-            auto v4 = [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); };
-            auto v1 = [&](int e) { return Zc<ZT>::ld(zo, e); };
+            auto v4 = [&](int e, float(&o)[4]) { LD<ZT>::ld4(zo, e, o); };
+            auto v1 = [&](int e) { return LD<ZT>::ld(zo, e); };
             if (MODE == HS_PROLONG && L.n2 % 8 == 0) {
                 QParents P;
-                quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return Zc<ZT>::ld2(pick(C.z, pl), e); },
-                             [&](int pl, int e) { return Zc<ZT>::ld(pick(C.z, pl), e); }, P);
+                quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return LD<ZT>::ld2(pick(C.z, pl), e); },
+                             [&](int pl, int e) { return LD<ZT>::ld(pick(C.z, pl), e); }, P);
                 quad_nbr_sum_pro(L, q, p, code, v4, v1, P, ns);
             } else if (MODE == HS_PROLONG)
                 quad_nbr_sum<true>(L, q, p, code, v4, v1,
-                                   [&](int i, int j, int k) { return parent_zc<ZT>(C, i, j, k); }, ns);
+                                   [&](int i, int j, int k) {
+                                       const int I = i >> 1, J = j >> 1, K = k >> 1;
+                                       return LD<ZT>::ld(pick(C.z, (I + J + K) & 1), (I * C.n1 + J) * C.H + (K >> 1));
+                                   }, ns);
             else
                 quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
         }
@@ -1837,9 +1860,9 @@ EDGE_D void co_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int leve
             unsigned co[4];
             quad_codes<SOLID>(L, oc, q, p ^ 1, co);
             float ro[4], zz[4];
-            if (level0) Zc<float>::ld4(pick(L.r, oc), q.t0, ro);
-            else Zc<ZT>::ld4(pick(L.r, oc), q.t0, ro);
-            Zc<ZT>::ld4(zo, q.t0, zz);
+            if (level0) LD<float>::ld4(pick(L.r, oc), q.t0, ro);
+            else LD<ZT>::ld4(pick(L.r, oc), q.t0, ro);
+            LD<ZT>::ld4(zo, q.t0, zz);
 #pragma unroll
             for (int m = 0; m < 4; m++)
                 if (co[m] & CELL_FLUID) zr += (double)zz[m] * (double)((ro[m] - mean) * zsc);
@@ -1848,7 +1871,7 @@ EDGE_D void co_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int leve
 }
 
 // k_restrict4's arithmetic on slots t0, t0 + stride, ...
-template <bool SOLID, class ZT>
+template <template <class> class LD, bool SOLID, class ZT>
 EDGE_D void co_restrict(const G& g, const Lvl& F, const Lvl& C, int level0, float mean, float zsc, bool first,
                         int t0, int stride) {
     const int nq = F.H >> 2;
@@ -1873,11 +1896,11 @@ EDGE_D void co_restrict(const G& g, const Lvl& F, const Lvl& C, int level0, floa
                     const float* zo = pick(F.z, pl ^ 1);
                     float ns[4], zc[4], rc[4];
                     quad_nbr_sum<false>(
-                        F, q, h, code, [&](int e, float(&o)[4]) { Zc<ZT>::ld4(zo, e, o); },
-                        [&](int e) { return Zc<ZT>::ld(zo, e); }, NoParent(), ns);
-                    Zc<ZT>::ld4(pick(F.z, pl), q.t0, zc);
-                    if (level0) Zc<float>::ld4(pick(F.r, pl), q.t0, rc);
-                    else Zc<ZT>::ld4(pick(F.r, pl), q.t0, rc);
+                        F, q, h, code, [&](int e, float(&o)[4]) { LD<ZT>::ld4(zo, e, o); },
+                        [&](int e) { return LD<ZT>::ld(zo, e); }, NoParent(), ns);
+                    LD<ZT>::ld4(pick(F.z, pl), q.t0, zc);
+                    if (level0) LD<float>::ld4(pick(F.r, pl), q.t0, rc);
+                    else LD<ZT>::ld4(pick(F.r, pl), q.t0, rc);
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         if (!(code[m] & CELL_FLUID)) continue;
@@ -1907,7 +1930,7 @@ EDGE_D void co_restrict(const G& g, const Lvl& F, const Lvl& C, int level0, floa
 }
 
 // k_cg_ap4's arithmetic (p = z + beta p, A p, p.Ap) on slots t0, t0 + stride, ...
-template <bool SOLID, class ZT>
+template <template <class> class LD, bool SOLID, class ZT>
 EDGE_D void co_ap(const G& g, const Lvl& L, const Fine& f, int pc, bool first, float beta, float zinv, int t0,
                   int stride, double& pap) {
     const int nq = L.n0 * L.n1 * (L.H >> 2);
@@ -1922,12 +1945,12 @@ EDGE_D void co_ap(const G& g, const Lvl& L, const Fine& f, int pc, bool first, f
             const float* zo = pick(L.z, pl ^ 1);
             const float* po = pick2(f.p, pc, pl ^ 1);
             auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
-                Zc<ZT>::ld4(zz, e, o);
+                LD<ZT>::ld4(zz, e, o);
 #pragma unroll
                 for (int m = 0; m < 4; m++) o[m] = o[m] * zinv;
                 if (!first) {
                     float b[4];
-                    Zc<float>::ld4(pp, e, b);
+                    LD<float>::ld4(pp, e, b);
 #pragma unroll
                     for (int m = 0; m < 4; m++) o[m] = __fadd_rn(o[m], __fmul_rn(beta, b[m]));
                 }
@@ -1937,8 +1960,8 @@ EDGE_D void co_ap(const G& g, const Lvl& L, const Fine& f, int pc, bool first, f
             quad_nbr_sum<false>(
                 L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
                 [&](int e) {
-                    const float ze = Zc<ZT>::ld(zo, e) * zinv;
-                    return first ? ze : __fadd_rn(ze, __fmul_rn(beta, __ldcg(po + e)));
+                    const float ze = LD<ZT>::ld(zo, e) * zinv;
+                    return first ? ze : __fadd_rn(ze, __fmul_rn(beta, LD<float>::ld(po, e)));
                 },
                 NoParent(), ns);
 #pragma unroll
@@ -1957,7 +1980,7 @@ EDGE_D void co_ap(const G& g, const Lvl& L, const Fine& f, int pc, bool first, f
 }
 
 // k_cg_xr4's arithmetic (x += alpha p, r -= alpha A p, r.r, sum r)
-template <bool SOLID>
+template <template <class> class LD, bool SOLID>
 EDGE_D void co_xr(const G& g, const Lvl& L, const Fine& f, int pc, bool first, float alpha, float mean, int t0,
                   int stride, double (&v)[2]) {
     const int nq = L.n0 * L.n1 * (L.H >> 2);
@@ -1971,12 +1994,12 @@ EDGE_D void co_xr(const G& g, const Lvl& L, const Fine& f, int pc, bool first, f
             quad_codes<SOLID>(L, pl, q, h, code);
             const float* po = pick2(f.p, pc, pl ^ 1);
             float pe[4], ns[4], r[4], x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            Zc<float>::ld4(pick2(f.p, pc, pl), q.t0, pe);
+            LD<float>::ld4(pick2(f.p, pc, pl), q.t0, pe);
             ld4c(pick(L.r, pl) + q.t0, r);
             if (!first) ld4c(pick(f.x, pl) + q.t0, x);
             quad_nbr_sum<false>(
-                L, q, h, code, [&](int e, float(&o)[4]) { Zc<float>::ld4(po, e, o); },
-                [&](int e) { return __ldcg(po + e); }, NoParent(), ns);
+                L, q, h, code, [&](int e, float(&o)[4]) { LD<float>::ld4(po, e, o); },
+                [&](int e) { return LD<float>::ld(po, e); }, NoParent(), ns);
 #pragma unroll
             for (int m = 0; m < 4; m++) {
                 r[m] = r[m] - mean;
@@ -2006,8 +2029,21 @@ constexpr int kCoopThreads = 256;
         }                                                \
     } while (0)
 
-template <bool SOLID, class ZT>
-__global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f, int mode) {
+// the phases' load policy: through L2 (Zc), or weak L1-cached loads (Zw)
+template <bool WEAK>
+struct LdSel {
+    template <class T>
+    using type = Zc<T>;
+};
+template <>
+struct LdSel<true> {
+    template <class T>
+    using type = Zw<T>;
+};
+#define LDT LdSel<WEAK>::template type
+
+template <bool SOLID, class ZT, bool WEAK>
+__global__ void __launch_bounds__(kCoopThreads, WEAK ? 4 : 3) k_coop(G g, Levels a, Fine f, int mode) {
     __shared__ Lvl sl[16];
     __shared__ CoopBar bar;
     count_launch(g.st);
@@ -2037,17 +2073,17 @@ __global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f,
             const int l0 = l == 0;
             const float mean = l0 ? st_ldf(&st->mean) : 0.0f, zsc = l0 ? st_ldf(&st->zsc) : 1.0f;
             double zr = 0.0;
-            co_sweep<HS_PROLONG, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+            co_sweep<LDT, HS_PROLONG, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
             COOP_SYNC(coop_sync(st, bar));
-            co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+            co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
             COOP_SYNC(coop_sync(st, bar));
-            co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+            co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
             COOP_SYNC(coop_sync(st, bar));
             if (l > 0) {
-                co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+                co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
                 COOP_SYNC(coop_sync(st, bar));
             } else {
-                co_sweep<HS_ZR, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+                co_sweep<LDT, HS_ZR, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
                 double v[1] = {zr};
                 COOP_SYNC(coop_reduce<1>(g, bar, v, [&](double (&w)[1]) {
                     zr_epilogue(gq, w[0]);
@@ -2065,7 +2101,7 @@ __global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f,
             const bool first = st_ldi(&st->it) == 0;
             const float beta = st_ldf(&st->beta), zinv = st_ldf(&st->zinv);
             double v[1] = {0.0};
-            co_ap<SOLID, ZT>(g, L, f, pc, first, beta, zinv, t0, stride, v[0]);
+            co_ap<LDT, SOLID, ZT>(g, L, f, pc, first, beta, zinv, t0, stride, v[0]);
             COOP_SYNC(coop_reduce<1>(g, bar, v, [&](double (&w)[1]) {
                 double pAp = (double)(float)w[0];
                 st->pAp = pAp;
@@ -2078,7 +2114,7 @@ __global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f,
             const bool first = st_ldi(&st->it) == 0;
             const float alpha = st_ldf(&st->alpha), mean = st_ldf(&st->mean);
             double v[2] = {0.0, 0.0};
-            co_xr<SOLID>(g, L, f, pc, first, alpha, mean, t0, stride, v);
+            co_xr<LDT, SOLID>(g, L, f, pc, first, alpha, mean, t0, stride, v);
             COOP_SYNC(coop_reduce<2>(g, bar, v, [&](double (&w)[2]) {
                 double rTr = (double)(float)w[0];
                 st->rTr = rTr;
@@ -2103,20 +2139,21 @@ __global__ void __launch_bounds__(kCoopThreads, 3) k_coop(G g, Levels a, Fine f,
         const float mean = l0 ? st_ldf(&st->mean) : 0.0f, zsc = l0 ? st_ldf(&st->zsc) : 1.0f;
         double zr = 0.0;
         if (l0) {
-            co_sweep<HS_FIRST, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+            co_sweep<LDT, HS_FIRST, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
             COOP_SYNC(coop_sync(st, bar));
         }
-        co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+        co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
         COOP_SYNC(coop_sync(st, bar));
-        co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
+        co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
         COOP_SYNC(coop_sync(st, bar));
-        co_sweep<HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
+        co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
         COOP_SYNC(coop_sync(st, bar));
-        co_restrict<SOLID, ZT>(g, L, C, l0, mean, zsc, l + 1 < lc, t0, stride);
+        co_restrict<LDT, SOLID, ZT>(g, L, C, l0, mean, zsc, l + 1 < lc, t0, stride);
         if (l + 1 < lc) COOP_SYNC(coop_sync(st, bar));
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 1);
 }
+#undef LDT
 
 // mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
 // wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479).
@@ -2561,12 +2598,12 @@ void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
 // one block per SM; EDGE_MGPCG_COOP=0 selects the per-level kernels.  The
 // grid is every block the device holds at once (occupancy x SMs, at most
 // kMaxBlocks, the capacity of the reduction partials).
-template <bool S, class ZT>
+template <bool S, class ZT, bool W>
 static int coop_grid_of() {
     int dev = 0, sms = 0, per_sm = 0, coop_ok = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
         cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop<S, ZT>, kCoopThreads, 0) != cudaSuccess) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop<S, ZT, W>, kCoopThreads, 0) != cudaSuccess) {
         (void)cudaGetLastError();
         return 0;
     }
@@ -2583,12 +2620,19 @@ void plan_coop(Ctx& c, bool solid) {
     if (V.lc < 1) return;
     for (int l = 0; l < V.lc; l++)
         if (!V.lv[l].vec) return;
+    const bool weak = env && env[0] == '2';
     int grid = 0;
-    if (c.ztype == 1) grid = solid ? coop_grid_of<true, __nv_bfloat16>() : coop_grid_of<false, __nv_bfloat16>();
-    else if (c.ztype == 2) grid = solid ? coop_grid_of<true, __half>() : coop_grid_of<false, __half>();
-    else grid = solid ? coop_grid_of<true, float>() : coop_grid_of<false, float>();
+    if (weak) {
+        if (c.ztype == 1) grid = solid ? coop_grid_of<true, __nv_bfloat16, true>() : coop_grid_of<false, __nv_bfloat16, true>();
+        else if (c.ztype == 2) grid = solid ? coop_grid_of<true, __half, true>() : coop_grid_of<false, __half, true>();
+        else grid = solid ? coop_grid_of<true, float, true>() : coop_grid_of<false, float, true>();
+    } else {
+        if (c.ztype == 1) grid = solid ? coop_grid_of<true, __nv_bfloat16, false>() : coop_grid_of<false, __nv_bfloat16, false>();
+        else if (c.ztype == 2) grid = solid ? coop_grid_of<true, __half, false>() : coop_grid_of<false, __half, false>();
+        else grid = solid ? coop_grid_of<true, float, false>() : coop_grid_of<false, float, false>();
+    }
     if (grid < 1) return;
-    c.coop = 1;
+    c.coop = weak ? 2 : 1;
     c.coop_grid = grid;
 }
 
@@ -2604,7 +2648,8 @@ static void launch_coop(const Ctx& c, cudaStream_t stream, int mode) {
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_coop<S, ZT>, c.g, c.lv, c.f, mode);
+    if (c.coop == 2) cudaLaunchKernelEx(&cfg, k_coop<S, ZT, true>, c.g, c.lv, c.f, mode);
+    else cudaLaunchKernelEx(&cfg, k_coop<S, ZT, false>, c.g, c.lv, c.f, mode);
 }
 
 template <bool S, class ZT>

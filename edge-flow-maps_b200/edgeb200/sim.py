@@ -499,7 +499,8 @@ def leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.03, circulation=1.0, x_st
 def random_potential_init(res, dx, kmax=8, slope=-17.0 / 6.0, seed=0, u_max=1.0, device="cuda"):
     """Divergence-free-in-the-continuum initial velocity u = curl A of a seeded
     random vector potential: every Fourier mode of the grid's periodic box
-    with integer index vector m, 1 <= |m| <= kmax, gets an independent
+    with integer index vector m, 1 <= |m| <= kmax (and below each axis's
+    Nyquist index), gets an independent
     complex normal amplitude per component scaled by |m|^slope (numpy
     default_rng(seed), modes in lexicographic order of (m0, m1, m2) with
     m2 >= 0); A is evaluated at the cell centres by an inverse real FFT,
@@ -513,7 +514,8 @@ def random_potential_init(res, dx, kmax=8, slope=-17.0 / 6.0, seed=0, u_max=1.0,
     r = np.arange(-kmax, kmax + 1)
     m0, m1, m2 = np.meshgrid(r, r, np.arange(0, kmax + 1), indexing="ij")
     k2 = m0 ** 2 + m1 ** 2 + m2 ** 2
-    sel = (k2 >= 1) & (k2 <= kmax * kmax)
+    # modes below each axis's Nyquist index only (no two modes share a bin)
+    sel = (k2 >= 1) & (k2 <= kmax * kmax) & (2 * np.abs(m0) < nx) & (2 * np.abs(m1) < ny) & (2 * m2 < nz)
     m0, m1, m2, k2 = m0[sel], m1[sel], m2[sel], k2[sel]
     amp = np.power(k2.astype(np.float64), slope / 2.0)
     coef = (rng.standard_normal((3, m0.size)) + 1j * rng.standard_normal((3, m0.size))) * amp
