@@ -2,6 +2,7 @@
 // step (sim/hermite.py, run_edge.py, run_ed4.py, run_ed8.py,
 // util/taichi_utils.py), one thread per cell or face.
 #include <cuda_runtime.h>
+#include <cstdlib>
 
 #include <algorithm>
 
@@ -212,16 +213,24 @@ EDGE_D void compose_jac(const float (&G)[3][3], const float (&C)[3][3], float (&
         }
 }
 
-template <bool IDENT, bool F64 = false>
-__global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+template <bool IDENT, bool F64 = false, int MINB = 4>
+__global__ void __launch_bounds__(128, MINB) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+    // The per-cell accumulators (the centre point's psi and Jacobian, the A
+    // and B groups of the mixed derivatives) live in shared memory, one
+    // column per thread, so that the registers hold only the current
+    // point's trajectory: 4 blocks of 128 threads per SM instead of 3.
+    __shared__ float acc[30][128];
+    float(&Pc)[3][128] = *reinterpret_cast<float(*)[3][128]>(&acc[0][0]);
+    float(&Tc)[9][128] = *reinterpret_cast<float(*)[9][128]>(&acc[3][0]);
+    float(&dA)[9][128] = *reinterpret_cast<float(*)[9][128]>(&acc[12][0]);
+    float(&dB)[9][128] = *reinterpret_cast<float(*)[9][128]>(&acc[21][0]);
+    const int tx = threadIdx.x;
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
     if (e >= n) return;
     int k = e % m.nz, j = (e / m.nz) % m.ny, i = e / (m.ny * m.nz);
     float X[3];
     cell_pos(i, j, k, m.dx, X);
-    float dA[3][3], dB[3][3];
-    float Pc[3], Tc[3][3];
 #pragma unroll 1
     for (int q = 0; q < 5; q++) {
         float P[3], C[3][3];
@@ -246,8 +255,8 @@ __global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float 
         }
         if (q == 0) {
             for (int c = 0; c < 3; c++) {
-                Pc[c] = P[c];
-                for (int d = 0; d < 3; d++) Tc[c][d] = T[c][d];
+                Pc[c][tx] = P[c];
+                for (int d = 0; d < 3; d++) Tc[3 * c + d][tx] = T[c][d];
             }
         } else {
             float sx = c_ed4_off[q - 1][0], sy = c_ed4_off[q - 1][1], sz = c_ed4_off[q - 1][2];
@@ -256,19 +265,22 @@ __global__ void __launch_bounds__(128, 3) k_march_edge_p(Mac mac, MapP m, float 
                 float a1 = sz * T[c][0], b1 = sx * T[c][2];
                 float a2 = sy * T[c][0], b2 = sx * T[c][1];
                 if (q == 1) {
-                    dA[c][0] = a0; dB[c][0] = b0; dA[c][1] = a1; dB[c][1] = b1; dA[c][2] = a2; dB[c][2] = b2;
+                    dA[3 * c][tx] = a0; dB[3 * c][tx] = b0; dA[3 * c + 1][tx] = a1; dB[3 * c + 1][tx] = b1;
+                    dA[3 * c + 2][tx] = a2; dB[3 * c + 2][tx] = b2;
                 } else {
-                    dA[c][0] += a0; dB[c][0] += b0; dA[c][1] += a1; dB[c][1] += b1; dA[c][2] += a2; dB[c][2] += b2;
+                    dA[3 * c][tx] += a0; dB[3 * c][tx] += b0; dA[3 * c + 1][tx] += a1; dB[3 * c + 1][tx] += b1;
+                    dA[3 * c + 2][tx] += a2; dB[3 * c + 2][tx] += b2;
                 }
             }
         }
     }
-    out[e] = make_float4(Pc[0], Pc[1], Pc[2], 0.f);
+    out[e] = make_float4(Pc[0][tx], Pc[1][tx], Pc[2][tx], 0.f);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        out[(size_t)(1 + d) * n + e] = make_float4(Tc[0][d], Tc[1][d], Tc[2][d], 0.f);
-        out[(size_t)(4 + d) * n + e] = make_float4((dA[0][d] + dB[0][d]) / 8.0f / eps, (dA[1][d] + dB[1][d]) / 8.0f / eps,
-                                                   (dA[2][d] + dB[2][d]) / 8.0f / eps, 0.f);
+        out[(size_t)(1 + d) * n + e] = make_float4(Tc[d][tx], Tc[3 + d][tx], Tc[6 + d][tx], 0.f);
+        out[(size_t)(4 + d) * n + e] =
+            make_float4((dA[d][tx] + dB[d][tx]) / 8.0f / eps, (dA[3 + d][tx] + dB[3 + d][tx]) / 8.0f / eps,
+                        (dA[6 + d][tx] + dB[6 + d][tx]) / 8.0f / eps, 0.f);
     }
 }
 
@@ -1312,9 +1324,20 @@ int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, f
     int n = nx * ny * nz;
     float4* o = (float4*)out_packed;
     if (variant == HV_GARM) {
-        if (identity) k_march_edge_p<true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
-        else if (f64) k_march_edge_p<false, true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
-        else k_march_edge_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        // EDGE_MARCH_BLOCKS=5: the register budget of 5 blocks per SM (96
+        // registers, a few spilled) instead of 4 (128)
+        static const bool five = getenv("EDGE_MARCH_BLOCKS") && getenv("EDGE_MARCH_BLOCKS")[0] == '5';
+        const int g = grid_for(n, 128);
+        if (identity) {
+            if (five) k_march_edge_p<true, false, 5><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else k_march_edge_p<true, false, 4><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        } else if (f64) {
+            if (five) k_march_edge_p<false, true, 5><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else k_march_edge_p<false, true, 4><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        } else {
+            if (five) k_march_edge_p<false, false, 5><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else k_march_edge_p<false, false, 4><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        }
     } else if (variant == HV_FD) {
         k_march_ed4_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
     } else {

@@ -196,123 +196,15 @@ struct ConvIn {
 constexpr int kSeg = 130;  // voxels staged per row (tile + 1 on each side)
 constexpr uint32_t kSegBytes = kSeg * 16;
 
-template <int COUT>
-__global__ void __launch_bounds__(128) k_conv_tc(Geo g, ConvIn in0, ConvIn in1, int nin, const float* __restrict__ bias,
-                                                 int flags, __nv_bfloat16* __restrict__ y, int* err) {
-    extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t tslot;
-    constexpr uint32_t NCOLS = COUT < 32 ? 32 : COUT;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nchmax = max(in0.cin, nin > 1 ? in1.cin : 0) / 8;
-    uint8_t* sseg = smem;
-    uint8_t* sw = smem + (size_t)3 * nchmax * kSegBytes;
-    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), NCOLS);
-    if (tid == 0) tc::mbar_init(tc::smem_u32(&mbar), 1);
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tbase = tslot;
-    const uint32_t idesc = tc::idesc_bf16(128, COUT, false, false);
-    uint32_t parity = 0;
-    bool bad = false;
-    for (int tile = blockIdx.x; tile < g.ntiles && !bad; tile += gridDim.x) {
-        const int v0 = tile * 128;
-        int nmma = 0;
-        bool pending = false;
-        for (int i = 0; i < nin && !bad; i++) {
-            const ConvIn in = i ? in1 : in0;
-            const int nch = in.cin / 8;
-            for (int dxi = 0; dxi < 3 && !bad; dxi++) {
-                if (pending) {  // the previous phase's MMAs still read shared memory
-                    bool ok = tc::mbar_wait(tc::smem_u32(&mbar), parity, kMaxPolls);
-                    parity ^= 1;
-                    pending = false;
-                    if (__syncthreads_or(!ok)) { bad = true; break; }
-                }
-                const long long base = (long long)v0 + (dxi - 1) * (long long)g.Sx - g.Sy - 1;
-                for (int e = tid; e < 3 * nch * kSeg; e += blockDim.x) {
-                    const int dyi = e / (nch * kSeg), rem = e - dyi * nch * kSeg;
-                    const int q = rem / kSeg, s = rem - q * kSeg;
-                    const long long v = base + (long long)dyi * g.Sy + s;
-                    const uint4 val = *reinterpret_cast<const uint4*>(in.x + act_off(g, q, v));
-                    *reinterpret_cast<uint4*>(sseg + ((size_t)(dyi * nch + q) * kSeg + s) * 16) = val;
-                }
-                const uint4* wsrc = reinterpret_cast<const uint4*>(in.w) + (size_t)dxi * 9 * nch * COUT;
-                for (int e = tid; e < 9 * nch * COUT; e += blockDim.x) reinterpret_cast<uint4*>(sw)[e] = wsrc[e];
-                tc::fence_smem_to_async();
-                tc::fence_before_sync();
-                __syncthreads();
-                tc::fence_after_sync();
-                if (tid == 0) {
-                    const uint32_t a0 = tc::smem_u32(sseg), b0 = tc::smem_u32(sw);
-                    for (int dyi = 0; dyi < 3; dyi++)
-                        for (int dzi = 0; dzi < 3; dzi++)
-                            for (int ks = 0; ks < nch / 2; ks++) {
-                                const uint64_t da = tc::sdesc(
-                                    a0 + (uint32_t)((dyi * nch + 2 * ks) * kSegBytes + dzi * 16), kSegBytes, 128);
-                                const uint64_t db = tc::sdesc(
-                                    b0 + (uint32_t)(((dyi * 3 + dzi) * nch + 2 * ks) * COUT * 16), COUT * 16, 128);
-                                tc::mma_bf16(tbase, da, db, idesc, nmma > 0 ? 1u : 0u);
-                                nmma++;
-                            }
-                    tc::commit(tc::smem_u32(&mbar));
-                }
-                pending = true;
-            }
-        }
-        if (bad) break;
-        {
-            bool ok = tc::mbar_wait(tc::smem_u32(&mbar), parity, kMaxPolls);
-            parity ^= 1;
-            if (__syncthreads_or(!ok)) { bad = true; break; }
-        }
-        tc::fence_after_sync();
-        // epilogue: this thread's voxel, all output channels
-        const int v = v0 + 32 * warp + lane;
-        int x, yy, z;
-        const bool in_dom = interior(g, v, x, yy, z);
-#pragma unroll
-        for (int c0 = 0; c0 < COUT; c0 += 16) {
-            float acc[16];
-            tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, acc);
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                uint4* dst = reinterpret_cast<uint4*>(y + act_off(g, (c0 >> 3) + h, v));
-                float old[8] = {0, 0, 0, 0, 0, 0, 0, 0}, o[8];
-                if (flags & 2) unpack8(*dst, old);
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    float t = acc[8 * h + j] + (bias ? bias[c0 + 8 * h + j] : 0.0f);
-                    if (flags & 1) t = fmaxf(t, 0.0f);
-                    t += old[j];
-                    o[j] = in_dom ? t : 0.0f;
-                }
-                *dst = pack8(o);
-            }
-        }
-        tc::fence_before_sync();
-        __syncthreads();
-        tc::fence_after_sync();
-    }
-    if (bad) {
-        if (tid == 0) atomicExch(err, 1);
-        tc::mbar_wait(tc::smem_u32(&mbar), parity, kMaxPolls);  // outstanding MMAs finish before TMEM is freed
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) tc::tmem_free(tbase, NCOLS);
-}
-
-// The same convolution with the staging done by the bulk-copy engine into one
-// or two stages: thread 0 issues, per phase (input, dx), one 2080-byte bulk copy per
-// (dy, channel chunk) row and one for the phase's weights into a stage, the
-// MMAs of a phase read the other stage while the next phase's copies land,
-// and the epilogue of a tile overlaps the copies of the next tile's first
-// phase (two stages).  Stage contents, descriptors and the MMA sequence are k_conv_tc's,
-// so the result is identical.  With nstage = 1 (the default) a phase's
-// copies wait for the previous phase's MMAs; the other blocks on the SM fill
-// that gap.
+// The convolution kernel.  Thread 0 stages, per phase (input, dx), one
+// 2080-byte bulk copy per (dy, channel chunk) row and one for the phase's
+// weights into a stage of shared memory (completion counted on an mbarrier
+// with expect_tx) and issues the phase's MMAs from it.  The kernel can ring
+// two stages (the next phase's copies landing while the MMAs read the
+// other); the launch uses one, whose smaller footprint lets two to four
+// times more blocks share an SM, which measured faster on every U-Net layer
+// (forward at 256x128x128: 3.03 ms against 3.52 ms with two stages, 4.88 ms
+// with the stages filled by the threads instead of the copy engine).
 template <int COUT>
 __global__ void __launch_bounds__(128) k_conv_bulk(Geo g, ConvIn in0, ConvIn in1, int nin,
                                                    const float* __restrict__ bias, int flags,
@@ -1011,49 +903,22 @@ static int resident_blocks(size_t smem, int cout) {
     return std::max(1, std::min(by_smem, by_tmem));
 }
 
-// Kernel choice per layer.  By default every layer takes the bulk-copy kernel
-// with one stage: the smaller shared-memory footprint lets two to four times
-// more blocks share an SM, which measured faster on every layer than two
-// stages (U-Net forward at 256x128x128: 3.03 ms against 3.52 ms).  For
-// comparison EDGE_CONV_STAGED=1 forces the thread-staged k_conv_tc and =3 two
-// stages wherever they fit; all choices give bit-identical outputs.
-static int g_conv_mode() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("EDGE_CONV_STAGED");
-        v = e ? e[0] - '0' : 0;
-    }
-    return v;
-}
-
 template <int COUT>
 int launch_conv(const Geo& g, ConvIn a, ConvIn b, int nin, const float* bias, int flags, __nv_bfloat16* y, int* err,
                 cudaStream_t st) {
     const int nchmax = std::max(a.cin, nin > 1 ? b.cin : 0) / 8;
     const size_t smem = (size_t)3 * nchmax * kSegBytes + (size_t)9 * nchmax * COUT * 16;
     if (smem > 200 * 1024) return EDGE_EINVAL;
-    const int mode = g_conv_mode();
-    if (mode != 1) {
-        const uint32_t stage = (uint32_t)((smem + 127) / 128 * 128);
-        const bool two = mode == 3 && 2 * (size_t)stage <= 200 * 1024;
-        const int nstage = two ? 2 : 1;
-        const size_t total = (size_t)nstage * stage;
-        cudaError_t e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
-        if (e != cudaSuccess) return (int)e;
-        e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return (int)e;
-        const int grid = std::min(g.ntiles, g_sms() * resident_blocks(total, COUT));
-        k_conv_bulk<COUT><<<grid, 128, total, st>>>(g, a, b, nin, bias, flags, y, err, nstage, stage);
-        return rc_last();
-    }
-    cudaError_t e = cudaFuncSetAttribute(k_conv_tc<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const uint32_t stage = (uint32_t)((smem + 127) / 128 * 128);
+    const int nstage = 1;
+    const size_t total = (size_t)nstage * stage;
+    cudaError_t e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total);
     if (e != cudaSuccess) return (int)e;
-    e = cudaFuncSetAttribute(k_conv_tc<COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    e = cudaFuncSetAttribute(k_conv_bulk<COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return (int)e;
-    const int grid = std::min(g.ntiles, g_sms() * resident_blocks(smem, COUT));
-    k_conv_tc<COUT><<<grid, 128, smem, st>>>(g, a, b, nin, bias, flags, y, err);
+    const int grid = std::min(g.ntiles, g_sms() * resident_blocks(total, COUT));
+    k_conv_bulk<COUT><<<grid, 128, total, st>>>(g, a, b, nin, bias, flags, y, err, nstage, stage);
     return rc_last();
 }
 
