@@ -2493,10 +2493,9 @@ static void launch_pdl(void (*k)(KArgs...), int grid, int block, size_t smem, cu
     cudaLaunchKernelEx(&cfg, k, args...);
 }
 
-// One V-cycle (mgpcg.py:177-195); with final_zr the last kernel also forms
-// z.r and the end-of-iteration bookkeeping (mgpcg.py:263-277).
+// the descent of a V-cycle: levels 0..lc-1 (sweeps and restrictions)
 template <bool S, class ZT>
-void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
+void vdown_t(const Ctx& c, cudaStream_t stream) {
     const Levels& V = c.lv;
     const int lc = V.lc;  // levels 0..lc-1 run per-level kernels, lc..L-1 the shared-memory group
     const int lgroup = V.lc;
@@ -2520,11 +2519,14 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
             launch_pdl(k_restrict<S, ZT>, rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream, c.g, L, C, l0, first);
         }
     }
-    if (final_zr && lc == 0) {
-        launch_pdl(k_coarse<true, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
-    } else {
-        launch_pdl(k_coarse<false, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
-    }
+}
+
+// the ascent of a V-cycle: levels lc-1..0 (prolongation and sweeps); with
+// final_zr the last sweep also forms z.r and the iteration's bookkeeping
+template <bool S, class ZT>
+void vup_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
+    const Levels& V = c.lv;
+    const int lc = V.lc;
     for (int l = lc - 1; l >= 0; l--) {
         const Lvl& L = V.lv[l];
         const Lvl& C = V.lv[l + 1];
@@ -2546,6 +2548,22 @@ void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
             else launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
         }
     }
+}
+
+
+// One V-cycle (mgpcg.py:177-195); with final_zr the last kernel also forms
+// z.r and the end-of-iteration bookkeeping (mgpcg.py:263-277).
+template <bool S, class ZT>
+void vcycle_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
+    const Levels& V = c.lv;
+    const int lc = V.lc;
+    vdown_t<S, ZT>(c, stream);
+    if (final_zr && lc == 0) {
+        launch_pdl(k_coarse<true, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
+    } else {
+        launch_pdl(k_coarse<false, S, ZT>, 1, 1024, c.csmem, stream, c.g, V);
+    }
+    vup_t<S, ZT>(c, stream, final_zr);
 }
 
 void enqueue_vcycle(const Ctx& c, bool solid, cudaStream_t stream, bool final_zr) {
@@ -2585,6 +2603,29 @@ void enqueue_cg(const Ctx& c, bool solid, cudaStream_t stream) {
     } else {
         if (solid) cg_kernels<true, float>(c, stream);
         else cg_kernels<false, float>(c, stream);
+    }
+}
+
+// The stepwise solve on the per-level kernels: a V-cycle's descent, and one
+// step = the ascent with z.r, the CG kernels, the next descent.
+template <bool S, class ZT>
+void step_pl_t(const Ctx& c, cudaStream_t stream, bool down_only) {
+    if (!down_only) {
+        vup_t<S, ZT>(c, stream, true);
+        cg_kernels<S, ZT>(c, stream);
+    }
+    vdown_t<S, ZT>(c, stream);
+}
+void enqueue_step_pl(const Ctx& c, bool solid, cudaStream_t stream, bool down_only) {
+    if (c.ztype == 1) {
+        if (solid) step_pl_t<true, __nv_bfloat16>(c, stream, down_only);
+        else step_pl_t<false, __nv_bfloat16>(c, stream, down_only);
+    } else if (c.ztype == 2) {
+        if (solid) step_pl_t<true, __half>(c, stream, down_only);
+        else step_pl_t<false, __half>(c, stream, down_only);
+    } else {
+        if (solid) step_pl_t<true, float>(c, stream, down_only);
+        else step_pl_t<false, float>(c, stream, down_only);
     }
 }
 
@@ -2687,7 +2728,7 @@ void enqueue_loop_body(const Ctx& c, bool solid, cudaStream_t stream) {
 
 // set-up kernels of Poisson / solve (everything before the CG loop)
 void enqueue_setup(Solver* s, Faces U, const float* rhs, double abs_tol, double rel_tol, int max_iters,
-                   cudaStream_t cs) {
+                   cudaStream_t cs, bool stepwise = false) {
     Ctx& c = s->ctx;
     const Lvl& L0 = c.lv.lv[0];
     int n = L0.n0 * L0.n1 * L0.n2;
@@ -2714,8 +2755,9 @@ void enqueue_setup(Solver* s, Faces U, const float* rhs, double abs_tol, double 
     if (s->solid) k_setup_rhs<true><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
     else k_setup_rhs<false><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
     if (s->solid && !rhs) k_solid_fix<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f);
-    if (c.coop) enqueue_coop(c, s->solid, cs, COOP_DOWN);  // the first V-cycle's down half
-    else enqueue_vcycle(c, s->solid, cs, true);           // first preconditioner application + z.r + tol
+    if (c.coop) enqueue_coop(c, s->solid, cs, COOP_DOWN);      // the first V-cycle's down half
+    else if (stepwise) enqueue_step_pl(c, s->solid, cs, true);  // the same on the per-level kernels
+    else enqueue_vcycle(c, s->solid, cs, true);               // first preconditioner application + z.r + tol
 }
 
 // gradient update (Poisson) or the solution copy (solve)
@@ -3085,7 +3127,7 @@ int edge_mgpcg_coarse_shape(void* handle, int* level, int* dims) {
     dims[0] = V.lv[V.lc].n0;
     dims[1] = V.lv[V.lc].n1;
     dims[2] = V.lv[V.lc].n2;
-    return s->ctx.coop ? EDGE_OK : EDGE_ESTATE;
+    return V.lc >= 1 ? EDGE_OK : EDGE_ESTATE;
 }
 
 int edge_mgpcg_coarse_get_r(void* handle, float* dense, void* stream) {
@@ -3110,7 +3152,7 @@ int edge_mgpcg_coarse_set_z(void* handle, const float* dense, void* stream) {
 int edge_mgpcg_coarse_default(void* handle, void* stream) {
     if (!handle) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    if (!s->ctx.coop) return EDGE_ESTATE;
+    if (s->ctx.lv.lc < 1) return EDGE_ESTATE;
     Ctx c = s->ctx;
     c.g.use_cond = 0;
     const int t = c.ztype;
@@ -3132,23 +3174,53 @@ int edge_mgpcg_solve_begin(void* handle, const float* b, double abs_tol, double 
                            void* stream) {
     if (!handle || !b) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    if (!s->ctx.coop) return EDGE_ESTATE;
+    if (s->ctx.lv.lc < 1) return EDGE_ESTATE;
     if (max_iters < 0) max_iters = s->solid ? 100 : 400;
     Faces U = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     s->ctx.g.use_cond = 0;
     s->ctx.g.use_vcond = 0;
-    enqueue_setup(s, U, b, abs_tol, rel_tol, max_iters, (cudaStream_t)stream);
+    s->ctx.g.nochk = 0;
+    enqueue_setup(s, U, b, abs_tol, rel_tol, max_iters, (cudaStream_t)stream, true);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_poisson_begin(void* handle, float* ux, float* uy, float* uz, double abs_tol, double rel_tol,
+                             int max_iters, void* stream) {
+    if (!handle || !ux || !uy || !uz) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    if (s->ctx.lv.lc < 1) return EDGE_ESTATE;
+    if (max_iters < 0) max_iters = s->solid ? 100 : 400;
+    Faces U = {{ux, uy, uz}, {nullptr, nullptr, nullptr}};
+    s->ctx.g.use_cond = 0;
+    s->ctx.g.use_vcond = 0;
+    s->ctx.g.nochk = 0;
+    enqueue_setup(s, U, nullptr, abs_tol, rel_tol, max_iters, (cudaStream_t)stream, true);
+    return cu(cudaPeekAtLastError());
+}
+
+int edge_mgpcg_poisson_end(void* handle, float* ux, float* uy, float* uz, float* fx, float* fy, float* fz,
+                           void* stream) {
+    if (!handle || !ux || !uy || !uz) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    Faces U = {{ux, uy, uz}, {fx, fy, fz}};
+    enqueue_finish(s, U, nullptr, nullptr, (cudaStream_t)stream);
     return cu(cudaPeekAtLastError());
 }
 
 int edge_mgpcg_solve_iter(void* handle, void* stream) {
     if (!handle) return EDGE_EINVAL;
     Solver* s = (Solver*)handle;
-    if (!s->ctx.coop) return EDGE_ESTATE;
+    if (s->ctx.lv.lc < 1) return EDGE_ESTATE;
     Ctx c = s->ctx;
     c.g.use_cond = 0;
+    c.g.use_vcond = 0;
+    c.g.nochk = 0;
     const int t = c.ztype;
     cudaStream_t st = (cudaStream_t)stream;
+    if (!c.coop) {
+        enqueue_step_pl(c, s->solid, st, false);
+        return cu(cudaPeekAtLastError());
+    }
     if (t == 1) {
         if (s->solid) launch_coop<true, __nv_bfloat16>(c, st, COOP_ITER);
         else launch_coop<false, __nv_bfloat16>(c, st, COOP_ITER);

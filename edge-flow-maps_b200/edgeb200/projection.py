@@ -107,6 +107,15 @@ class Projection:
         N.call("edge_mgpcg_solve_begin", self._h, ptr(b, "b"), ctypes.c_double(abs_tol), ctypes.c_double(rel_tol),
                int(max_iters), stream())
 
+    def poisson_begin(self, u_x, u_y, u_z, abs_tol=1e-12, rel_tol=1e-12, max_iters=-1):
+        N.call("edge_mgpcg_poisson_begin", self._h, ptr(u_x, "u_x"), ptr(u_y, "u_y"), ptr(u_z, "u_z"),
+               ctypes.c_double(abs_tol), ctypes.c_double(rel_tol), int(max_iters), stream())
+
+    def poisson_end(self, u_x, u_y, u_z, f=None):
+        fx, fy, fz = (None, None, None) if f is None else f
+        N.call("edge_mgpcg_poisson_end", self._h, ptr(u_x, "u_x"), ptr(u_y, "u_y"), ptr(u_z, "u_z"), ptr(fx),
+               ptr(fy), ptr(fz), stream())
+
     def coarse_get_r(self, dense):
         N.call("edge_mgpcg_coarse_get_r", self._h, ptr(dense), stream())
 

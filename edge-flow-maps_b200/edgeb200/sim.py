@@ -33,12 +33,15 @@ VARIANTS = {"edge": N.HERMITE_GARM, "ed4": N.HERMITE_FD, "ed8": N.HERMITE_FULL, 
 class EdgeSim:
     def __init__(self, res, dx, variant="edge", cfl=0.5, reinit_every=12, ed_eps=None, base_level=3,
                  bfecc_clamp=True, visualize_dt=0.1, abs_tol=1e-12, rel_tol=1e-12, device="cuda", solid=None,
-                 emitters=None, packed=True, precision=0):
+                 emitters=None, packed=True, precision=0, learned=None):
         """precision: 0 runs the reference's float32 arithmetic; 1 (BF16) and
         2 (FP16) store the projection's V-cycle levels in 16 bits (float32
         residuals and arithmetic, float64 dot products, as in
         Projection(precision=...)) and accumulate the EDGE march's composed
-        Jacobian in float64."""
+        Jacobian in float64.  learned: U-Net parameters (edgeb200.train_unet
+        load_params) of the learned coarse-level solver; both projections of
+        every step then run MGPCG with the network as the V-cycle's coarse
+        group (edgeb200.unet.LearnedCoarsePCG, plain MGPCG as fallback)."""
         if variant not in VARIANTS:
             raise ValueError(f"variant must be one of {sorted(VARIANTS)}")
         if precision not in (0, 1, 2):
@@ -100,6 +103,10 @@ class EdgeSim:
         else:
             self.proj = Projection(r, base_level=base_level, precision=self.precision)
             self.max_iters = 400  # mgpcg.py:434-438
+        self.learned = None
+        if learned is not None:
+            from .unet import LearnedCoarsePCG
+            self.learned = LearnedCoarsePCG(self.proj, learned)
         self.emitters = emitters
         self.side_stream = torch.cuda.Stream(device=device)
         self.particles = None
@@ -258,7 +265,8 @@ class EdgeSim:
         ops.advect_u_sl(self.u, dx, 0.5 * curr_dt, self.tmp_u)
         self.u, self.tmp_u = self.tmp_u, self.u
         tm.stop("pre-advect")
-        self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
+        proj = self.learned if self.learned is not None else self.proj
+        proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
         tm.start("advect")
         # The backward-map march and the forward-map march both read only the
         # projected u: the forward map runs on a side stream next to the march
@@ -323,10 +331,10 @@ class EdgeSim:
             P = self.particles
             for v in P["vis"]:
                 v.zero_()
-            self.proj.poisson(*self.u, f=P["vis"], abs_tol=self.abs_tol, rel_tol=self.rel_tol,
-                              max_iters=self.max_iters)
+            proj.poisson(*self.u, f=P["vis"], abs_tol=self.abs_tol, rel_tol=self.rel_tol,
+                         max_iters=self.max_iters)
         else:
-            self.proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
+            proj.poisson(*self.u, abs_tol=self.abs_tol, rel_tol=self.rel_tol, max_iters=self.max_iters)
         tm.stop("substep")
         return curr_dt
 

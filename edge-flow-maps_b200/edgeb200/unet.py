@@ -436,6 +436,7 @@ class LearnedCoarsePCG:
         self.stall = float(stall)
         self.graphs = {}
         self.use_graphs = bool(graphs)
+        self.fell_back = False
 
     def _step(self, mode):
         if mode == "net":
@@ -470,11 +471,26 @@ class LearnedCoarsePCG:
                 return
         g.replay()
 
+    def poisson(self, u_x, u_y, u_z, f=None, abs_tol=1e-12, rel_tol=1e-12, max_iters=-1, mode="net"):
+        """The projection (Projection.poisson's arguments and effect) with the
+        learned coarse solver."""
+        self.P.poisson_begin(u_x, u_y, u_z, abs_tol=abs_tol, rel_tol=rel_tol, max_iters=max_iters)
+        fell = self._loop(mode)
+        self.P.poisson_end(u_x, u_y, u_z, f)
+        self.fell_back = fell
+
     def solve(self, b, x, abs_tol=1e-12, rel_tol=1e-12, max_iters=400, mode="net"):
         """x solves A x = b (the solver's tolerance semantics, mgpcg.py:224).
         Returns (iterations, r.r, status, fell_back)."""
         P = self.P
         P.solve_begin(b, abs_tol=abs_tol, rel_tol=rel_tol, max_iters=max_iters)
+        fell_back = self._loop(mode)
+        P.solve_end(b, x)
+        it, rtr, st = P.result()
+        return it, rtr, st, fell_back
+
+    def _loop(self, mode):
+        P = self.P
         fell_back = False
         prev = None
         while True:
@@ -485,6 +501,4 @@ class LearnedCoarsePCG:
             if mode == "net" and prev is not None and rtr > self.stall * self.stall * prev:
                 mode, fell_back = "vcycle", True
             prev = rtr
-        P.solve_end(b, x)
-        it, rtr, st = P.result()
-        return it, rtr, st, fell_back
+        return fell_back

@@ -273,7 +273,7 @@ int edge_mgpcg_apply_A_f64(void *handle, const double *p, double *Ap, void *stre
  * the learned preconditioner's path).  The V-cycle's levels lc..L-1 normally
  * run in one shared-memory block (the coarse group); these calls let the
  * caller replace that group by its own solver of the level-lc residual
- * equation.  Available on the cooperative path only (EDGE_ESTATE otherwise).
+ * equation.  EDGE_ESTATE when the whole grid fits the coarse group (lc = 0).
  *   coarse_shape: lc and its cell dims (int[3]);
  *   solve_begin:  set-up of solve(b) up to the first V-cycle's coarse level;
  *   coarse_get_r: the level-lc residual as a float32 cell array;
@@ -293,6 +293,14 @@ int edge_mgpcg_coarse_set_z(void *handle, const float *dense, void *stream);
 int edge_mgpcg_coarse_default(void *handle, void *stream);
 int edge_mgpcg_solve_iter(void *handle, void *stream);
 int edge_mgpcg_solve_end(void *handle, const float *b, float *x, void *stream);
+/* The same for the projection (edge_mgpcg_poisson): poisson_begin applies
+ * the walls / solid velocities and forms the divergence, poisson_end
+ * subtracts the pressure gradient (and writes -grad p into f*, each may be
+ * NULL, as Poisson_with_buffer does). */
+int edge_mgpcg_poisson_begin(void *handle, float *ux, float *uy, float *uz, double abs_tol, double rel_tol,
+                             int max_iters, void *stream);
+int edge_mgpcg_poisson_end(void *handle, float *ux, float *uy, float *uz, float *fx, float *fy, float *fz,
+                           void *stream);
 /* Iterations, r.r and whether the CG loop still runs (1) or has ended (0);
  * synchronises the stream. */
 int edge_mgpcg_progress(void *handle, int *iters, double *rTr, int *running, void *stream);
