@@ -724,10 +724,10 @@ def run_ours(args, rank, world, local_rank):
                "d2h_bytes_per_step": nbytes}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sec, cores, k = cpu_reference_steps(1, 0)
+        sec, cores, k = cpu_reference_steps(1, 1)
         cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "1 full substep of the same workload (first step after reinit), C/OpenMP restatement "
-                         "of the reference kernels"}
+               "sample": "1 full substep of the same workload in the middle of a reinitialisation interval (after "
+                         "one untimed substep), C/OpenMP restatement of the reference kernels"}
     # ED4 / ED8 / GE / EFM steps of the same workload (a few steps each, outside the
     # timed region of the EDGE line)
     variants = {}
