@@ -366,7 +366,7 @@ def _refined_stats(P, b, reps, ref, inner_rel):
 def pcg_measure(res, reps=5, variants=True):
     """Pressure solve to 1e-6 relative residual on a seeded N(0,1)
     mean-removed right-hand side: the plain float32 solver (the roofline
-    line; cooperative iteration kernel, and the per-level kernels beside it),
+    line),
     the BF16 and FP16 mixed-precision solvers, and iterative refinement that
     brings the TRUE residual to 1e-6 (float64 residual and iterate around
     float32 or FP16 inner solves); errors against an FP64 solve."""
@@ -379,7 +379,6 @@ def pcg_measure(res, reps=5, variants=True):
     b = b.float().cuda()
     tol = PCG_REL * PCG_REL * bb
     nc = res[0] * res[1] * res[2]
-    os.environ.pop("EDGE_MGPCG_COOP", None)
     out, P = _solve_stats(res, b, bb, tol, 0, reps, None)
     ref = fp64_solve(P, b)
     x = torch.zeros(res, device="cuda")
@@ -395,12 +394,6 @@ def pcg_measure(res, reps=5, variants=True):
         return out
     out["refined"] = {"fp32": _refined_stats(P, b, reps, ref, 1e-2)}
     P.close()
-    # the per-level kernels (no cooperative launch), same arithmetic
-    os.environ["EDGE_MGPCG_COOP"] = "0"
-    pl, Pp = _solve_stats(res, b, bb, tol, 0, reps, ref)
-    Pp.close()
-    os.environ.pop("EDGE_MGPCG_COOP", None)
-    out["per_level_kernels"] = {"ms": pl["ms"], "iters": pl["iters"]}
     out["mixed"] = {}
     for name, prec in (("bf16", 1), ("fp16", 2)):
         m, Pm = _solve_stats(res, b, bb, tol, prec, reps, ref)

@@ -1105,7 +1105,6 @@ const char* edge_error_string(int code) {
         case EDGE_ENAN: return "non-finite residual";
         case EDGE_ESTALL: return "residual stalled";
         case EDGE_ESTATE: return "invalid call order or handle state";
-        case EDGE_ETIMEOUT: return "a bounded wait inside a solver launch ran out of time";
         default: return code > 0 ? cudaGetErrorString((cudaError_t)code) : "unknown error";
     }
 }

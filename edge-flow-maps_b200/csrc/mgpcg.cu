@@ -40,20 +40,18 @@ using namespace edge;
 
 namespace {
 
-enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_NOCONV = 2, ST_NAN = 3, ST_TIMEOUT = 4 };
+enum { ST_RUNNING = 0, ST_CONVERGED = 1, ST_NOCONV = 2, ST_NAN = 3 };
 
 struct SolveState {
     double zTr, pAp, rTr, rsum, tol, abs_tol, rel_tol, div_sum;
     float alpha, beta, mean, zsc;
     float zinv;   // 1 / zsc
     int zscaled;  // FP16 level storage: zsc follows the residual's RMS (set_zscale)
-    int pad1, pad2;
+    int restart;  // 1: the next z.r epilogue restarts the recursion (beta = 0)
+    int pad2;
     int it, max_iters, status, setup;
     int pcur, all_neumann, n_fluid, x_valid;
     unsigned int counter[8];
-    // grid barrier of the cooperative iteration kernel: arrivals, generation,
-    // and the flag a block sets when a wait ran out of time
-    unsigned int bar_count, bar_gen, bar_abort, bar_pad;
     unsigned long long kernels;  // kernels of this solver run so far (launch accounting)
 };
 
@@ -134,9 +132,6 @@ struct Ctx {
     Fine f;
     int csmem;  // dynamic shared memory of k_coarse (bytes)
     int ztype;  // storage of the V-cycle's level arrays: 0 FP32, 1 BF16, 2 FP16 (mixed-precision solvers)
-    // 1: the CG loop runs k_coarse + k_coop(ITER) per iteration on a grid of
-    // coop_grid co-resident blocks (plan_coop); 0: the per-level kernels
-    int coop = 0, coop_grid = 0;
 };
 
 EDGE_D void set_cond(const G& g, unsigned v) {
@@ -456,7 +451,8 @@ EDGE_D void zr_epilogue(const G& g, double zr) {
         st->tol = fmax(st->abs_tol, zTr * st->rel_tol);
         if (st->max_iters <= 0) st->status = ST_NOCONV;
     } else {
-        st->beta = (float)(zTr / (st->zTr + 1e-12));
+        st->beta = st->restart ? 0.0f : (float)(zTr / (st->zTr + 1e-12));
+        st->restart = 0;
         st->zTr = zTr;
         st->it += 1;
         if (st->it >= st->max_iters) st->status = ST_NOCONV;
@@ -580,6 +576,7 @@ __global__ void __launch_bounds__(256) k_setup_rhs(G g, Lvl L, Fine f, Faces U, 
             st->it = 0;
             st->status = ST_RUNNING;
             st->setup = 1;
+            st->restart = 0;
             st->beta = 0.0f;
             st->alpha = 0.0f;
             st->pcur = 0;
@@ -1657,504 +1654,6 @@ __global__ void __launch_bounds__(256) k_restrict4(G g, Lvl F, Lvl C, int level0
     }
 }
 
-// z of the coarse level at the parent of fine cell (i, j, k), read through L2
-template <class ZT>
-EDGE_D float parent_zc(const Lvl& C, int i, int j, int k) {
-    int I = i >> 1, J = j >> 1, K = k >> 1;
-    int e = (I * C.n1 + J) * C.H + (K >> 1);
-    return Zc<ZT>::ld(pick(C.z, (I + J + K) & 1), e);
-}
-
-// ---------------------------------------------------------------------------
-// Cooperative CG iteration (k_coop): the levels that run per-level kernels
-// (0..lc-1) and the CG vector updates of one iteration in ONE launch over a
-// grid of co-resident blocks (cooperative launch), phases separated by a grid
-// barrier instead of a kernel boundary.  An iteration of the graph's loop is
-// then two launches: k_coarse (the shared-memory coarse group, one block) and
-//   k_coop(ITER): up sweeps lc-1..0 (the fine level's last one forms z.r and
-//                 beta), p = z + beta p with A p and p.Ap, the x and r updates
-//                 with r.r and the convergence test, then - while running -
-//                 the down sweeps and restrictions 0..lc-1 of the next
-//                 V-cycle;
-// the set-up ends with k_coop(DOWN), the down half alone.  Each phase runs
-// the same per-cell arithmetic, in the same order, as the per-level kernels
-// (k_hsweep4, k_restrict4, k_cg_ap4, k_cg_xr4); the reductions' per-block
-// partials are summed in block order by the last block to arrive at the
-// barrier, which publishes the scalars before it releases the others.
-// Data written inside the launch is read through L2 (ld.global.cg).  Every
-// wait is bounded: a block whose wait runs out of time sets an abort flag that
-// every other waiting block sees, the solve ends with ST_TIMEOUT, and all
-// blocks return.
-// ---------------------------------------------------------------------------
-enum { COOP_DOWN = 0, COOP_ITER = 1 };
-constexpr unsigned long long kCoopWaitNs = 2000000000ull;  // 2 s
-
-EDGE_D unsigned ld_acquire_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-EDGE_D void st_release_u32(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-EDGE_D unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-struct CoopBar {
-    unsigned gen;  // generation this block expects next (thread 0)
-    int ok;        // 0 once the launch is aborted (shared)
-};
-
-// Thread 0: wait until the barrier's generation reaches `target`; false when
-// the launch was aborted or this wait ran out of time (which aborts it).
-EDGE_D bool coop_wait(SolveState* st, unsigned target) {
-    const unsigned long long t0 = global_ns();
-    unsigned n = 0;
-    while (ld_acquire_u32(&st->bar_gen) != target) {
-        if (*((volatile unsigned*)&st->bar_abort)) return false;
-        if ((++n & 63u) == 0 && global_ns() - t0 > kCoopWaitNs) {
-            atomicExch(&st->bar_abort, 1u);
-            st->status = ST_TIMEOUT;
-            return false;
-        }
-    }
-    return true;
-}
-
-// Grid barrier; returns false in every thread of the block once the launch
-// is aborted.
-EDGE_D bool coop_sync(SolveState* st, CoopBar& b) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned target = b.gen + 1;
-        __threadfence();
-        bool ok = true;
-        if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
-            __threadfence();  // acquire: the other blocks' writes before their arrivals
-            atomicExch(&st->bar_count, 0u);  // no block arrives again before the release below
-            st_release_u32(&st->bar_gen, target);
-        } else {
-            ok = coop_wait(st, target);
-        }
-        b.gen = target;
-        b.ok = ok;
-    }
-    __syncthreads();
-    return b.ok;
-}
-
-// Grid barrier with a reduction: the block's partials v (summed over the
-// block) are published, the last block to arrive sums all blocks' partials
-// in block order and runs epi(sums) in its thread 0 before releasing the
-// others, so every block reads epi's results after the barrier.
-template <int N, class EPI>
-EDGE_D bool coop_reduce(const G& g, CoopBar& b, double (&v)[N], EPI epi) {
-    __shared__ int last;
-    SolveState* st = g.st;
-    block_sum<N>(v);
-    const int nblk = gridDim.x;
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < N; q++) g.partials[q * nblk + blockIdx.x] = v[q];
-        __threadfence();
-        last = atomicAdd(&st->bar_count, 1u) == (unsigned)nblk - 1;
-    }
-    __syncthreads();
-    const unsigned target = b.gen + 1;
-    if (last) {
-        __threadfence();
-        double w[N];
-#pragma unroll
-        for (int q = 0; q < N; q++) {
-            double s = 0.0;
-            for (int k = threadIdx.x; k < nblk; k += blockDim.x) s += __ldcg(g.partials + q * nblk + k);
-            w[q] = s;
-        }
-        block_sum<N>(w);
-        if (threadIdx.x == 0) {
-            epi(w);
-            atomicExch(&st->bar_count, 0u);
-            __threadfence();
-            st_release_u32(&st->bar_gen, target);
-            b.ok = 1;
-        }
-    } else if (threadIdx.x == 0) {
-        b.ok = coop_wait(st, target);
-    }
-    if (threadIdx.x == 0) b.gen = target;
-    __syncthreads();
-    return b.ok;
-}
-
-EDGE_D float st_ldf(const float* p) { return *((const volatile float*)p); }
-EDGE_D int st_ldi(const int* p) { return *((const volatile int*)p); }
-
-// Weak loads of data written earlier in the same launch (plain ld.global,
-// L1-cached): correct after the grid barrier, whose acquire and block
-// barrier order them after the other blocks' released writes.
-template <class ZT>
-struct Zw;
-template <>
-struct Zw<float> {
-    static EDGE_D float ld(const float* b, int e) { return b[e]; }
-    static EDGE_D float2 ld2(const float* b, int e) { return *reinterpret_cast<const float2*>(b + e); }
-    static EDGE_D void ld4(const float* b, int e, float (&v)[4]) {
-        float4 t = *reinterpret_cast<const float4*>(b + e);
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    }
-};
-template <>
-struct Zw<__nv_bfloat16> : Zs<__nv_bfloat16> {};
-template <>
-struct Zw<__half> : Zs<__half> {};
-
-// one half sweep of colour `color` on a four-slot level (k_hsweep4's
-// arithmetic), slots t0, t0 + stride, ...; HS_ZR adds z.r over both colours
-// to zr
-template <template <class> class LD, int MODE, bool SOLID, class ZT>
-EDGE_D void co_sweep(const G& g, const Lvl& L, const Lvl& C, int color, int level0, float mean, float zsc, int t0,
-                     int stride, double& zr) {
-    const int oc = color ^ 1;
-    const float* rs = pick(L.r, color);
-    const float* zo = pick(L.z, oc);
-    float* zs = pick(L.z, color);
-    const int nq = L.n0 * L.n1 * (L.H >> 2);
-    for (int t = t0; t < nq; t += stride) {
-        const Quad q = quad_of(L, t);
-        const int p = (q.i + q.j + color) & 1;
-        unsigned code[4];
-        quad_codes<SOLID>(L, color, q, p, code);
-        float rv[4], ns[4] = {0.0f, 0.0f, 0.0f, 0.0f}, zn[4];
-        if (level0) LD<float>::ld4(rs, q.t0, rv);
-        else LD<ZT>::ld4(rs, q.t0, rv);
-        if (MODE != HS_FIRST) {
-            auto v4 = [&](int e, float(&o)[4]) { LD<ZT>::ld4(zo, e, o); };
-            auto v1 = [&](int e) { return LD<ZT>::ld(zo, e); };
-            if (MODE == HS_PROLONG && L.n2 % 8 == 0) {
-                QParents P;
-                quad_parents(L, C, q.i, q.j, q.kk0, p, [&](int pl, int e) { return LD<ZT>::ld2(pick(C.z, pl), e); },
-                             [&](int pl, int e) { return LD<ZT>::ld(pick(C.z, pl), e); }, P);
-                quad_nbr_sum_pro(L, q, p, code, v4, v1, P, ns);
-            } else if (MODE == HS_PROLONG)
-                quad_nbr_sum<true>(L, q, p, code, v4, v1,
-                                   [&](int i, int j, int k) {
-                                       const int I = i >> 1, J = j >> 1, K = k >> 1;
-                                       return LD<ZT>::ld(pick(C.z, (I + J + K) & 1), (I * C.n1 + J) * C.H + (K >> 1));
-                                   }, ns);
-            else
-                quad_nbr_sum<false>(L, q, p, code, v4, v1, NoParent(), ns);
-        }
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            rv[m] = (rv[m] - mean) * zsc;
-            zn[m] = (code[m] & CELL_FLUID)
-                        ? (rv[m] + ns[m]) / nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + p)
-                        : 0.0f;
-            if (MODE == HS_ZR && (code[m] & CELL_FLUID)) zr += (double)zn[m] * (double)rv[m];
-        }
-        Zs<ZT>::st4(zs, q.t0, zn);
-        if (MODE == HS_ZR) {
-            unsigned co[4];
-            quad_codes<SOLID>(L, oc, q, p ^ 1, co);
-            float ro[4], zz[4];
-            if (level0) LD<float>::ld4(pick(L.r, oc), q.t0, ro);
-            else LD<ZT>::ld4(pick(L.r, oc), q.t0, ro);
-            LD<ZT>::ld4(zo, q.t0, zz);
-#pragma unroll
-            for (int m = 0; m < 4; m++)
-                if (co[m] & CELL_FLUID) zr += (double)zz[m] * (double)((ro[m] - mean) * zsc);
-        }
-    }
-}
-
-// k_restrict4's arithmetic on slots t0, t0 + stride, ...
-template <template <class> class LD, bool SOLID, class ZT>
-EDGE_D void co_restrict(const G& g, const Lvl& F, const Lvl& C, int level0, float mean, float zsc, bool first,
-                        int t0, int stride) {
-    const int nq = F.H >> 2;
-    for (int t = t0; t < C.n0 * C.n1 * nq; t += stride) {
-        const int rowc = fdiv(t, F.dQ);
-        const int K0 = (t - rowc * nq) << 2;
-        const int I = fdiv(rowc, C.d1);
-        const int J = rowc - I * C.n1;
-        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int b = 0; b < 2; b++) {
-                const int i = 2 * I + a, j = 2 * J + b;
-                const Quad q{i, j, K0, (i * F.n1 + j) * F.H + K0};
-                const int c0 = (i + j) & 1;
-#pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    const int pl = c0 ^ h;
-                    unsigned code[4];
-                    quad_codes<SOLID>(F, pl, q, h, code);
-                    const float* zo = pick(F.z, pl ^ 1);
-                    float ns[4], zc[4], rc[4];
-                    quad_nbr_sum<false>(
-                        F, q, h, code, [&](int e, float(&o)[4]) { LD<ZT>::ld4(zo, e, o); },
-                        [&](int e) { return LD<ZT>::ld(zo, e); }, NoParent(), ns);
-                    LD<ZT>::ld4(pick(F.z, pl), q.t0, zc);
-                    if (level0) LD<float>::ld4(pick(F.r, pl), q.t0, rc);
-                    else LD<ZT>::ld4(pick(F.r, pl), q.t0, rc);
-#pragma unroll
-                    for (int m = 0; m < 4; m++) {
-                        if (!(code[m] & CELL_FLUID)) continue;
-                        float nf = nf_of<SOLID>(g.walls, F, code[m], i, j, 2 * (K0 + m) + h);
-                        float az = __fsub_rn(__fmul_rn(nf, zc[m]), ns[m]);
-                        float res = (rc[m] - mean) * zsc - az;
-                        acc[m] += res * 0.5f;
-                    }
-                }
-            }
-        const int ecb = (I * C.n1 + J) * C.H + (K0 >> 1);
-        const int pa = (I + J) & 1;
-        Zs<ZT>::st2(pick(C.r, pa), ecb, acc[0], acc[2]);
-        Zs<ZT>::st2(pick(C.r, pa ^ 1), ecb, acc[1], acc[3]);
-        if (first) {
-            const int m0 = pa;
-            float zz[2];
-#pragma unroll
-            for (int u = 0; u < 2; u++) {
-                const int m = m0 + 2 * u, K = K0 + m;
-                const unsigned cc = SOLID ? (unsigned)C.code[0][ecb + u] : range_code(C, I, J, K);
-                zz[u] = (cc & CELL_FLUID) ? (acc[m] + 0.0f) / nf_of<SOLID>(g.walls, C, cc, I, J, K) : 0.0f;
-            }
-            Zs<ZT>::st2(C.z[0], ecb, zz[0], zz[1]);
-        }
-    }
-}
-
-// k_cg_ap4's arithmetic (p = z + beta p, A p, p.Ap) on slots t0, t0 + stride, ...
-template <template <class> class LD, bool SOLID, class ZT>
-EDGE_D void co_ap(const G& g, const Lvl& L, const Fine& f, int pc, bool first, float beta, float zinv, int t0,
-                  int stride, double& pap) {
-    const int nq = L.n0 * L.n1 * (L.H >> 2);
-    for (int t = t0; t < nq; t += stride) {
-        const Quad q = quad_of(L, t);
-        const int c0 = (q.i + q.j) & 1;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int pl = c0 ^ h;
-            unsigned code[4];
-            quad_codes<SOLID>(L, pl, q, h, code);
-            const float* zo = pick(L.z, pl ^ 1);
-            const float* po = pick2(f.p, pc, pl ^ 1);
-            auto pn4 = [&](const float* zz, const float* pp, int e, float(&o)[4]) {
-                LD<ZT>::ld4(zz, e, o);
-#pragma unroll
-                for (int m = 0; m < 4; m++) o[m] = o[m] * zinv;
-                if (!first) {
-                    float b[4];
-                    LD<float>::ld4(pp, e, b);
-#pragma unroll
-                    for (int m = 0; m < 4; m++) o[m] = __fadd_rn(o[m], __fmul_rn(beta, b[m]));
-                }
-            };
-            float pe[4], ns[4];
-            pn4(pick(L.z, pl), pick2(f.p, pc, pl), q.t0, pe);
-            quad_nbr_sum<false>(
-                L, q, h, code, [&](int e, float(&o)[4]) { pn4(zo, po, e, o); },
-                [&](int e) {
-                    const float ze = LD<ZT>::ld(zo, e) * zinv;
-                    return first ? ze : __fadd_rn(ze, __fmul_rn(beta, LD<float>::ld(po, e)));
-                },
-                NoParent(), ns);
-#pragma unroll
-            for (int m = 0; m < 4; m++) {
-                if (code[m] & CELL_FLUID) {
-                    float nf = nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
-                    float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
-                    pap += (double)pe[m] * (double)ape;
-                } else {
-                    pe[m] = 0.0f;
-                }
-            }
-            st4(pick2(f.p, pc ^ 1, pl) + q.t0, pe);
-        }
-    }
-}
-
-// k_cg_xr4's arithmetic (x += alpha p, r -= alpha A p, r.r, sum r)
-template <template <class> class LD, bool SOLID>
-EDGE_D void co_xr(const G& g, const Lvl& L, const Fine& f, int pc, bool first, float alpha, float mean, int t0,
-                  int stride, double (&v)[2]) {
-    const int nq = L.n0 * L.n1 * (L.H >> 2);
-    for (int t = t0; t < nq; t += stride) {
-        const Quad q = quad_of(L, t);
-        const int c0 = (q.i + q.j) & 1;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int pl = c0 ^ h;
-            unsigned code[4];
-            quad_codes<SOLID>(L, pl, q, h, code);
-            const float* po = pick2(f.p, pc, pl ^ 1);
-            float pe[4], ns[4], r[4], x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            LD<float>::ld4(pick2(f.p, pc, pl), q.t0, pe);
-            ld4c(pick(L.r, pl) + q.t0, r);
-            if (!first) ld4c(pick(f.x, pl) + q.t0, x);
-            quad_nbr_sum<false>(
-                L, q, h, code, [&](int e, float(&o)[4]) { LD<float>::ld4(po, e, o); },
-                [&](int e) { return LD<float>::ld(po, e); }, NoParent(), ns);
-#pragma unroll
-            for (int m = 0; m < 4; m++) {
-                r[m] = r[m] - mean;
-                if (code[m] & CELL_FLUID) {
-                    x[m] = first ? __fmul_rn(alpha, pe[m]) : __fadd_rn(x[m], __fmul_rn(alpha, pe[m]));
-                    float nf = nf_of<SOLID>(g.walls, L, code[m], q.i, q.j, 2 * (q.kk0 + m) + h);
-                    float ape = __fsub_rn(__fmul_rn(nf, pe[m]), ns[m]);
-                    r[m] = __fsub_rn(r[m], __fmul_rn(alpha, ape));
-                    v[0] += (double)r[m] * (double)r[m];
-                }
-                v[1] += r[m];
-            }
-            st4(pick(f.x, pl) + q.t0, x);
-            st4(pick(L.r, pl) + q.t0, r);
-        }
-    }
-}
-
-constexpr int kCoopThreads = 256;
-
-// a phase boundary; an aborted launch ends the loop and returns
-#define COOP_SYNC(expr)                                  \
-    do {                                                 \
-        if (!(expr)) {                                   \
-            if (threadIdx.x == 0) set_cond(g, 0);        \
-            return;                                      \
-        }                                                \
-    } while (0)
-
-// the phases' load policy: through L2 (Zc), or weak L1-cached loads (Zw)
-template <bool WEAK>
-struct LdSel {
-    template <class T>
-    using type = Zc<T>;
-};
-template <>
-struct LdSel<true> {
-    template <class T>
-    using type = Zw<T>;
-};
-#define LDT LdSel<WEAK>::template type
-
-template <bool SOLID, class ZT, bool WEAK>
-__global__ void __launch_bounds__(kCoopThreads, WEAK ? 4 : 3) k_coop(G g, Levels a, Fine f, int mode) {
-    __shared__ Lvl sl[16];
-    __shared__ CoopBar bar;
-    count_launch(g.st);
-    copy_levels(a, sl);
-    SolveState* st = g.st;
-    if (threadIdx.x == 0) {
-        bar.gen = ld_acquire_u32(&st->bar_gen);
-        bar.ok = *((volatile unsigned*)&st->bar_abort) == 0;
-    }
-    __syncthreads();
-    COOP_SYNC(bar.ok);
-    const int lc = a.lc;
-    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-    G gq = g;
-    gq.use_cond = 0;  // the loop condition is set once, below
-    if (mode == COOP_ITER) {
-        // a launch after the loop ended (the stepwise solve) does nothing; no
-        // block writes the status before the first barrier of this launch
-        if (st_ldi(&st->status) != ST_RUNNING) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
-            return;
-        }
-        // up sweeps of the V-cycle whose coarse group k_coarse just ran
-        for (int l = lc - 1; l >= 0; l--) {
-            const Lvl& L = sl[l];
-            const Lvl& C = sl[l + 1];
-            const int l0 = l == 0;
-            const float mean = l0 ? st_ldf(&st->mean) : 0.0f, zsc = l0 ? st_ldf(&st->zsc) : 1.0f;
-            double zr = 0.0;
-            co_sweep<LDT, HS_PROLONG, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
-            COOP_SYNC(coop_sync(st, bar));
-            co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
-            COOP_SYNC(coop_sync(st, bar));
-            co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
-            COOP_SYNC(coop_sync(st, bar));
-            if (l > 0) {
-                co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
-                COOP_SYNC(coop_sync(st, bar));
-            } else {
-                co_sweep<LDT, HS_ZR, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
-                double v[1] = {zr};
-                COOP_SYNC(coop_reduce<1>(g, bar, v, [&](double (&w)[1]) {
-                    zr_epilogue(gq, w[0]);
-                    if (st->it > st->max_iters + 8) st->status = ST_NOCONV;
-                }));
-            }
-        }
-        if (st_ldi(&st->status) != ST_RUNNING) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
-            return;
-        }
-        const Lvl& L = sl[0];
-        {
-            const int pc = st_ldi(&st->pcur);
-            const bool first = st_ldi(&st->it) == 0;
-            const float beta = st_ldf(&st->beta), zinv = st_ldf(&st->zinv);
-            double v[1] = {0.0};
-            co_ap<LDT, SOLID, ZT>(g, L, f, pc, first, beta, zinv, t0, stride, v[0]);
-            COOP_SYNC(coop_reduce<1>(g, bar, v, [&](double (&w)[1]) {
-                double pAp = (double)(float)w[0];
-                st->pAp = pAp;
-                st->alpha = (float)(st->zTr / (pAp + 1e-12));
-                st->pcur = pc ^ 1;
-            }));
-        }
-        {
-            const int pc = st_ldi(&st->pcur);
-            const bool first = st_ldi(&st->it) == 0;
-            const float alpha = st_ldf(&st->alpha), mean = st_ldf(&st->mean);
-            double v[2] = {0.0, 0.0};
-            co_xr<LDT, SOLID>(g, L, f, pc, first, alpha, mean, t0, stride, v);
-            COOP_SYNC(coop_reduce<2>(g, bar, v, [&](double (&w)[2]) {
-                double rTr = (double)(float)w[0];
-                st->rTr = rTr;
-                st->rsum = w[1];
-                st->x_valid = 1;
-                st->mean = st->all_neumann ? (float)(w[1] / ((double)L.n0 * L.n1 * L.n2)) : 0.0f;
-                set_zscale(st, rTr, (double)L.n0 * L.n1 * L.n2);
-                if (!(rTr == rTr) || rTr > 1e300) st->status = ST_NAN;
-                else if (rTr < st->tol) st->status = ST_CONVERGED;
-            }));
-        }
-        if (st_ldi(&st->status) != ST_RUNNING) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
-            return;
-        }
-    }
-    // down sweeps and restrictions of the next V-cycle, levels 0..lc-1
-    for (int l = 0; l < lc; l++) {
-        const Lvl& L = sl[l];
-        const Lvl& C = sl[l + 1];
-        const int l0 = l == 0;
-        const float mean = l0 ? st_ldf(&st->mean) : 0.0f, zsc = l0 ? st_ldf(&st->zsc) : 1.0f;
-        double zr = 0.0;
-        if (l0) {
-            co_sweep<LDT, HS_FIRST, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
-            COOP_SYNC(coop_sync(st, bar));
-        }
-        co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
-        COOP_SYNC(coop_sync(st, bar));
-        co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 0, l0, mean, zsc, t0, stride, zr);
-        COOP_SYNC(coop_sync(st, bar));
-        co_sweep<LDT, HS_PLAIN, SOLID, ZT>(g, L, C, 1, l0, mean, zsc, t0, stride, zr);
-        COOP_SYNC(coop_sync(st, bar));
-        co_restrict<LDT, SOLID, ZT>(g, L, C, l0, mean, zsc, l + 1 < lc, t0, stride);
-        if (l + 1 < lc) COOP_SYNC(coop_sync(st, bar));
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 1);
-}
-#undef LDT
-
 // mgpcg.py:406-432 subtract_grad_p (p = x, get_result mgpcg.py:77-85) + the
 // wall part of the final apply_bc; Poisson_with_buffer's force (mgpcg.py:448-479).
 // One thread per slot: the faces on the low side of its two cells in each
@@ -2196,6 +1695,10 @@ __global__ void __launch_bounds__(256) k_grad_p(G g, Lvl L, Fine f, Faces U) {
 
 // red-black planes <-> lexicographic field of one level; `valid` (may be
 // NULL) gates the planes' content (x before the first update reads as 0)
+__global__ void k_set_restart(SolveState* st) {
+    if (threadIdx.x == 0) st->restart = 1;
+}
+
 // zsc of an FP16 solver from the RMS of level 0's r planes (V-cycle calls)
 __global__ void __launch_bounds__(256) k_zscale(G g, Lvl L) {
     double v[1] = {0.0};
@@ -2634,98 +2137,6 @@ void enqueue_iteration(const Ctx& c, bool solid, cudaStream_t stream) {
     enqueue_vcycle(c, solid, stream, true);
 }
 
-// The cooperative path (k_coop): taken when levels 0..lc-1 all run the
-// four-slot kernels and the device launches a cooperative grid of at least
-// one block per SM; EDGE_MGPCG_COOP=0 selects the per-level kernels.  The
-// grid is every block the device holds at once (occupancy x SMs, at most
-// kMaxBlocks, the capacity of the reduction partials).
-template <bool S, class ZT, bool W>
-static int coop_grid_of() {
-    int dev = 0, sms = 0, per_sm = 0, coop_ok = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
-        cudaDeviceGetAttribute(&coop_ok, cudaDevAttrCooperativeLaunch, dev) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop<S, ZT, W>, kCoopThreads, 0) != cudaSuccess) {
-        (void)cudaGetLastError();
-        return 0;
-    }
-    if (!coop_ok || per_sm < 1) return 0;
-    return std::min(per_sm * sms, kMaxBlocks);
-}
-
-void plan_coop(Ctx& c, bool solid) {
-    c.coop = 0;
-    c.coop_grid = 0;
-    const char* env = getenv("EDGE_MGPCG_COOP");
-    if (env && env[0] == '0') return;
-    const Levels& V = c.lv;
-    if (V.lc < 1) return;
-    for (int l = 0; l < V.lc; l++)
-        if (!V.lv[l].vec) return;
-    const bool weak = env && env[0] == '2';
-    int grid = 0;
-    if (weak) {
-        if (c.ztype == 1) grid = solid ? coop_grid_of<true, __nv_bfloat16, true>() : coop_grid_of<false, __nv_bfloat16, true>();
-        else if (c.ztype == 2) grid = solid ? coop_grid_of<true, __half, true>() : coop_grid_of<false, __half, true>();
-        else grid = solid ? coop_grid_of<true, float, true>() : coop_grid_of<false, float, true>();
-    } else {
-        if (c.ztype == 1) grid = solid ? coop_grid_of<true, __nv_bfloat16, false>() : coop_grid_of<false, __nv_bfloat16, false>();
-        else if (c.ztype == 2) grid = solid ? coop_grid_of<true, __half, false>() : coop_grid_of<false, __half, false>();
-        else grid = solid ? coop_grid_of<true, float, false>() : coop_grid_of<false, float, false>();
-    }
-    if (grid < 1) return;
-    c.coop = weak ? 2 : 1;
-    c.coop_grid = grid;
-}
-
-template <bool S, class ZT>
-static void launch_coop(const Ctx& c, cudaStream_t stream, int mode) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c.coop_grid);
-    cfg.blockDim = dim3(kCoopThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    if (c.coop == 2) cudaLaunchKernelEx(&cfg, k_coop<S, ZT, true>, c.g, c.lv, c.f, mode);
-    else cudaLaunchKernelEx(&cfg, k_coop<S, ZT, false>, c.g, c.lv, c.f, mode);
-}
-
-template <bool S, class ZT>
-static void coop_t(const Ctx& c, cudaStream_t stream, int mode) {
-    if (mode == COOP_ITER) {
-        // the coarse group of the V-cycle whose down half the previous
-        // launch ran; inside the loop the solve is known to be running
-        G gc = c.g;
-        gc.nochk = 1;
-        launch_pdl(k_coarse<false, S, ZT>, 1, 1024, c.csmem, stream, gc, c.lv);
-    }
-    launch_coop<S, ZT>(c, stream, mode);
-}
-
-// k_coop(DOWN) at the end of the set-up, or one loop iteration
-// (k_coarse + k_coop(ITER))
-void enqueue_coop(const Ctx& c, bool solid, cudaStream_t stream, int mode) {
-    if (c.ztype == 1) {
-        if (solid) coop_t<true, __nv_bfloat16>(c, stream, mode);
-        else coop_t<false, __nv_bfloat16>(c, stream, mode);
-    } else if (c.ztype == 2) {
-        if (solid) coop_t<true, __half>(c, stream, mode);
-        else coop_t<false, __half>(c, stream, mode);
-    } else {
-        if (solid) coop_t<true, float>(c, stream, mode);
-        else coop_t<false, float>(c, stream, mode);
-    }
-}
-
-// one iteration of the CG loop on either path
-void enqueue_loop_body(const Ctx& c, bool solid, cudaStream_t stream) {
-    if (c.coop) enqueue_coop(c, solid, stream, COOP_ITER);
-    else enqueue_iteration(c, solid, stream);
-}
-
 // set-up kernels of Poisson / solve (everything before the CG loop)
 void enqueue_setup(Solver* s, Faces U, const float* rhs, double abs_tol, double rel_tol, int max_iters,
                    cudaStream_t cs, bool stepwise = false) {
@@ -2750,14 +2161,12 @@ void enqueue_setup(Solver* s, Faces U, const float* rhs, double abs_tol, double 
             k_codes<<<rgrid((long long)V.n0 * V.n1 * V.n2), 256, 0, cs>>>(c.g, V);
         }
     }
-    // fresh reduction counters and grid barrier
-    cudaMemsetAsync(c.g.st->counter, 0, offsetof(SolveState, kernels) - offsetof(SolveState, counter), cs);
+    cudaMemsetAsync(c.g.st->counter, 0, sizeof(c.g.st->counter), cs);  // fresh reduction counters
     if (s->solid) k_setup_rhs<true><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
     else k_setup_rhs<false><<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f, U, rhs, abs_tol, rel_tol, max_iters);
     if (s->solid && !rhs) k_solid_fix<<<rgrid(L0.P), 256, 0, cs>>>(c.g, L0, c.f);
-    if (c.coop) enqueue_coop(c, s->solid, cs, COOP_DOWN);      // the first V-cycle's down half
-    else if (stepwise) enqueue_step_pl(c, s->solid, cs, true);  // the same on the per-level kernels
-    else enqueue_vcycle(c, s->solid, cs, true);               // first preconditioner application + z.r + tol
+    if (stepwise) enqueue_step_pl(c, s->solid, cs, true);  // the stepwise solve: the first V-cycle's descent
+    else enqueue_vcycle(c, s->solid, cs, true);          // first preconditioner application + z.r + tol
 }
 
 // gradient update (Poisson) or the solution copy (solve)
@@ -2812,12 +2221,6 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     CK(cudaGraphAddNode(&cnode, graph, &leaf, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     cudaGraph_t b2;
-    if (s->ctx.coop) {
-        //    k_coarse + k_coop(ITER), which sets the loop condition itself
-        CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        enqueue_coop(s->ctx, s->solid, cs, COOP_ITER);
-        CK(cudaStreamEndCapture(cs, &b2));
-    } else {
     //    the CG kernels, then if (still running) { V-cycle }: the V-cycle's
     //    kernels are captured with nochk (see stopped())
     cudaGraphConditionalHandle vh;
@@ -2850,7 +2253,6 @@ int build_graph(Solver* s, Faces U, const float* rhs, float* xout, double abs_to
     enqueue_vcycle(vc, s->solid, cs, true);
     CK(cudaStreamEndCapture(cs, &b2));
     s->ctx.g.use_vcond = 0;  // launches outside this graph set no IF condition
-    }
     // 3) finish
     CK(cudaStreamBeginCaptureToGraph(cs, graph, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal));
     enqueue_finish(s, U, rhs, xout, cs);
@@ -2873,7 +2275,7 @@ int run_solve_eager(Solver* s, Faces U, const float* rhs, float* xout, double ab
         CK(cudaMemcpyAsync(&s->st_host->status, &s->ctx.g.st->status, sizeof(int), cudaMemcpyDeviceToHost, cs));
         CK(cudaStreamSynchronize(cs));
         if (s->st_host->status != ST_RUNNING) break;
-        enqueue_loop_body(s->ctx, s->solid, cs);
+        enqueue_iteration(s->ctx, s->solid, cs);
     }
     enqueue_finish(s, U, rhs, xout, cs);
     return cu(cudaPeekAtLastError());
@@ -2906,7 +2308,6 @@ int status_code(int st) {
     switch (st) {
         case ST_CONVERGED: return EDGE_OK;
         case ST_NAN: return EDGE_ENAN;
-        case ST_TIMEOUT: return EDGE_ETIMEOUT;
         default: return EDGE_ENOCONV;
     }
 }
@@ -2973,7 +2374,6 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
     }
     plan_coarse(c, s->solid);
     if (r == EDGE_OK) r = prepare_coarse_kernels(c);
-    if (r == EDGE_OK) plan_coop(c, s->solid);
     const size_t pa0 = plane_alloc(c.lv.lv[0].P);
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.x[0], 2 * pa0 * sizeof(float));
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.p[0][0], 4 * pa0 * sizeof(float));
@@ -3058,6 +2458,13 @@ int edge_mgpcg_result(void* handle, int* iters, double* rTr, int* status, void* 
     if (status)
         *status = status_code(st.status);
     return EDGE_OK;
+}
+
+int edge_mgpcg_restart(void* handle, void* stream) {
+    if (!handle) return EDGE_EINVAL;
+    Solver* s = (Solver*)handle;
+    k_set_restart<<<1, 32, 0, (cudaStream_t)stream>>>(s->ctx.g.st);
+    return cu(cudaPeekAtLastError());
 }
 
 int edge_mgpcg_progress(void* handle, int* iters, double* rTr, int* running, void* stream) {
@@ -3215,22 +2622,7 @@ int edge_mgpcg_solve_iter(void* handle, void* stream) {
     c.g.use_cond = 0;
     c.g.use_vcond = 0;
     c.g.nochk = 0;
-    const int t = c.ztype;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (!c.coop) {
-        enqueue_step_pl(c, s->solid, st, false);
-        return cu(cudaPeekAtLastError());
-    }
-    if (t == 1) {
-        if (s->solid) launch_coop<true, __nv_bfloat16>(c, st, COOP_ITER);
-        else launch_coop<false, __nv_bfloat16>(c, st, COOP_ITER);
-    } else if (t == 2) {
-        if (s->solid) launch_coop<true, __half>(c, st, COOP_ITER);
-        else launch_coop<false, __half>(c, st, COOP_ITER);
-    } else {
-        if (s->solid) launch_coop<true, float>(c, st, COOP_ITER);
-        else launch_coop<false, float>(c, st, COOP_ITER);
-    }
+    enqueue_step_pl(c, s->solid, (cudaStream_t)stream, false);
     return cu(cudaPeekAtLastError());
 }
 

@@ -18,11 +18,11 @@ inline int st(void) {
     return e == cudaSuccess ? EDGE_OK : (int)e;
 }
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
-// EDGE_P2G_DIRECT=1: one global atomic per particle and tap (the plain
-// scatter, for comparison); default: the shared-memory staged scatter
+// EDGE_P2G_TILE=1: the shared-memory staged scatter; default: one global
+// atomic per particle and tap
 inline bool p2g_direct() {
-    static const bool d = getenv("EDGE_P2G_DIRECT") && getenv("EDGE_P2G_DIRECT")[0] == '1';
-    return d;
+    static const bool t = getenv("EDGE_P2G_TILE") && getenv("EDGE_P2G_TILE")[0] == '1';
+    return !t;
 }
 
 // lp.py:6-29 update_particles_acc

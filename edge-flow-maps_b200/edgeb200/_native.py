@@ -21,7 +21,6 @@ EDGE_ENOCONV = -3
 EDGE_ENAN = -4
 EDGE_ESTALL = -5
 EDGE_ESTATE = -6
-EDGE_ETIMEOUT = -7
 
 HERMITE_FD = 0
 HERMITE_GARM = 1

@@ -79,6 +79,10 @@ class Projection:
         N.call("edge_mgpcg_result", self._h, ctypes.byref(it), ctypes.byref(rtr), ctypes.byref(st), stream())
         return it.value, rtr.value, st.value
 
+    def restart(self):
+        """The next CG update of a stepwise solve restarts the recursion."""
+        N.call("edge_mgpcg_restart", self._h, stream())
+
     def progress(self):
         """(iterations, r.r, whether the CG loop is still running);
         synchronises the stream."""

@@ -423,7 +423,8 @@ class LearnedCoarsePCG:
     a few hundred times fewer voxels than the fine grid.
 
     Fallback: when an iteration reduces |r| by less than `stall`, the rest of
-    the solve takes the built-in coarse group (plain MGPCG).  One iteration
+    the solve takes the built-in coarse group (plain MGPCG), the CG recursion
+    restarted (p = z) from the current iterate.  One iteration
     (coarse step + CG iteration) is a CUDA graph replayed per iteration; the
     host reads the status (and r.r for the stall test) between iterations."""
 
@@ -499,6 +500,9 @@ class LearnedCoarsePCG:
             if not running:
                 break
             if mode == "net" and prev is not None and rtr > self.stall * self.stall * prev:
+                # the built-in coarse group from here on, the recursion
+                # restarted from the current iterate (p = z)
                 mode, fell_back = "vcycle", True
+                P.restart()
             prev = rtr
         return fell_back

@@ -37,7 +37,6 @@ extern "C" {
 #define EDGE_ENAN (-4)       /* non-finite residual */
 #define EDGE_ESTALL (-5)     /* residual stalled (flexible PCG fallback taken) */
 #define EDGE_ESTATE (-6)     /* call order / handle state error */
-#define EDGE_ETIMEOUT (-7)   /* a bounded wait inside a solver launch ran out of time */
 
 /* Hermite variants (sim/hermite.py) */
 #define EDGE_HERMITE_FD 0    /* interp_(grad_)hermite_fd_unroll, hermite.py:65-295 (ED4) */
@@ -301,6 +300,9 @@ int edge_mgpcg_poisson_begin(void *handle, float *ux, float *uy, float *uz, doub
                              int max_iters, void *stream);
 int edge_mgpcg_poisson_end(void *handle, float *ux, float *uy, float *uz, float *fx, float *fy, float *fz,
                            void *stream);
+/* Restart the CG recursion of a stepwise solve: the next iteration takes
+ * p = z (beta = 0), e.g. after the caller changes its coarse solver. */
+int edge_mgpcg_restart(void *handle, void *stream);
 /* Iterations, r.r and whether the CG loop still runs (1) or has ended (0);
  * synchronises the stream. */
 int edge_mgpcg_progress(void *handle, int *iters, double *rTr, int *running, void *stream);

@@ -259,55 +259,6 @@ def test_mixed_precision_vs_fp64(precision, vtol, amp):
     assert errs[0] < 1e-3 and errs[1] < 3 * errs[0] + 1e-6, errs
 
 
-def _coop_case(res, base_level, solid, precision, poisson):
-    rng = np.random.default_rng(3)
-    mask = bvel = None
-    if solid:
-        m = np.zeros(res, np.int32)
-        m[res[0] // 3:res[0] // 3 + 6, res[1] // 3:2 * res[1] // 3, res[2] // 4:res[2] // 2] = 1
-        mask, bvel = torch.from_numpy(m).cuda(), torch.zeros(res + (3,), device="cuda")
-        bvel[..., 0] = 0.25
-    if poisson:
-        u = [rng.normal(size=s).astype(np.float32) for s in O.face_shapes(res)]
-        return mask, bvel, u
-    b = rng.normal(size=res).astype(np.float32)
-    b -= b.mean()
-    return mask, bvel, b
-
-
-@pytest.mark.parametrize("res,base_level,solid,precision", [((256, 128, 128), 2, False, 0),
-                                                            ((128, 64, 64), 1, False, 0),
-                                                            ((128, 64, 64), 1, True, 0),
-                                                            ((64, 32, 32), 2, False, 1),
-                                                            ((128, 64, 64), 2, True, 1)])
-def test_cooperative_iteration_matches_per_level_kernels(res, base_level, solid, precision, monkeypatch):
-    """The cooperative iteration kernel (k_coarse + k_coop per CG iteration,
-    grid barriers between phases) runs the per-level kernels' arithmetic:
-    the projected velocity, the solution of a solve and the iteration counts
-    are identical bit for bit (the reductions' partials are summed in another
-    block order, in float64, and rounded to float32 before use)."""
-    from edgeb200.projection import Projection
-    mask, bvel, u = _coop_case(res, base_level, solid, precision, True)
-    _, _, b = _coop_case(res, base_level, solid, precision, False)
-    out = []
-    for flag in ("1", "2", "0"):
-        monkeypatch.setenv("EDGE_MGPCG_COOP", flag)
-        P = Projection(res, base_level=base_level, mask=mask, bvel=bvel, precision=precision)
-        ug = [T_(a) for a in u]
-        P.poisson(*ug)
-        r1 = P.result()
-        x = torch.zeros(res, device="cuda")
-        P.solve(T_(b), x, abs_tol=0.0, rel_tol=1e-6)
-        out.append(([N_(t) for t in ug], N_(x), r1, P.result()))
-        P.close()
-    assert out[-1][2][2] == 0
-    for o in out[:-1]:
-        assert o[2] == out[-1][2] and o[3] == out[-1][3]
-        for a, c in zip(o[0], out[-1][0]):
-            np.testing.assert_array_equal(a, c)
-        np.testing.assert_array_equal(o[1], out[-1][1])
-
-
 _EAGER_SCRIPT = r"""
 import sys
 import numpy as np, torch
@@ -327,21 +278,20 @@ np.savez(sys.argv[1], ux=u[0].cpu().numpy(), uy=u[1].cpu().numpy(), uz=u[2].cpu(
 
 def test_host_driven_loop_matches_graph(tmp_path):
     """The host-driven CG loop (EDGE_MGPCG_EAGER=1: one status read per
-    iteration), on the cooperative and on the per-level path, gives the
-    graph-captured solve's result bit for bit.  The switch is read once per
-    process, so each runs in a child process."""
+    iteration) gives the graph-captured solve's result bit for bit.  The
+    switch is read once per process, so each runs in a child process."""
     import os
     import subprocess
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     pkg = os.path.join(root, "edge-flow-maps_b200")
     outs = {}
-    for eager, coop in (("0", "1"), ("1", "1"), ("1", "0")):
-        path = str(tmp_path / f"e{eager}c{coop}.npz")
-        env = dict(os.environ, EDGE_MGPCG_EAGER=eager, EDGE_MGPCG_COOP=coop)
+    for eager in ("0", "1"):
+        path = str(tmp_path / f"e{eager}.npz")
+        env = dict(os.environ, EDGE_MGPCG_EAGER=eager)
         subprocess.run([sys.executable, "-c", _EAGER_SCRIPT, path, pkg, root], env=env, check=True, timeout=600)
-        outs[(eager, coop)] = np.load(path)
-    ref = outs[("0", "1")]
+        outs[eager] = np.load(path)
+    ref = outs["0"]
     assert int(ref["res"][1]) == 0
     for k, d in outs.items():
         for f in ("ux", "uy", "uz", "res", "rtr"):
