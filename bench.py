@@ -638,6 +638,39 @@ def c4_measure(steps=100, precision=2, warm=2):
             "fp64_projection_rel_error_max": max(errs)}
 
 
+def mixed_learned_steps(steps=12, warm=3):
+    """EDGE steps/s of the headline workload with the FP16 V-cycle and the
+    float64 Jacobian composition (precision 2), and with the learned
+    coarse-level solver on top (both projections of every step), next to
+    the float32 steps; CUDA events around `steps` steps after `warm`."""
+    import torch
+    from edgeb200.sim import EdgeSim, four_vortex_init
+    from edgeb200.train_unet import load_params
+    params = load_params(COARSE_WEIGHTS) if os.path.exists(COARSE_WEIGHTS) else None
+    out = {}
+    for name, prec, learned in (("fp32", 0, None), ("mixed_fp16", 2, None), ("learned_fp32", 0, params),
+                                ("learned_mixed_fp16", 2, params)):
+        if name.startswith("learned") and params is None:
+            continue
+        sim = EdgeSim(RES, DX, variant="edge", cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * DX,
+                      base_level=BASE_LEVEL, bfecc_clamp=True, visualize_dt=0.1, packed=True, precision=prec,
+                      learned=learned)
+        u, smoke = four_vortex_init(RES, DX)
+        sim.set_velocity(*u)
+        sim.set_smoke(smoke)
+        sim.proj.poisson(*sim.u)
+        for _ in range(warm):
+            sim.step()
+        torch.cuda.synchronize()
+        ms = _event_ms(lambda: [sim.step() for _ in range(steps)], 1) / steps
+        out[name] = {"ms_per_step": ms, "steps_per_s": 1e3 / ms, "last_solve_iters": sim.proj.result()[0]}
+        if learned is not None:
+            out[name]["fell_back_last_solve"] = bool(sim.learned.fell_back)
+        del sim
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_c4_only(args):
     import torch
     torch.cuda.set_device(0)
@@ -758,6 +791,7 @@ def run_ours(args, rank, world, local_rank):
             del vs
             torch.cuda.empty_cache()
     c2 = c2_measure() if not (args.res or args.no_extras) else None
+    mixed_steps = mixed_learned_steps() if not (args.res or args.no_extras) else None
     pcg = pcg_measure(RES) if not (args.res or args.no_extras) else None
     if pcg is not None:
         pcg["learned"] = learned_measure(RES)
@@ -804,6 +838,7 @@ def run_ours(args, rank, world, local_rank):
             "variants": variants or None,
             "c2_solid_particles": c2,
             "c4_mixed": c4,
+            "precision_steps": mixed_steps,
             "mgpcg_iters": list(iters),
             "clocks": clk.summary(),
             "gpu_launches": launches,

@@ -193,7 +193,9 @@ def evaluate_coarse(params, sizes=((96, 96, 96), (128, 64, 64), (256, 128, 128))
                     precision=0, timing=True):
     """Iterations (and wall time of the stepwise loop) of MGPCG to rel_tol on
     seeded N(0,1) right-hand sides never seen in training, with the built-in
-    coarse group and with the network as the coarse solver."""
+    coarse group, with the network as the coarse solver, and with the
+    coarse-level equation solved exactly (the bound on what any coarse
+    solver can gain)."""
     out = {}
     for res in sizes:
         lg = int(math.log2(min(res)))
@@ -201,7 +203,7 @@ def evaluate_coarse(params, sizes=((96, 96, 96), (128, 64, 64), (256, 128, 128))
         L = LearnedCoarsePCG(P, params)
         x = torch.zeros(res, device="cuda")
         row = {"coarse_dims": list(L.dims)}
-        for mode in ("vcycle", "net"):
+        for mode in ("vcycle", "net", "exact"):
             its, ms, fb = [], [], []
             for sd in seeds:
                 b = random_rhs(res, sd)

@@ -444,12 +444,26 @@ class LearnedCoarsePCG:
             self.P.coarse_get_r(self.r)
             self.net.forward(self.r, self.z)
             self.P.coarse_set_z(self.z)
+        elif mode == "exact":
+            # the coarse-level equation solved to 1e-7 (the best any coarse
+            # solver can do; for measurement, not speed)
+            self.P.coarse_get_r(self.r)
+            self.exact_solver().solve(self.r, self.z, abs_tol=0.0, rel_tol=1e-14, max_iters=400)
+            self.P.coarse_set_z(self.z)
         else:
             self.P.coarse_default()
         self.P.solve_iter()
 
+    def exact_solver(self):
+        if getattr(self, "_exact", None) is None:
+            import math
+            from .projection import Projection
+            lg = int(math.log2(min(self.dims)))
+            self._exact = Projection(self.dims, base_level=max(1, lg - 2))
+        return self._exact
+
     def _run(self, mode):
-        if not self.use_graphs:
+        if not self.use_graphs or mode == "exact":
             self._step(mode)
             return
         g = self.graphs.get(mode)
