@@ -143,7 +143,11 @@ __global__ void __launch_bounds__(kP2GThreads) k_lp_p2g_tile(int nx, int ny, int
     __shared__ float tile[kP2GTile];
     __shared__ int lo_s[9], hi_s[9];
     __shared__ int use_tile;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    // the block's 256 particles are taken lane-major: lane l of warp w takes
+    // particle 8 l + w, so the lanes of a warp hold particles 8 apart (in
+    // the workloads' cell order, one per cell) and their taps hit a face of
+    // the tile at most a few at a time, not all eight particles of a cell
+    const int e = blockIdx.x * blockDim.x + (threadIdx.x & 31) * 8 + (threadIdx.x >> 5);
     float p[3] = {0.f, 0.f, 0.f};
     bool live = e < num;
     if (live) {

@@ -154,7 +154,7 @@ def _config_sims(res, base_level):
     return a, c
 
 
-def train_coarse(sizes=((128, 64, 64), (256, 128, 128)), steps_per_source=850, lr=1e-3, seed=0, params=None,
+def train_coarse(sizes=((128, 64, 64), (256, 128, 128)), steps_per_source=1000, lr=1e-3, seed=0, params=None,
                  log=print):
     """Train the coarse-level network on (r_lc, exact z_lc) pairs from plain
     MGPCG solves of the projections of configurations 1 and 2 at each size.
@@ -162,6 +162,10 @@ def train_coarse(sizes=((128, 64, 64), (256, 128, 128)), steps_per_source=850, l
     pairs = 0
     net = None
     t0 = time.time()
+    # The exact coarse solution is tens of times larger than its right-hand
+    # side (1/lambda_min of the coarse operator); the network learns it
+    # divided by a fixed gain, folded into the last layer afterwards.
+    gain = None
     for res in sizes:
         P = Projection(res, base_level=2)
         level, dims = P.coarse_shape()
@@ -176,7 +180,10 @@ def train_coarse(sizes=((128, 64, 64), (256, 128, 128)), steps_per_source=850, l
                 if float(b.abs().max()) == 0.0:
                     continue
                 for r in coarse_residuals(P, b):
-                    loss = net.train_step(r, exact(r), lr=lr)
+                    z = exact(r)
+                    if gain is None:
+                        gain = float(z.norm() / r.norm())
+                    loss = net.train_step(r, z / gain, lr=lr)
                     pairs += 1
             if k % 100 == 0:
                 log(f"{res} step {k} pairs {pairs} loss {float(loss):.4g} {time.time() - t0:.1f}s")
@@ -186,7 +193,11 @@ def train_coarse(sizes=((128, 64, 64), (256, 128, 128)), steps_per_source=850, l
         torch.cuda.empty_cache()
     if net.timed_out():
         raise RuntimeError("a tensor-core wait gave up during training")
-    return net.params, pairs
+    params = {k: v.clone() for k, v in net.params.items()}
+    params["W5"] *= gain
+    params["b5"] *= gain
+    log(f"output gain {gain:.4g}")
+    return params, pairs
 
 
 def evaluate_coarse(params, sizes=((96, 96, 96), (128, 64, 64), (256, 128, 128)), seeds=(1, 2, 3), rel_tol=1e-6,
@@ -235,7 +246,7 @@ def main(argv=None):
     ap.add_argument("--out", default=None)
     ap.add_argument("--eval", action="store_true", help="report iterations to 1e-6 (with --init: no training)")
     ap.add_argument("--coarse", action="store_true", help="train the coarse-level network (LearnedCoarsePCG)")
-    ap.add_argument("--steps-per-source", type=int, default=850)
+    ap.add_argument("--steps-per-source", type=int, default=1000)
     a = ap.parse_args(argv)
     if a.coarse:
         params = load_params(a.init) if a.init else None
