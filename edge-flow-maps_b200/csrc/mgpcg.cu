@@ -1883,13 +1883,17 @@ void set_level_dims(Lvl& V, int n0, int n1, int n2) {
     V.dQ = make_fdiv((unsigned)std::max(1, V.H / 4));
 }
 
+// A captured solve graph holds every pointer its kernels read or write: the
+// face velocities and forces (Poisson), the right-hand side and the solution
+// (solve), so all of them key it.
 struct GraphKey {
-    const void* a[7];
+    const void* a[8];
     double abs_tol, rel_tol;
     int max_iters;
     bool operator<(const GraphKey& o) const {
-        return std::tie(a[0], a[1], a[2], a[3], a[4], a[5], a[6], abs_tol, rel_tol, max_iters) <
-               std::tie(o.a[0], o.a[1], o.a[2], o.a[3], o.a[4], o.a[5], o.a[6], o.abs_tol, o.rel_tol, o.max_iters);
+        return std::tie(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], abs_tol, rel_tol, max_iters) <
+               std::tie(o.a[0], o.a[1], o.a[2], o.a[3], o.a[4], o.a[5], o.a[6], o.a[7], o.abs_tol, o.rel_tol,
+                        o.max_iters);
     }
 };
 
@@ -2289,7 +2293,8 @@ int run_solve(Solver* s, Faces U, const float* rhs, float* xout, double abs_tol,
     memset(&key, 0, sizeof(key));
     key.a[0] = U.u[0]; key.a[1] = U.u[1]; key.a[2] = U.u[2];
     key.a[3] = U.f[0]; key.a[4] = U.f[1]; key.a[5] = U.f[2];
-    key.a[6] = rhs ? (const void*)rhs : (const void*)xout;
+    key.a[6] = rhs;
+    key.a[7] = xout;
     key.abs_tol = abs_tol; key.rel_tol = rel_tol; key.max_iters = max_iters;
     auto it = s->graphs.find(key);
     cudaGraphExec_t exec;

@@ -323,3 +323,22 @@ def test_refined_solve_reaches_true_tolerance(precision):
     assert true <= 1.01e-6, true
     ref = fp64_solve(P, b.float())
     assert rel_error(x.float(), ref) < 1e-4
+
+
+def test_solve_writes_each_callers_output():
+    """Solves of the same right-hand side into two different output
+    tensors each write their own output (the captured solve graph is keyed
+    by the output pointer as well)."""
+    from edgeb200.projection import Projection
+    res = (64, 32, 32)
+    g = torch.Generator().manual_seed(2)
+    b = torch.randn(res, generator=g)
+    b = (b - b.mean()).cuda()
+    P = Projection(res, base_level=2)
+    x1 = torch.zeros(res, device="cuda")
+    x2 = torch.zeros(res, device="cuda")
+    P.solve(b, x1, abs_tol=0.0, rel_tol=1e-12)
+    P.solve(b, x2, abs_tol=0.0, rel_tol=1e-12)
+    torch.cuda.synchronize()
+    assert float(x2.abs().max()) > 0
+    assert torch.equal(x1, x2)
