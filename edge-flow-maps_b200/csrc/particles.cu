@@ -4,7 +4,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cstdlib>
 
 #include "edge_common.cuh"
 
@@ -18,12 +17,6 @@ inline int st(void) {
     return e == cudaSuccess ? EDGE_OK : (int)e;
 }
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
-// EDGE_P2G_TILE=1: the shared-memory staged scatter; default: one global
-// atomic per particle and tap
-inline bool p2g_direct() {
-    static const bool t = getenv("EDGE_P2G_TILE") && getenv("EDGE_P2G_TILE")[0] == '1';
-    return !t;
-}
 
 // lp.py:6-29 update_particles_acc
 __global__ void k_lp_acc(Mac mac, const float* __restrict__ vel, const float* __restrict__ pos, float* acc, int num,
@@ -114,141 +107,6 @@ __global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float* dx_, float* dy
                 }
             }
         }
-    }
-}
-
-// The same scatter staged through shared memory.  A block takes 256
-// consecutive particles; when the faces they touch (the bounding box of their
-// 4x4x4 stencils, per face grid) fit the block's tile, the block accumulates
-// there with shared-memory atomics and adds each touched face to the global
-// grid once, instead of one global atomic per particle and tap (particles
-// stored in cell order, as the workloads seed them, touch a few hundred faces
-// per block; 256 x 81 taps otherwise).  A block whose particles are spread
-// wider scatters directly.  Same weights and values as k_lp_p2g; only the
-// order of the float additions differs (as between two runs of the atomic
-// scatter).
-constexpr int kP2GThreads = 256;
-constexpr int kP2GTile = 10240;  // floats of shared memory per block (40 KB)
-
-EDGE_D bool p2g_inside(const float (&p)[3], float dx, float Lx, float Ly, float Lz) {
-    return !(p[0] < 3 * dx || p[1] < 3 * dx || p[2] < 3 * dx || p[0] > Lx - 3 * dx || p[1] > Ly - 3 * dx ||
-             p[2] > Lz - 3 * dx);
-}
-
-__global__ void __launch_bounds__(kP2GThreads) k_lp_p2g_tile(int nx, int ny, int nz, float dx, float* dx_, float* dy_,
-                                                             float* dz_, const float* __restrict__ vdiff,
-                                                             const float* __restrict__ pos,
-                                                             const float* __restrict__ rad, int num, float lrad,
-                                                             float Lx, float Ly, float Lz) {
-    __shared__ float tile[kP2GTile];
-    __shared__ int lo_s[9], hi_s[9];
-    __shared__ int use_tile;
-    // the block's 256 particles are taken lane-major: lane l of warp w takes
-    // particle 8 l + w, so the lanes of a warp hold particles 8 apart (in
-    // the workloads' cell order, one per cell) and their taps hit a face of
-    // the tile at most a few at a time, not all eight particles of a cell
-    const int e = blockIdx.x * blockDim.x + (threadIdx.x & 31) * 8 + (threadIdx.x >> 5);
-    float p[3] = {0.f, 0.f, 0.f};
-    bool live = e < num;
-    if (live) {
-        p[0] = pos[3 * e];
-        p[1] = pos[3 * e + 1];
-        p[2] = pos[3 * e + 2];
-        live = p2g_inside(p, dx, Lx, Ly, Lz);
-    }
-    const float g[3] = {p[0] / dx, p[1] / dx, p[2] / dx};
-    // base index of each face grid's stencil (lp.py:130, 139, 148)
-    int base[3][3];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) base[a][c] = (int)(g[c] - ((c == a) ? 0.0f : 0.5f));
-    if (threadIdx.x < 9) {
-        lo_s[threadIdx.x] = 0x7fffffff;
-        hi_s[threadIdx.x] = -0x7fffffff;
-    }
-    __syncthreads();
-    if (live) {
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                atomicMin(&lo_s[3 * a + c], base[a][c] - 1);
-                atomicMax(&hi_s[3 * a + c], base[a][c] + 2);
-            }
-    }
-    __syncthreads();
-    // tile layout: face grid a occupies ext[a] = product of its box sides
-    int off[4];
-    int ext[3][3];
-    off[0] = 0;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        long long v = 1;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            ext[a][c] = hi_s[3 * a + c] >= lo_s[3 * a + c] ? hi_s[3 * a + c] - lo_s[3 * a + c] + 1 : 0;
-            v *= ext[a][c];
-        }
-        off[a + 1] = off[a] + (int)min(v, (long long)kP2GTile + 1);
-    }
-    if (threadIdx.x == 0) use_tile = off[3] <= kP2GTile;
-    __syncthreads();
-    const bool tiled = use_tile;
-    if (tiled)
-        for (int t = threadIdx.x; t < off[3]; t += blockDim.x) tile[t] = 0.0f;
-    __syncthreads();
-    if (live) {
-        const float r = rad[e];
-        const float scale = r * r * r / (lrad * lrad * lrad);
-        float* D[3] = {dx_, dy_, dz_};
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const float offc[3] = {a == 0 ? 0.0f : 0.5f, a == 1 ? 0.0f : 0.5f, a == 2 ? 0.0f : 0.5f};
-            const int n0 = nx + (a == 0), n1 = ny + (a == 1), n2 = nz + (a == 2);
-            const float val = vdiff[3 * e + a];
-            for (int oi = -1; oi < 3; oi++) {
-                const int f0 = base[a][0] + oi;
-                if (f0 < 0 || f0 >= n0) continue;
-                const float wx = N2(g[0] - (float)f0 - offc[0]);
-                if (wx == 0.0f) continue;
-                for (int oj = -1; oj < 3; oj++) {
-                    const int f1 = base[a][1] + oj;
-                    if (f1 < 0 || f1 >= n1) continue;
-                    const float wy = N2(g[1] - (float)f1 - offc[1]);
-                    if (wy == 0.0f) continue;
-                    for (int ok = -1; ok < 3; ok++) {
-                        const int f2 = base[a][2] + ok;
-                        if (f2 < 0 || f2 >= n2) continue;
-                        const float w = wx * wy * N2(g[2] - (float)f2 - offc[2]);
-                        if (w == 0.0f) continue;
-                        const float add = val * w * scale;
-                        if (tiled) {
-                            const int t = off[a] + ((f0 - lo_s[3 * a]) * ext[a][1] + (f1 - lo_s[3 * a + 1])) * ext[a][2] +
-                                          (f2 - lo_s[3 * a + 2]);
-                            atomicAdd(&tile[t], add);
-                        } else {
-                            atomicAdd(D[a] + idx3(f0, f1, f2, n1, n2), add);
-                        }
-                    }
-                }
-            }
-        }
-    }
-    if (!tiled) return;
-    __syncthreads();
-    float* D[3] = {dx_, dy_, dz_};
-    for (int t = threadIdx.x; t < off[3]; t += blockDim.x) {
-        const float v = tile[t];
-        if (v == 0.0f) continue;
-        const int a = t < off[1] ? 0 : (t < off[2] ? 1 : 2);
-        int q = t - off[a];
-        const int k = q % ext[a][2];
-        q /= ext[a][2];
-        const int j = q % ext[a][1];
-        const int i = q / ext[a][1];
-        const int n1 = ny + (a == 1), n2 = nz + (a == 2);
-        atomicAdd(D[a] + idx3(lo_s[3 * a] + i, lo_s[3 * a + 1] + j, lo_s[3 * a + 2] + k, n1, n2), v);
     }
 }
 
@@ -349,12 +207,8 @@ int edge_lp_p2g(int nx, int ny, int nz, float dx, float* dragx, float* dragy, fl
     if ((e = cudaMemsetAsync(dragy, 0, (size_t)nx * (ny + 1) * nz * 4, s)) != cudaSuccess) return (int)e;
     if ((e = cudaMemsetAsync(dragz, 0, (size_t)nx * ny * (nz + 1) * 4, s)) != cudaSuccess) return (int)e;
     if (num == 0) return EDGE_OK;
-    if (p2g_direct())
-        k_lp_p2g<<<grid_for(num), 256, 0, s>>>(nx, ny, nz, dx, dragx, dragy, dragz, vdiff, pos, rad, num, laden_radius,
-                                               Lx, Ly, Lz);
-    else
-        k_lp_p2g_tile<<<grid_for(num, kP2GThreads), kP2GThreads, 0, s>>>(nx, ny, nz, dx, dragx, dragy, dragz, vdiff,
-                                                                          pos, rad, num, laden_radius, Lx, Ly, Lz);
+    k_lp_p2g<<<grid_for(num), 256, 0, s>>>(nx, ny, nz, dx, dragx, dragy, dragz, vdiff, pos, rad, num, laden_radius, Lx,
+                                           Ly, Lz);
     return st();
 }
 
