@@ -754,7 +754,7 @@ __global__ void __launch_bounds__(128) k_advect_sl(Mac mac, float dt, float* ox,
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
     FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
-    float p1[3], v1[3], v2[3], v3[3], v4[3], v5[3], q[3];
+    float p1[3], v1[3], v2[3], v3[3], v4[3], q[3];
     face_pos(f.axis, f.i, f.j, f.k, mac.dx, p1);
     mac_sample<false>(mac, p1, v1, nullptr);
     for (int c = 0; c < 3; c++) q[c] = p1[c] - v1[c] * dt * 0.5f;
@@ -764,9 +764,9 @@ __global__ void __launch_bounds__(128) k_advect_sl(Mac mac, float dt, float* ox,
     for (int c = 0; c < 3; c++) q[c] = p1[c] - v3[c] * dt;
     mac_sample<false>(mac, q, v4, nullptr);
     for (int c = 0; c < 3; c++) q[c] = p1[c] - (v1[c] + 2.0f * v2[c] + 2.0f * v3[c] + v4[c]) / 6.0f * dt;
-    mac_sample<false>(mac, q, v5, nullptr);
+    // only the face's own component of the last sample is kept
     float* o = f.axis == 0 ? ox : (f.axis == 1 ? oy : oz);
-    o[f.e] = sel3(v5, f.axis);
+    o[f.e] = mac_sample_comp(mac, q, f.axis);
 }
 
 struct Face3 {

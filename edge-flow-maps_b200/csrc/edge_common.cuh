@@ -167,6 +167,21 @@ EDGE_D void mac_sample(const Mac& m, const float p[3], float v[3], float G[3][3]
     v[2] = bspline_sum<GRAD>(m.u[2], m.ny, m.nz + 1, A5[0], A5[1], A0[2], m.inv_dx, GRAD ? G[2] : nullptr);
 }
 
+// Component a of interp_u_MAC alone (mac_sample's arithmetic for that
+// component): the semi-Lagrangian advection keeps only the face's own
+// component of its last sample.
+EDGE_D float mac_sample_comp(const Mac& m, const float p[3], int a) {
+    float q[3] = {over_dx(p[0], m.dx, m.inv_dx, m.pow2), over_dx(p[1], m.dx, m.inv_dx, m.pow2),
+                  over_dx(p[2], m.dx, m.inv_dx, m.pow2)};
+    Axis3 A[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        A[d] = d == a ? bspline_axis<false>(q[d], m.hi0[d]) : bspline_axis<false>(q[d] - 0.5f, m.hi5[d]);
+    if (a == 0) return bspline_sum<false>(m.u[0], m.ny, m.nz, A[0], A[1], A[2], m.inv_dx, nullptr);
+    if (a == 1) return bspline_sum<false>(m.u[1], m.ny + 1, m.nz, A[0], A[1], A[2], m.inv_dx, nullptr);
+    return bspline_sum<false>(m.u[2], m.ny, m.nz + 1, A[0], A[1], A[2], m.inv_dx, nullptr);
+}
+
 // ---------------------------------------------------------------------------
 // trilinear dye sampler on 4-channel cell fields (taichi_utils.py:172-227)
 // ---------------------------------------------------------------------------
