@@ -31,6 +31,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <tuple>
 #include <vector>
 
@@ -86,6 +87,7 @@ struct Lvl {
     int vec;             // H % 4 == 0: the level runs the four-slot (float4) kernels
     float* r[2];         // residual planes
     float* z[2];         // preconditioned residual planes
+    float* zt;           // third z plane for the fused half-sweep pairs (or NULL)
     unsigned short* code[2];  // solid solver: neighbour codes per plane (else NULL)
     int* bm;             // solid solver: lexicographic mask (level 0: the caller's)
 };
@@ -1589,6 +1591,154 @@ __global__ void __launch_bounds__(256) k_cg_xr4(G g, Lvl L, Fine f) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Two consecutive half sweeps in one launch, through a shared-memory tile
+// with a halo.  A block owns TI x TJ rows (i, j) of the level, every row
+// whole in k.  It stages the other colour's z of its rows plus two on each
+// side (with the coarse parent's z added when the first sweep is the
+// prolongation sweep), runs the first half sweep (colour cA) on its rows plus
+// one on each side - the halo cells are computed by both neighbouring blocks
+// from the same inputs, so they agree bit for bit, and only the owner stores
+// them - then the second half sweep (colour cB) on its rows, reading the
+// first sweep's results from shared memory.  Each cell's arithmetic is
+// k_hsweep4's, in the same order (the first sweep's values pass through the
+// level's storage type before the second reads them, as they do through
+// global memory between two launches).
+//
+// The second sweep's results go to zBout, a plane other than the one colour
+// cB is staged from: another block may still be staging those rows as its
+// halo.  The host tracks which of the level's three z planes (z[0], z[1], zt)
+// holds each colour after every launch.
+// ---------------------------------------------------------------------------
+constexpr size_t kPairSmemMax = 200 * 1024;
+constexpr int kPairDefault = 0;
+
+// shared memory of a pair launch with TI x TJ owned rows of H slots
+inline size_t pair_smem(int TI, int TJ, int H) {
+    return (size_t)((TI + 4) * (TJ + 4) + (TI + 2) * (TJ + 2)) * H * sizeof(float);
+}
+
+// v rounded to the level's storage type (what a store and a reload return)
+template <class ZT>
+EDGE_D float zt_round(float v) { return v; }
+template <>
+EDGE_D float zt_round<__nv_bfloat16>(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+template <>
+EDGE_D float zt_round<__half>(float v) { return __half2float(__float2half_rn(v)); }
+
+// nbr_sum over a staged tile: the same directions, order and code tests;
+// W = row width of the staged tile, s = the cell's index in it
+template <class F>
+EDGE_D float nbr_sum_s(unsigned code, int s, int k, int W, int H, F val) {
+    float ret = 0.0f;
+    if (code & NB_XP) ret += val(s + W * H);
+    if (code & NB_XM) ret += val(s - W * H);
+    if (code & NB_YP) ret += val(s + H);
+    if (code & NB_YM) ret += val(s - H);
+    if (code & NB_ZP) ret += val(s + (k & 1));
+    if (code & NB_ZM) ret += val(s - 1 + (k & 1));
+    return ret;
+}
+
+template <int MA, int MB, bool SOLID, class ZT, int TI, int TJ>
+__global__ void __launch_bounds__(256) k_hs_pair(G g, Lvl L, Lvl C, int level0, int cA, float* zBout) {
+    pdl_enter();
+    count_launch(g.st);
+    if (stopped(g)) {
+        if (MB == HS_ZR && blockIdx.x == 0 && threadIdx.x == 0) set_cond(g, 0);
+        return;
+    }
+    extern __shared__ float sm[];
+    const int H = L.H, cB = cA ^ 1;
+    constexpr int WB = TJ + 4, WA = TJ + 2, RB = (TI + 4) * WB, RA = (TI + 2) * WA;
+    float* zB = sm;
+    float* zA = sm + RB * H;
+    const float mean = level0 ? g.st->mean : 0.0f, zsc = level0 ? g.st->zsc : 1.0f;
+    const int nti = (L.n0 + TI - 1) / TI, ntj = (L.n1 + TJ - 1) / TJ;
+    const float* __restrict__ zo = pick(L.z, cB);
+    float* __restrict__ zAg = pick(L.z, cA);
+    float* __restrict__ zBg = zBout;
+    const float* __restrict__ rA = pick(L.r, cA);
+    const float* __restrict__ rB = pick(L.r, cB);
+    double v[1] = {0.0};
+    for (int tile = blockIdx.x; tile < nti * ntj; tile += gridDim.x) {
+        const int i0 = (tile / ntj) * TI, j0 = (tile % ntj) * TJ;
+        // 1. colour cB's z on the rows i0-2 .. i0+TI+1, j0-2 .. j0+TJ+1
+        if (MA != HS_FIRST) {
+            for (int t = threadIdx.x; t < RB * H; t += blockDim.x) {
+                const int row = fdiv(t, L.dH), kk = t - row * H;
+                const int i = i0 - 2 + row / WB, j = j0 - 2 + row % WB;
+                float z = 0.0f;
+                if (i >= 0 && i < L.n0 && j >= 0 && j < L.n1) {
+                    const int k = 2 * kk + ((i + j + cB) & 1);
+                    z = Zs<ZT>::ld(zo, (i * L.n1 + j) * H + kk);
+                    if (MA == HS_PROLONG && k < L.n2) z = z + parent_zg<ZT>(C, i, j, k);
+                }
+                zB[t] = z;
+            }
+            __syncthreads();
+        }
+        // 2. first half sweep (colour cA) on the rows i0-1 .. i0+TI, j0-1 .. j0+TJ
+        for (int t = threadIdx.x; t < RA * H; t += blockDim.x) {
+            const int row = fdiv(t, L.dH), kk = t - row * H;
+            const int ii = row / WA, jj = row % WA;
+            const int i = i0 - 1 + ii, j = j0 - 1 + jj;
+            float zn = 0.0f;
+            if (i >= 0 && i < L.n0 && j >= 0 && j < L.n1) {
+                const int k = 2 * kk + ((i + j + cA) & 1);
+                const int e = (i * L.n1 + j) * H + kk;
+                const unsigned code = k < L.n2 ? code_at<SOLID>(L, cA, e, i, j, k) : 0u;
+                if (code & CELL_FLUID) {
+                    const float rv = (rld<ZT>(rA, e, level0) - mean) * zsc;
+                    float ns = 0.0f;
+                    if (MA != HS_FIRST)
+                        ns = nbr_sum_s(code, ((ii + 1) * WB + (jj + 1)) * H + kk, k, WB, H,
+                                       [&](int q) { return zB[q]; });
+                    zn = (rv + ns) / nf_of<SOLID>(g.walls, L, code, i, j, k);
+                }
+                if (ii >= 1 && ii <= TI && jj >= 1 && jj <= TJ) Zs<ZT>::st(zAg, e, zn);
+                zn = zt_round<ZT>(zn);
+            }
+            zA[t] = zn;
+        }
+        __syncthreads();
+        // 3. second half sweep (colour cB) on the owned rows
+        for (int t = threadIdx.x; t < TI * TJ * H; t += blockDim.x) {
+            const int row = fdiv(t, L.dH), kk = t - row * H;
+            const int ii = row / TJ, jj = row % TJ;
+            const int i = i0 + ii, j = j0 + jj;
+            if (i >= L.n0 || j >= L.n1) continue;
+            const int k = 2 * kk + ((i + j + cB) & 1);
+            const int e = (i * L.n1 + j) * H + kk;
+            const int sa = ((ii + 1) * WA + (jj + 1)) * H + kk;
+            const unsigned code = k < L.n2 ? code_at<SOLID>(L, cB, e, i, j, k) : 0u;
+            float zn = 0.0f;
+            float rv = 0.0f;
+            if (code & CELL_FLUID) {
+                rv = (rld<ZT>(rB, e, level0) - mean) * zsc;
+                const float ns = nbr_sum_s(code, sa, k, WA, H, [&](int q) { return zA[q]; });
+                zn = (rv + ns) / nf_of<SOLID>(g.walls, L, code, i, j, k);
+                if (MB == HS_ZR) v[0] += (double)zn * (double)rv;
+            }
+            Zs<ZT>::st(zBg, e, zn);
+            if (MB == HS_ZR) {
+                // the colour-cA cell of the same slot, final after the first sweep
+                const int kA = 2 * kk + ((i + j + cA) & 1);
+                if (kA < L.n2 && (code_at<SOLID>(L, cA, e, i, j, kA) & CELL_FLUID))
+                    v[0] += (double)zA[sa] * (double)((rld<ZT>(rA, e, level0) - mean) * zsc);
+            }
+        }
+        __syncthreads();  // the tile's shared arrays are refilled by the next tile
+    }
+    if (MB == HS_ZR) {
+        if (last_block<1>(g, 4, v)) {
+            double sm1[1];
+            final_sum<1>(g, 4, sm1);
+            if (threadIdx.x == 0) zr_epilogue(g, sm1[0]);
+        }
+    }
+}
+
 // restriction, four coarse cells (I, J, K0..K0+3) per thread: their children
 // are slots K0..K0+3 of both planes in the four fine rows (2I+a, 2J+b)
 template <bool SOLID, class ZT>
@@ -1943,6 +2093,9 @@ static int coarse_smem_attrs(int bytes) {
     return EDGE_OK;
 }
 
+template <class ZT>
+static int pair_attrs_z();
+
 int prepare_coarse_kernels(const Ctx& c) {
     if ((size_t)c.csmem > kCoarseSmem) return EDGE_EINVAL;  // the coarsest level alone must fit
     if (c.csmem > 48 * 1024) {
@@ -1951,7 +2104,18 @@ int prepare_coarse_kernels(const Ctx& c) {
         if (r == EDGE_OK) r = coarse_smem_attrs<__half>(c.csmem);
         if (r != EDGE_OK) return r;
     }
-    return EDGE_OK;
+    // the fused half-sweep pairs' tiles (up to kPairSmemMax bytes), once per device
+    static std::mutex mu;
+    static std::set<int> done;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count(dev)) return EDGE_OK;
+    int r = pair_attrs_z<float>();
+    if (r == EDGE_OK) r = pair_attrs_z<__nv_bfloat16>();
+    if (r == EDGE_OK) r = pair_attrs_z<__half>();
+    if (r == EDGE_OK) done.insert(dev);
+    return r;
 }
 
 // Blocks of kernel k (block threads, smem bytes of dynamic shared memory)
@@ -2000,7 +2164,102 @@ static void launch_pdl(void (*k)(KArgs...), int grid, int block, size_t smem, cu
     cudaLaunchKernelEx(&cfg, k, args...);
 }
 
-// the descent of a V-cycle: levels 0..lc-1 (sweeps and restrictions)
+// Fused half-sweep pairs (k_hs_pair): 0 off, else the tile of rows a block
+// owns: 1 = 8 x 4, 2 = 8 x 8, 3 = 16 x 8.  EDGE_MGPCG_PAIR overrides the
+// default; read once per process.
+static int pair_mode() {
+    static const int m = [] {
+        const char* e = getenv("EDGE_MGPCG_PAIR");
+        const int v = e ? atoi(e) : kPairDefault;
+        return v >= 0 && v <= 3 ? v : kPairDefault;
+    }();
+    return m;
+}
+static void pair_tile(int mode, int& ti, int& tj) {
+    ti = mode == 3 ? 16 : 8;
+    tj = mode == 1 ? 4 : 8;
+}
+
+// whether level l runs its sweeps as fused pairs
+static bool use_pair(const Ctx& c, int l) {
+    const Lvl& L = c.lv.lv[l];
+    const int m = pair_mode();
+    if (m == 0 || L.zt == nullptr || l >= c.lv.lc) return false;
+    int ti, tj;
+    pair_tile(m, ti, tj);
+    return pair_smem(ti, tj, L.H) <= kPairSmemMax;
+}
+
+// level L with colour q's z held in plane zq
+inline Lvl with_z(const Lvl& L, int q, float* zq) {
+    Lvl x = L;
+    x.z[q] = zq;
+    return x;
+}
+
+// Where level l's z is after its up sweeps (what the prolongation into level
+// l - 1 reads): a paired level below the fine one ends with colour 1 in zt.
+static Lvl up_layout(const Ctx& c, int l) {
+    const Lvl& L = c.lv.lv[l];
+    return l > 0 && use_pair(c, l) ? with_z(L, 1, L.zt) : L;
+}
+
+template <int MA, int MB, bool S, class ZT>
+static void launch_pair(const Ctx& c, const Lvl& L, const Lvl& C, int l0, int cA, float* out, cudaStream_t st) {
+    int ti, tj;
+    const int m = pair_mode();
+    pair_tile(m, ti, tj);
+    const size_t sm = pair_smem(ti, tj, L.H);
+    const int tiles = ((L.n0 + ti - 1) / ti) * ((L.n1 + tj - 1) / tj);
+    const int g = std::min(tiles, kMaxBlocks);
+    if (m == 1) launch_pdl(k_hs_pair<MA, MB, S, ZT, 8, 4>, g, 256, sm, st, c.g, L, C, l0, cA, out);
+    else if (m == 2) launch_pdl(k_hs_pair<MA, MB, S, ZT, 8, 8>, g, 256, sm, st, c.g, L, C, l0, cA, out);
+    else launch_pdl(k_hs_pair<MA, MB, S, ZT, 16, 8>, g, 256, sm, st, c.g, L, C, l0, cA, out);
+}
+
+template <int MA, int MB, bool S, class ZT>
+static int pair_attrs_t() {
+    const int b = (int)kPairSmemMax;
+    CK(cudaFuncSetAttribute(k_hs_pair<MA, MB, S, ZT, 8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CK(cudaFuncSetAttribute(k_hs_pair<MA, MB, S, ZT, 8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    CK(cudaFuncSetAttribute(k_hs_pair<MA, MB, S, ZT, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    return EDGE_OK;
+}
+template <bool S, class ZT>
+static int pair_attrs_s() {
+    int r = pair_attrs_t<HS_FIRST, HS_PLAIN, S, ZT>();
+    if (r == EDGE_OK) r = pair_attrs_t<HS_PLAIN, HS_PLAIN, S, ZT>();
+    if (r == EDGE_OK) r = pair_attrs_t<HS_PROLONG, HS_PLAIN, S, ZT>();
+    if (r == EDGE_OK) r = pair_attrs_t<HS_PLAIN, HS_ZR, S, ZT>();
+    return r;
+}
+template <class ZT>
+static int pair_attrs_z() {
+    int r = pair_attrs_s<false, ZT>();
+    return r == EDGE_OK ? pair_attrs_s<true, ZT>() : r;
+}
+
+// one half sweep of colour `color`, unfused
+template <int MODE, bool S, class ZT>
+static void launch_hs(const Ctx& c, const Lvl& L, const Lvl& C, int l0, int color, cudaStream_t stream) {
+    if (L.vec)
+        launch_pdl(k_hsweep4<MODE, S, ZT>, rgrid((long long)L.n0 * L.n1 * (L.H / 4)), 256, 0, stream, c.g, L, C, l0,
+                   color);
+    else
+        launch_pdl(k_hsweep<MODE, S, ZT>, rgrid(L.P), 256, 0, stream, c.g, L, C, l0, color);
+}
+
+template <bool S, class ZT>
+static void launch_restrict(const Ctx& c, const Lvl& L, const Lvl& C, int l0, int first, cudaStream_t stream) {
+    if (L.vec)
+        launch_pdl(k_restrict4<S, ZT>, rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream, c.g, L, C, l0, first);
+    else
+        launch_pdl(k_restrict<S, ZT>, rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream, c.g, L, C, l0, first);
+}
+
+// the descent of a V-cycle: levels 0..lc-1 (sweeps and restrictions).
+// Sweeps per level (mgpcg.py:177-187): colours 0, 1, 0, 1 at the fine level
+// (the first reads no z), 1, 0, 1 below it (the restriction wrote colour 0).
 template <bool S, class ZT>
 void vdown_t(const Ctx& c, cudaStream_t stream) {
     const Levels& V = c.lv;
@@ -2010,49 +2269,54 @@ void vdown_t(const Ctx& c, cudaStream_t stream) {
         const Lvl& L = V.lv[l];
         const Lvl& C = V.lv[l + 1];
         const int l0 = l == 0, first = l + 1 < lgroup;
-        if (L.vec) {
-            const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-            if (l == 0) launch_pdl(k_hsweep4<HS_FIRST, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            launch_pdl(k_restrict4<S, ZT>, rgrid((long long)C.n0 * C.n1 * (L.H / 4)), 256, 0, stream, c.g, L, C, l0, first);
+        if (use_pair(c, l) && l == 0) {
+            // colour 1 goes to zt, then back to z[1]
+            launch_pair<HS_FIRST, HS_PLAIN, S, ZT>(c, L, C, l0, 0, L.zt, stream);
+            launch_pair<HS_PLAIN, HS_PLAIN, S, ZT>(c, with_z(L, 1, L.zt), C, l0, 0, L.z[1], stream);
+            launch_restrict<S, ZT>(c, L, C, l0, first, stream);
+        } else if (use_pair(c, l)) {
+            // colour 1 ends in zt (and stays there through the up sweeps)
+            launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 1, stream);
+            launch_pair<HS_PLAIN, HS_PLAIN, S, ZT>(c, L, C, l0, 0, L.zt, stream);
+            launch_restrict<S, ZT>(c, with_z(L, 1, L.zt), C, l0, first, stream);
         } else {
-            const int g = rgrid(L.P);
-            if (l == 0) launch_pdl(k_hsweep<HS_FIRST, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            launch_pdl(k_restrict<S, ZT>, rgrid((long long)C.n0 * C.n1 * C.n2), 256, 0, stream, c.g, L, C, l0, first);
+            if (l == 0) launch_hs<HS_FIRST, S, ZT>(c, L, C, l0, 0, stream);
+            launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 1, stream);
+            launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 0, stream);
+            launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 1, stream);
+            launch_restrict<S, ZT>(c, L, C, l0, first, stream);
         }
     }
 }
 
-// the ascent of a V-cycle: levels lc-1..0 (prolongation and sweeps); with
-// final_zr the last sweep also forms z.r and the iteration's bookkeeping
+// the ascent of a V-cycle: levels lc-1..0 (prolongation and sweeps
+// 1, 0, 1, 0, mgpcg.py:189-195); with final_zr the last sweep also forms z.r
+// and the iteration's bookkeeping
 template <bool S, class ZT>
 void vup_t(const Ctx& c, cudaStream_t stream, bool final_zr) {
     const Levels& V = c.lv;
     const int lc = V.lc;
     for (int l = lc - 1; l >= 0; l--) {
         const Lvl& L = V.lv[l];
-        const Lvl& C = V.lv[l + 1];
+        const Lvl C = l + 1 < lc ? up_layout(c, l + 1) : V.lv[l + 1];
         const int l0 = l == 0;
         const bool zr = l == 0 && final_zr;
-        if (L.vec) {
-            const int g = rgrid((long long)L.n0 * L.n1 * (L.H / 4));
-            launch_pdl(k_hsweep4<HS_PROLONG, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            if (zr) launch_pdl(k_hsweep4<HS_ZR, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            else launch_pdl(k_hsweep4<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+        if (use_pair(c, l) && l == 0) {
+            // colour 0 goes to zt, then back to z[0]
+            launch_pair<HS_PROLONG, HS_PLAIN, S, ZT>(c, L, C, l0, 1, L.zt, stream);
+            if (zr) launch_pair<HS_PLAIN, HS_ZR, S, ZT>(c, with_z(L, 0, L.zt), C, l0, 1, L.z[0], stream);
+            else launch_pair<HS_PLAIN, HS_PLAIN, S, ZT>(c, with_z(L, 0, L.zt), C, l0, 1, L.z[0], stream);
+        } else if (use_pair(c, l)) {
+            // colour 1 is in zt since the descent; colour 0 goes to z[1], then back to z[0]
+            const Lvl Lx = with_z(L, 1, L.zt);
+            launch_pair<HS_PROLONG, HS_PLAIN, S, ZT>(c, Lx, C, l0, 1, L.z[1], stream);
+            launch_pair<HS_PLAIN, HS_PLAIN, S, ZT>(c, with_z(Lx, 0, L.z[1]), C, l0, 1, L.z[0], stream);
         } else {
-            const int g = rgrid(L.P);
-            launch_pdl(k_hsweep<HS_PROLONG, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 1);
-            if (zr) launch_pdl(k_hsweep<HS_ZR, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
-            else launch_pdl(k_hsweep<HS_PLAIN, S, ZT>, g, 256, 0, stream, c.g, L, C, l0, 0);
+            launch_hs<HS_PROLONG, S, ZT>(c, L, C, l0, 1, stream);
+            launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 0, stream);
+            launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 1, stream);
+            if (zr) launch_hs<HS_ZR, S, ZT>(c, L, C, l0, 0, stream);
+            else launch_hs<HS_PLAIN, S, ZT>(c, L, C, l0, 0, stream);
         }
     }
 }
@@ -2378,6 +2642,13 @@ int edge_mgpcg_create(void** handle, int nx, int ny, int nz, int base_level, con
         }
     }
     plan_coarse(c, s->solid);
+    // the third z plane of each per-level V-cycle level (fused half-sweep pairs)
+    for (int l = 0; l < c.lv.lc && r == EDGE_OK; l++) {
+        Lvl& V = c.lv.lv[l];
+        const size_t esz = precision != 0 ? 2 : 4;
+        r = alloc(s, (void**)&V.zt, plane_alloc(V.P) * esz);
+        if (r == EDGE_OK) r = cu(cudaMemset(V.zt, 0, plane_alloc(V.P) * esz));
+    }
     if (r == EDGE_OK) r = prepare_coarse_kernels(c);
     const size_t pa0 = plane_alloc(c.lv.lv[0].P);
     if (r == EDGE_OK) r = alloc(s, (void**)&c.f.x[0], 2 * pa0 * sizeof(float));
@@ -2783,6 +3054,11 @@ extern "C" int edge_mgpcg_poisson_noalloc(int nx, int ny, int nz, int base_level
     c.g.st = A->state;
     c.g.use_cond = 0;
     plan_coarse(c, false);
+    // third z planes for the fused half-sweep pairs, where the scratch has room
+    long long extra = 0;
+    for (int l = 0; l < c.lv.lc; l++) extra += (c.lv.lv[l].P + 63) / 64 * 64;
+    if (off + extra <= kNoAllocFloats)
+        for (int l = 0; l < c.lv.lc; l++) c.lv.lv[l].zt = take(c.lv.lv[l].P);
     r = prepare_coarse_kernels(c);
     if (r != EDGE_OK) return r;
     // the loop state starts clean on every call (the arrays keep the last

@@ -63,28 +63,6 @@ __global__ void k_lp_vel_diff(Mac mac, const float* __restrict__ vel, float* vdi
     for (int c = 0; c < 3; c++) vdiff[3 * e + c] = kk * (vel[3 * e + c] - v[c]);
 }
 
-// Adds v[0..3] to the four consecutive floats f[g .. g+3] with 16- and
-// 8-byte vector atomics on the aligned pieces (f 16-byte aligned); zero
-// pieces are skipped.  Vector atomics (sm_90+) move a piece in one request.
-EDGE_D void add_row4(float* f, long long g, const float (&v)[4]) {
-    const int m = (int)(g & 3);
-    if (m == 0) {
-        atomicAdd(reinterpret_cast<float4*>(f + g), make_float4(v[0], v[1], v[2], v[3]));
-    } else if (m == 2) {
-        if (v[0] != 0.0f || v[1] != 0.0f) atomicAdd(reinterpret_cast<float2*>(f + g), make_float2(v[0], v[1]));
-        if (v[2] != 0.0f || v[3] != 0.0f) atomicAdd(reinterpret_cast<float2*>(f + g + 2), make_float2(v[2], v[3]));
-    } else {
-        // m == 1: g+1 .. g+2 is 8-byte aligned; m == 3: g+1 is 16-byte aligned
-        if (v[0] != 0.0f) atomicAdd(f + g, v[0]);
-        if (m == 3) {
-            atomicAdd(reinterpret_cast<float4*>(f + g + 1), make_float4(v[1], v[2], v[3], 0.0f));
-        } else {
-            if (v[1] != 0.0f || v[2] != 0.0f) atomicAdd(reinterpret_cast<float2*>(f + g + 1), make_float2(v[1], v[2]));
-            if (v[3] != 0.0f) atomicAdd(f + g + 3, v[3]);
-        }
-    }
-}
-
 // lp.py:100-156 laden_particles_back_with_computing_particle: quadratic
 // B-spline scatter of the drag onto the three face grids (atomic adds, like
 // the reference's `+=` in a parallel loop)
@@ -101,8 +79,6 @@ __global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float* dx_, float* dy
     float r = rad[e];
     float scale = r * r * r / (lrad * lrad * lrad);
     float* D[3] = {dx_, dy_, dz_};
-    const bool vec_ok = ((reinterpret_cast<size_t>(dx_) | reinterpret_cast<size_t>(dy_) |
-                          reinterpret_cast<size_t>(dz_)) & 15) == 0;
     for (int a = 0; a < 3; a++) {
         float off[3];
         int base[3];
@@ -112,10 +88,6 @@ __global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float* dx_, float* dy
         }
         int n0 = nx + (a == 0), n1 = ny + (a == 1), n2 = nz + (a == 2);
         float val = vdiff[3 * e + a];
-        // the row's four taps f2 = base - 1 .. base + 2, and the float after
-        // them that an aligned 16-byte piece may cover with a zero, lie in
-        // the grid (particles within 3 dx of a wall are skipped above)
-        const bool rows_in = base[2] >= 1 && base[2] + 3 < n2 && vec_ok;
         for (int oi = -1; oi < 3; oi++) {
             int f0 = base[0] + oi;
             if (f0 < 0 || f0 >= n0) continue;
@@ -126,18 +98,6 @@ __global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float* dx_, float* dy
                 if (f1 < 0 || f1 >= n1) continue;
                 float wy = N2(g[1] - (float)f1 - off[1]);
                 if (wy == 0.0f) continue;
-                if (rows_in) {
-                    // the row's values (one of the four weights is zero) as
-                    // vector atomics on aligned pieces of the four faces
-                    float v[4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const float w = wx * wy * N2(g[2] - (float)(base[2] - 1 + q) - off[2]);
-                        v[q] = val * w * scale;
-                    }
-                    add_row4(D[a], (long long)idx3(f0, f1, base[2] - 1, n1, n2), v);
-                    continue;
-                }
                 for (int ok = -1; ok < 3; ok++) {
                     int f2 = base[2] + ok;
                     if (f2 < 0 || f2 >= n2) continue;

@@ -342,3 +342,67 @@ def test_solve_writes_each_callers_output():
     torch.cuda.synchronize()
     assert float(x2.abs().max()) > 0
     assert torch.equal(x1, x2)
+
+
+_PAIR_SCRIPT = r"""
+import sys
+import numpy as np, torch
+sys.path[:0] = [sys.argv[2], sys.argv[3]]
+from edgeb200.projection import Projection
+out = {}
+cases = [((128, 64, 64), 2, 0, False), ((128, 64, 64), 2, 1, False), ((128, 64, 64), 2, 2, False),
+         ((128, 64, 64), 2, 0, True), ((128, 64, 64), 2, 1, True), ((200, 72, 24), 1, 0, False),
+         ((200, 72, 24), 1, 2, True)]
+for n, (res, base, prec, solid) in enumerate(cases):
+    rng = np.random.default_rng(20 + n)
+    kw = {}
+    if solid:
+        i, j, k = np.meshgrid(*(np.arange(m) for m in res), indexing="ij")
+        mask = ((np.abs(j - res[1] // 2) < (i - 20) * 0.6) & (i > 20) & (i < 60) & (k > 2)).astype(np.int32)
+        bvel = np.zeros(res + (3,), np.float32)
+        bvel[..., 0] = 0.25
+        kw = dict(mask=torch.from_numpy(mask).cuda(), bvel=torch.from_numpy(bvel).cuda())
+    shapes = [(res[0] + 1, res[1], res[2]), (res[0], res[1] + 1, res[2]), (res[0], res[1], res[2] + 1)]
+    u = [torch.from_numpy(rng.normal(size=s).astype(np.float32)).cuda() for s in shapes]
+    P = Projection(res, base_level=base, precision=prec, **kw)
+    P.poisson(*u, abs_tol=1e-9, rel_tol=1e-9, max_iters=60)
+    it, rtr, st = P.result()
+    for a in range(3):
+        out[f"u{a}_{n}"] = u[a].cpu().numpy()
+    out[f"res_{n}"] = np.array([it, st])
+    out[f"rtr_{n}"] = np.array(rtr)
+    out[f"kernels_{n}"] = np.array(P.kernel_count())
+    P.close()
+np.savez(sys.argv[1], **out)
+"""
+
+
+def test_fused_half_sweep_pairs_match_unfused(tmp_path):
+    """The V-cycle's half sweeps fused in pairs (k_hs_pair: a shared-memory
+    tile with a two-row halo, the second sweep written to a third z plane)
+    give the unfused sweeps' result bit for bit: FP32, BF16 and FP16 level
+    storage, plain and solid solvers, and a ragged grid whose tiles overhang
+    the level and whose second level has no four-slot layout.  The switch is
+    read once per process, so each tile shape runs in a child process."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pkg = os.path.join(root, "edge-flow-maps_b200")
+    outs = {}
+    for mode in ("0", "1", "2", "3"):
+        path = str(tmp_path / f"p{mode}.npz")
+        env = dict(os.environ, EDGE_MGPCG_PAIR=mode)
+        subprocess.run([sys.executable, "-c", _PAIR_SCRIPT, path, pkg, root], env=env, check=True, timeout=900)
+        outs[mode] = np.load(path)
+    ref = outs["0"]
+    for n in range(7):
+        assert int(ref[f"res_{n}"][0]) > 2
+    for mode, d in outs.items():
+        for f in ref.files:
+            if f.startswith("kernels"):
+                continue
+            np.testing.assert_array_equal(d[f], ref[f], err_msg=f"{f} mode {mode}")
+        # fewer launches per V-cycle when the pairs run
+        if mode != "0":
+            assert int(d["kernels_0"]) < int(ref["kernels_0"]), (mode, int(d["kernels_0"]), int(ref["kernels_0"]))
