@@ -548,6 +548,77 @@ def c2_measure(steps=5, warm=3, per_cell=8):
     return out
 
 
+C0_RES = (64, 32, 32)
+
+
+def c0_measure(steps=100):
+    """Configuration 0 in full: the 64x32x32 leapfrogging rings (4 levels,
+    reinit every 12, CFL 0.5) for `steps` EDGE steps from t = 0, on the
+    device (CUDA events around all steps; a separate 3-step run first warms
+    the kernels and captures the solve graphs) and on the host cores (the
+    oracle, C/OpenMP, every step timed), each choosing its own dt.  Also the
+    relative L2 difference of velocity and dye after the last step between
+    the two, next to the same difference between the oracle and its FMA twin
+    (the oracle compiled with contracted multiply-adds): how far two float32
+    evaluation orders drift apart over the run."""
+    import numpy as np
+    import torch
+    from edgeb200.sim import EdgeSim, leapfrog_init
+    from oracle import edge_oracle as O
+    res = C0_RES
+    dx = 1.0 / res[1]
+    u, smoke = leapfrog_init(res, dx, radii=(0.21, 0.28), sigma=0.03, circulation=1.0, x_start=0.3)
+    kw = dict(variant="edge", cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * dx, base_level=2, bfecc_clamp=True,
+              visualize_dt=1e9)
+    warm = EdgeSim(res, dx, **kw)
+    warm.set_velocity(*u)
+    warm.set_smoke(smoke)
+    for _ in range(3):
+        warm.step()
+    del warm
+    sim = EdgeSim(res, dx, **kw)
+    sim.set_velocity(*u)
+    sim.set_smoke(smoke)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sim.step()
+    e1.record()
+    torch.cuda.synchronize()
+    gpu_s = e0.elapsed_time(e1) / 1e3 / steps
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    u0 = [t.cpu().numpy() for t in u]
+    sm0 = smoke.cpu().numpy()
+    okw = dict(cfl=CFL, reinit_every=REINIT, ed_eps=EPS_FRAC * dx, base_level=2)
+    A = O.EdgeState(res, dx, [a.copy() for a in u0], sm0.copy())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.edge_substep(A, **okw)
+    cpu_s = (time.perf_counter() - t0) / steps
+    B = O.EdgeState(res, dx, [a.copy() for a in u0], sm0.copy())
+    with O.fma_twin():
+        for _ in range(steps):
+            O.edge_substep(B, **okw)
+
+    def rel(x, y):
+        x = np.asarray(x, np.float64)
+        y = np.asarray(y, np.float64)
+        return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30))
+
+    return {"workload": "leapfrogging rings 64x32x32, EDGE, CFL 0.5, reinit 12, 4-level MGPCG", "steps": steps,
+            "gpu_ms_per_step": 1e3 * gpu_s, "gpu_steps_per_s": 1.0 / gpu_s,
+            "cpu_ms_per_step": 1e3 * cpu_s, "cpu_steps_per_s": 1.0 / cpu_s,
+            "cpu_cores": int(os.environ["OMP_NUM_THREADS"]),
+            "cpu_kind": "port (C/OpenMP restatement of the reference kernels)",
+            "final_rel_l2": {"u_device_vs_oracle": max(rel(t.cpu().numpy(), a) for t, a in zip(sim.u, A.u)),
+                             "u_twin_vs_oracle": max(rel(b, a) for b, a in zip(B.u, A.u)),
+                             "smoke_device_vs_oracle": rel(sim.smoke.cpu().numpy(), A.smoke),
+                             "smoke_twin_vs_oracle": rel(B.smoke, A.smoke)}}
+
+
 C4_RES = (512, 256, 256)
 
 
@@ -870,6 +941,8 @@ def main():
     ap.add_argument("--c2-only", action="store_true", help="only the solid + particle configuration")
     ap.add_argument("--c4-only", action="store_true", help="only the 512x256x256 mixed-precision configuration")
     ap.add_argument("--c4-steps", type=int, default=100)
+    ap.add_argument("--c0-full", action="store_true",
+                    help="configuration 0 in full (100 steps) on the device and on the host cores (oracle)")
     ap.add_argument("--no-variants", action="store_true", help="skip the ED4/ED8/GE/EFM step timings")
     ap.add_argument("--no-extras", action="store_true",
                     help="only the EDGE steps (no ED4/ED8, PCG or FP32-peak measurements; profiling)")
@@ -892,6 +965,11 @@ def main():
         return 0
     if args.c4_only:
         return run_c4_only(args)
+    if args.c0_full:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"c0_full": c0_measure()}), flush=True)
+        return 0
     return run_ours(args, rank, world, local_rank)
 
 

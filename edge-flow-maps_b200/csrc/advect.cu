@@ -550,23 +550,27 @@ __global__ void k_coef_p(MapP m, float4* __restrict__ g) {
     g[(size_t)7 * n + e] = make_float4(o[3][0], o[3][1], o[3][2], 0.f);
 }
 
-// face map on the packed layout
+// face map on the packed layout, one launch per face axis A: the map at the
+// face and the derivative along A (only that gradient column is evaluated)
 // (register caps: ED4 / EDGE 128 registers, 4 CTAs per SM; ED8 102, 5 CTAs
 // per SM; both measured faster than the uncapped builds)
-template <int V>
-__global__ void __launch_bounds__(128, V == HV_FULL ? 5 : 4) k_face_map_p(MapP m, float* fpx, float* fpy, float* fpz, float* fcx,
-                                                    float* fcy, float* fcz) {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_faces(m.nx, m.ny, m.nz)) return;
-    FaceIdx f = face_decompose(t, m.nx, m.ny, m.nz);
+template <int V, int A>
+__global__ void __launch_bounds__(128, V == HV_FULL ? 5 : 4) k_face_map_p(MapP m, float* fp, float* fc) {
+    const int n1 = m.ny + (A == 1), n2 = m.nz + (A == 2);
+    const long long nf = (long long)(m.nx + (A == 0)) * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nf) return;
+    const int e = (int)t;
+    const int k = (int)(t % n2);
+    const long long r = t / n2;
+    const int j = (int)(r % n1), i = (int)(r / n1);
     float X[3], val[3], G[3][3];
-    face_pos(f.axis, f.i, f.j, f.k, m.dx, X);
-    hermite3p<V, true>(m, X, val, G);
-    float* fp = f.axis == 0 ? fpx : (f.axis == 1 ? fpy : fpz);
-    float* fc = f.axis == 0 ? fcx : (f.axis == 1 ? fcy : fcz);
+    face_pos(A, i, j, k, m.dx, X);
+    hermite3p<V, true, A>(m, X, val, G);
+#pragma unroll
     for (int c = 0; c < 3; c++) {
-        fp[3 * f.e + c] = val[c];
-        fc[3 * f.e + c] = sel3(G[c], f.axis);
+        fp[3 * e + c] = val[c];
+        fc[3 * e + c] = G[c][A];
     }
 }
 
@@ -1345,10 +1349,22 @@ int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const fl
         return EDGE_EINVAL;
     if (!al16(packed)) return EDGE_EALIGN;
     MapP m = make_mapp(packed, nx, ny, nz, dx);
-    int g = grid_for(n_faces(nx, ny, nz), 128);
-    if (variant == HV_FD) k_face_map_p<HV_FD_P><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
-    else if (variant == HV_GARM) k_face_map_p<HV_GARM_P><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
-    else k_face_map_p<HV_FULL><<<g, 128, 0, S(stream)>>>(m, fpsix, fpsiy, fpsiz, fcolx, fcoly, fcolz);
+    const int gx = grid_for((long long)(nx + 1) * ny * nz, 128), gy = grid_for((long long)nx * (ny + 1) * nz, 128),
+              gz = grid_for((long long)nx * ny * (nz + 1), 128);
+    cudaStream_t st = S(stream);
+    if (variant == HV_FD) {
+        k_face_map_p<HV_FD_P, 0><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+        k_face_map_p<HV_FD_P, 1><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+        k_face_map_p<HV_FD_P, 2><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+    } else if (variant == HV_GARM) {
+        k_face_map_p<HV_GARM_P, 0><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+        k_face_map_p<HV_GARM_P, 1><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+        k_face_map_p<HV_GARM_P, 2><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+    } else {
+        k_face_map_p<HV_FULL, 0><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+        k_face_map_p<HV_FULL, 1><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+        k_face_map_p<HV_FULL, 2><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+    }
     return launch_status();
 }
 

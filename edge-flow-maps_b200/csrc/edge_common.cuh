@@ -560,9 +560,14 @@ EDGE_D void hcoef_p(const MapP& m, int ii, int jj, int kk, int im, int ip, int j
 }
 
 // hermite3 on the packed layout: the 8 corners are visited once and feed all
-// three components.
-template <int VARIANT, bool GRAD>
+// three components.  GSEL >= 0 computes only column GSEL of the gradient
+// (grad[c][GSEL]; the other columns are left unset) with the same arithmetic:
+// the face map keeps only the derivative along the face's own axis.
+template <int VARIANT, bool GRAD, int GSEL = -1>
 EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[3][3]) {
+    constexpr bool GX = GRAD && (GSEL < 0 || GSEL == 0);
+    constexpr bool GY = GRAD && (GSEL < 0 || GSEL == 1);
+    constexpr bool GZ = GRAD && (GSEL < 0 || GSEL == 2);
     float q[3] = {over_dx(p[0], m.dx, m.inv_dx, m.pow2) - 0.5f, over_dx(p[1], m.dx, m.inv_dx, m.pow2) - 0.5f,
                   over_dx(p[2], m.dx, m.inv_dx, m.pow2) - 0.5f};
     HAxis X = haxis(q[0], m.hi[0], m.nx), Y = haxis(q[1], m.hi[1], m.ny), Z = haxis(q[2], m.hi[2], m.nz);
@@ -588,10 +593,10 @@ EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[
                         float P0 = Z.f[k] * t[c][a * 4 + 0] + Z.g[k] * t[c][a * 4 + 1];
                         float P1 = Z.f[k] * t[c][a * 4 + 2] + Z.g[k] * t[c][a * 4 + 3];
                         Ax[c][a] += Y.f[j] * P0 + Y.g[j] * P1;
-                        if (GRAD) {
+                        if (GY) Bx[c][a] += Y.df[j] * P0 + Y.dg[j] * P1;
+                        if (GZ) {
                             float dP0 = Z.df[k] * t[c][a * 4 + 0] + Z.dg[k] * t[c][a * 4 + 1];
                             float dP1 = Z.df[k] * t[c][a * 4 + 2] + Z.dg[k] * t[c][a * 4 + 3];
-                            Bx[c][a] += Y.df[j] * P0 + Y.dg[j] * P1;
                             dAx[c][a] += Y.f[j] * dP0 + Y.g[j] * dP1;
                         }
                     }
@@ -600,22 +605,18 @@ EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             v[c] += X.f[i] * Ax[c][0] + X.g[i] * Ax[c][1];
-            if (GRAD) {
-                gx[c] += X.df[i] * Ax[c][0] + X.dg[i] * Ax[c][1];
-                gy[c] += X.f[i] * Bx[c][0] + X.g[i] * Bx[c][1];
-                gz[c] += X.f[i] * dAx[c][0] + X.g[i] * dAx[c][1];
-            }
+            if (GX) gx[c] += X.df[i] * Ax[c][0] + X.dg[i] * Ax[c][1];
+            if (GY) gy[c] += X.f[i] * Bx[c][0] + X.g[i] * Bx[c][1];
+            if (GZ) gz[c] += X.f[i] * dAx[c][0] + X.g[i] * dAx[c][1];
         }
     }
     const float inv = 1.0f / m.dx;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         val[c] = v[c];
-        if (GRAD) {
-            grad[c][0] = gx[c] * inv;
-            grad[c][1] = gy[c] * inv;
-            grad[c][2] = gz[c] * inv;
-        }
+        if (GX) grad[c][0] = gx[c] * inv;
+        if (GY) grad[c][1] = gy[c] * inv;
+        if (GZ) grad[c][2] = gz[c] * inv;
     }
 }
 
