@@ -315,6 +315,7 @@ class EdgeSim:
             io["copy"].wait_event(ev_dye)
             with torch.cuda.stream(io["copy"]):
                 io["host_smoke"].copy_(self.smoke, non_blocking=True)
+                io["smoke_out"] = io["copy"].record_event()
         # u = (grad psi)^T u_init(psi)                                 run_edge.py:669
         ops.pullback_u(self.init_u, dx, self.fpsi, self.fcol, self.u)
         # err = 0.5*(F^T u(phi) - u_init)                             run_edge.py:671-676
@@ -338,39 +339,70 @@ class EdgeSim:
         tm.stop("substep")
         return curr_dt
 
-    def step_host(self, host_u, host_smoke, dt=None):
+    def step_host(self, host_u, host_smoke, dt=None, chunks=4):
         """One step whose state comes from and goes back to pinned host
         buffers (the three face velocity arrays and the dye), as a caller
-        that keeps the fields on the host drives the simulation.  The copies
-        run on a copy stream beside the computation: the velocity in before
-        the step starts; the dye in while the step's first half runs (a step
-        reads the incoming dye only at a reinitialisation or with emitters,
-        and otherwise the dye chain overwrites it, so only those wait for
-        it); the dye out as soon as the dye chain ends, during the velocity
-        chain and the projection; the velocity out at the end.  Returns dt;
+        that keeps the fields on the host drives the simulation.  Returns dt;
         the host buffers hold the step's results once the current stream and
-        `self.copy_stream` have completed (torch.cuda.synchronize())."""
+        the two copy streams have completed (torch.cuda.synchronize(); the
+        last copies of a step run on `self.copy_stream`).
+
+        The copies run on two copy streams beside the computation, host to
+        device on `self.copy_in_stream`, device to host on `self.copy_stream`:
+        the velocity in before the step starts; the dye in while the step's
+        first half runs (a step reads the incoming dye only at a
+        reinitialisation or with emitters, and otherwise the dye chain
+        overwrites it, so only those wait for it); the dye out as soon as the
+        dye chain ends, during the velocity chain and the projection; the
+        velocity out at the end.  Each velocity array moves in `chunks`
+        pieces, and a piece of the next step's copy in waits only for the
+        same piece of this step's copy out, so the two directions of the
+        round trip overlap instead of following each other."""
         if not hasattr(self, "copy_stream"):
-            self.copy_stream = torch.cuda.Stream(device=self.u[0].device)
+            dev = self.u[0].device
+            self.copy_stream = torch.cuda.Stream(device=dev)
+            self.copy_in_stream = torch.cuda.Stream(device=dev)
+            self._host_out = None  # events of the previous step_host's copies out
         main = torch.cuda.current_stream()
-        cs = self.copy_stream
-        cs.wait_event(main.record_event())  # the previous step's kernels are done with the buffers
-        with torch.cuda.stream(cs):
-            for d, h in zip(self.u, host_u):
+        ci, co = self.copy_in_stream, self.copy_stream
+        pieces = []
+        for d, h in zip(self.u, host_u):
+            fd, fh = d.view(-1), h.view(-1)
+            n = fd.numel()
+            step_n = -(-n // max(1, int(chunks)))
+            for a0 in range(0, n, step_n):
+                pieces.append((fd[a0:a0 + step_n], fh[a0:a0 + step_n]))
+        prev = self._host_out
+        if prev is not None and len(prev["u"]) != len(pieces):
+            prev = {"u": [prev["u"][-1]] * len(pieces), "smoke": prev["smoke"]}
+        ci.wait_event(main.record_event())  # the previous step's kernels are done with the buffers
+        with torch.cuda.stream(ci):
+            for q, (d, h) in enumerate(pieces):
+                if prev is not None:
+                    ci.wait_event(prev["u"][q])  # this piece of the host buffer has been read back
                 d.copy_(h, non_blocking=True)
-            u_in = cs.record_event()
+            u_in = ci.record_event()
+            if prev is not None:
+                ci.wait_event(prev["smoke"])
             self.smoke.copy_(host_smoke, non_blocking=True)
-            smoke_in = cs.record_event()
+            smoke_in = ci.record_event()
         main.wait_event(u_in)
-        self._io = {"copy": cs, "smoke_in": smoke_in, "host_smoke": host_smoke}
+        io = {"copy": co, "smoke_in": smoke_in, "host_smoke": host_smoke}
+        self._io = io
         try:
             dt = self.step(dt=dt)
         finally:
             self._io = None
-        cs.wait_event(main.record_event())
-        with torch.cuda.stream(cs):
-            for h, d in zip(host_u, self.u):
+        co.wait_event(main.record_event())
+        with torch.cuda.stream(co):
+            if "smoke_out" not in io:
+                host_smoke.copy_(self.smoke, non_blocking=True)
+                io["smoke_out"] = co.record_event()
+            outs = []
+            for d, h in pieces:
                 h.copy_(d, non_blocking=True)
+                outs.append(co.record_event())
+        self._host_out = {"u": outs, "smoke": io["smoke_out"]}
         return dt
 
     def _particles_forces(self, dt):
