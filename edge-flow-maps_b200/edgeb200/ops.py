@@ -16,7 +16,7 @@ F = ctypes.c_float
 
 # kernels each entry point launches (memcpy/memset nodes are not counted)
 _KERNELS = {"edge_max_speed": 2, "edge_copy": 0, "edge_lp_max_speed": 2, "edge_march_ge": 3,
-            "edge_march_ge_packed": 3, "edge_calc_fd_3_from_grad": 2}
+            "edge_march_ge_packed": 3, "edge_calc_fd_3_from_grad": 2, "edge_face_map_packed": 3}
 _launched = [0]
 
 
