@@ -798,6 +798,8 @@ def run_ours(args, rank, world, local_rank):
     # the velocity and dye in from pinned host memory and reads them back
     # (EdgeSim.step_host: the copies on a copy stream beside the computation)
     e2e = None
+    if args.e2e_steps < 0:
+        args.e2e_steps = args.steps
     if args.e2e_steps > 0:
         host_u = [torch.empty(t_.shape, dtype=torch.float32, pin_memory=True) for t_ in sim.u]
         host_s = torch.empty(sim.smoke.shape, dtype=torch.float32, pin_memory=True)
@@ -931,7 +933,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default="edge", choices=["edge", "ed4", "ed8", "ge", "efm"])
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=-1,
+                    help="steps of the end-to-end (host buffers) measurement; default: --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=2)
     ap.add_argument("--unpacked", action="store_true", help="separate-field map layout in the device driver "
