@@ -75,18 +75,19 @@ EDGE_D Axis3 bspline_axis(float u, float hi) {
     a.base = b;
     // x0 lies in [0.5, 1.5) (exactly: s - b is exact), so the branches of
     // N2 / dN2 at x0, x0 - 1 and x0 - 2 are known: the same operations as the
-    // general functions, without their compares.
+    // general functions, without their compares.  The third tap's zero
+    // branch (|x0 - 2| = 1.5, i.e. x0 = 0.5) needs no select either: there
+    // t2 = 0 and 2 a2 - 3 = 0, so the polynomial gives the same zero; and
+    // |x1| |x1| = x1 x1, sign(x1) * (-2 |x1|) = -2 x1 exactly.
     const float x1 = x0 - 1.0f, x2 = x0 - 2.0f;  // x1 in [-0.5, 0.5), x2 in [-1.5, -0.5)
     const float t0 = 1.5f - x0, a2 = -x2, t2 = 1.5f - a2;
     a.w[0] = 0.5f * (t0 * t0);
-    a.w[1] = 0.75f - fabsf(x1) * fabsf(x1);
-    a.w[2] = a2 < 1.5f ? 0.5f * (t2 * t2) : 0.0f;
+    a.w[1] = 0.75f - x1 * x1;
+    a.w[2] = 0.5f * (t2 * t2);
     if (GRAD) {
         a.dw[0] = 0.5f * (2.0f * x0 - 3.0f);
-        const float r1 = -2.0f * fabsf(x1);
-        a.dw[1] = x1 < 0.0f ? -r1 : r1;
-        const float r2 = a2 < 1.5f ? 0.5f * (2.0f * a2 - 3.0f) : 0.0f;
-        a.dw[2] = -r2;
+        a.dw[1] = -2.0f * x1;
+        a.dw[2] = -(0.5f * (2.0f * a2 - 3.0f));
     }
     return a;
 }
