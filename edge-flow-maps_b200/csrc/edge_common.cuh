@@ -291,14 +291,16 @@ struct HAxis {
     int c0, cm, cp, cpp;   // iu, iu-1, iu+1, iu+2 (clamped as sample() does)
     float f[2], g[2], df[2], dg[2];
 };
+// hermite_f/g and derivatives at x with |x| <= 1 (haxis passes x in [0, 1)
+// and [-1, 0)).  The reference's |x| >= 1 branch gives 0; at |x| = 1 every
+// polynomial below is exactly 0 as well, so no select is needed.
 EDGE_D void hbasis(float x, float& f, float& g, float& df, float& dg) {
     float a = fabsf(x);
-    bool in = a < 1.0f;
     float a2 = a * a, a3 = a2 * a;
-    f = in ? 2.0f * a3 - 3.0f * a2 + 1.0f : 0.0f;
-    float gg = in ? a3 - 2.0f * a2 + a : 0.0f;
-    float dff = in ? 6.0f * a2 - 6.0f * a : 0.0f;
-    dg = in ? 3.0f * a2 - 4.0f * a + 1.0f : 0.0f;
+    f = 2.0f * a3 - 3.0f * a2 + 1.0f;
+    float gg = a3 - 2.0f * a2 + a;
+    float dff = 6.0f * a2 - 6.0f * a;
+    dg = 3.0f * a2 - 4.0f * a + 1.0f;
     g = x < 0.0f ? -gg : gg;
     df = x < 0.0f ? -dff : dff;
 }
