@@ -649,8 +649,12 @@ EDGE_D void rk4_pos(const Mac& mac, float psi[3], float dt) {
 // keeps the kernels inside the instruction cache.
 template <int NC>
 EDGE_D void rk4_jac(const Mac& mac, float psi[3], float C[NC][3], float dt) {
-    float u[3], G[3][3], q[3], Cs[NC][3], d[NC][3], su[3], sd[NC][3];
+    float u[3], G[3][3], q[3], Cs[NC][3], d[NC][3], su[3] = {0.0f, 0.0f, 0.0f}, sd[NC][3];
     float h = 0.5f * dt;
+#pragma unroll
+    for (int a = 0; a < NC; a++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) sd[a][c] = 0.0f;
 #pragma unroll
     for (int c = 0; c < 3; c++) q[c] = psi[c];
 #pragma unroll
@@ -665,13 +669,14 @@ EDGE_D void rk4_jac(const Mac& mac, float psi[3], float C[NC][3], float dt) {
         for (int a = 0; a < NC; a++)
 #pragma unroll
             for (int r = 0; r < 3; r++) d[a][r] = G[r][0] * Cs[a][0] + G[r][1] * Cs[a][1] + G[r][2] * Cs[a][2];
+        // the RK4 sums, started at zero: 0 + 1 * u is u exactly
         const float wt = (stage == 0 || stage == 3) ? 1.0f : 2.0f;
 #pragma unroll
-        for (int c = 0; c < 3; c++) su[c] = stage == 0 ? u[c] : su[c] + wt * u[c];
+        for (int c = 0; c < 3; c++) su[c] = su[c] + wt * u[c];
 #pragma unroll
         for (int a = 0; a < NC; a++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) sd[a][c] = stage == 0 ? d[a][c] : sd[a][c] + wt * d[a][c];
+            for (int c = 0; c < 3; c++) sd[a][c] = sd[a][c] + wt * d[a][c];
         if (stage < 3) {
             const float hh = stage < 2 ? h : dt;
 #pragma unroll
