@@ -70,9 +70,9 @@ EDGE_D Axis3 bspline_axis(float u, float hi) {
     Axis3 a;
     float s = fmaxf(1.0f, fminf(u, hi));
     float iu = floorf(s);
-    int b = (s - iu < 0.5f) ? (int)iu - 1 : (int)iu;
-    float x0 = s - (float)b;
-    a.base = b;
+    const float bf = (s - iu < 0.5f) ? iu - 1.0f : iu;  // the first tap, an integer held exactly
+    float x0 = s - bf;
+    a.base = (int)bf;
     // x0 lies in [0.5, 1.5) (exactly: s - b is exact), so the branches of
     // N2 / dN2 at x0, x0 - 1 and x0 - 2 are known: the same operations as the
     // general functions, without their compares.  The third tap's zero
