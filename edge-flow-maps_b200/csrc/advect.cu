@@ -213,8 +213,20 @@ EDGE_D void compose_jac(const float (&G)[3][3], const float (&C)[3][3], float (&
         }
 }
 
-template <bool IDENT, bool F64 = false>
-__global__ void __launch_bounds__(128, 5) k_march_edge_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+// The sampler struct with its power-of-two flag fixed at compile time: the
+// hot kernels are built for both cases (P2 = pow2f(dx), chosen at launch), so
+// over_dx is the exact multiply by 1/dx or the division with no run-time
+// select between them (which made every sample evaluate the division too).
+template <bool P2, class T>
+EDGE_D T with_pow2(T s) {
+    s.pow2 = P2 ? 1 : 0;
+    return s;
+}
+
+template <bool IDENT, bool F64, bool P2>
+__global__ void __launch_bounds__(128, 5) k_march_edge_p(Mac mac_, MapP m_, float dt, float eps, float4* __restrict__ out) {
+    const Mac mac = with_pow2<P2>(mac_);
+    const MapP m = with_pow2<P2>(m_);
     // The per-cell accumulators (the centre point's psi and Jacobian, the A
     // and B groups of the mixed derivatives) live in shared memory, one
     // column per thread, so that the registers hold only the current
@@ -287,7 +299,10 @@ __global__ void __launch_bounds__(128, 5) k_march_edge_p(Mac mac, MapP m, float 
 }
 
 // ED4 march on the packed layout; output planes 0-3.
-__global__ void __launch_bounds__(128) k_march_ed4_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+template <bool P2>
+__global__ void __launch_bounds__(128) k_march_ed4_p(Mac mac_, MapP m_, float dt, float eps, float4* __restrict__ out) {
+    const Mac mac = with_pow2<P2>(mac_);
+    const MapP m = with_pow2<P2>(m_);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
     if (e >= n) return;
@@ -315,7 +330,10 @@ __global__ void __launch_bounds__(128) k_march_ed4_p(Mac mac, MapP m, float dt, 
 }
 
 // ED8 march on the packed layout; output planes 0-7.
-__global__ void __launch_bounds__(128) k_march_ed8_p(Mac mac, MapP m, float dt, float eps, float4* __restrict__ out) {
+template <bool P2>
+__global__ void __launch_bounds__(128) k_march_ed8_p(Mac mac_, MapP m_, float dt, float eps, float4* __restrict__ out) {
+    const Mac mac = with_pow2<P2>(mac_);
+    const MapP m = with_pow2<P2>(m_);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
     if (e >= n) return;
@@ -385,8 +403,10 @@ __global__ void __launch_bounds__(128) k_march_ge(Mac mac, MapF m, float dt, flo
 }
 
 // packed layout: planes 0-3 of `out`
-template <bool F64 = false>
-__global__ void __launch_bounds__(128) k_march_ge_p(Mac mac, MapP m, float dt, float4* __restrict__ out) {
+template <bool F64, bool P2>
+__global__ void __launch_bounds__(128) k_march_ge_p(Mac mac_, MapP m_, float dt, float4* __restrict__ out) {
+    const Mac mac = with_pow2<P2>(mac_);
+    const MapP m = with_pow2<P2>(m_);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = m.n;
     if (e >= n) return;
@@ -554,8 +574,9 @@ __global__ void k_coef_p(MapP m, float4* __restrict__ g) {
 // face and the derivative along A (only that gradient column is evaluated)
 // (register caps: ED4 / EDGE 128 registers, 4 CTAs per SM; ED8 102, 5 CTAs
 // per SM; both measured faster than the uncapped builds)
-template <int V, int A>
-__global__ void __launch_bounds__(128, V == HV_FULL ? 5 : 4) k_face_map_p(MapP m, float* fp, float* fc) {
+template <int V, int A, bool P2>
+__global__ void __launch_bounds__(128, V == HV_FULL ? 5 : 4) k_face_map_p(MapP m_, float* fp, float* fc) {
+    const MapP m = with_pow2<P2>(m_);
     const int n1 = m.ny + (A == 1), n2 = m.nz + (A == 2);
     const long long nf = (long long)(m.nx + (A == 0)) * n1 * n2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -697,8 +718,10 @@ __global__ void __launch_bounds__(128) k_face_map(MapF m, float* fpx, float* fpy
 }
 
 // advance_map x3 (run_edge.py:330-357)
-__global__ void __launch_bounds__(128) k_advance_map(Mac mac, float dt, float* phix, float* phiy, float* phiz,
+template <bool P2>
+__global__ void __launch_bounds__(128) k_advance_map(Mac mac_, float dt, float* phix, float* phiy, float* phiz,
                                                      float* Fx, float* Fy, float* Fz) {
+    const Mac mac = with_pow2<P2>(mac_);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
     FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
@@ -729,8 +752,10 @@ struct VelRing {
     int steps;
 };
 
-__global__ void __launch_bounds__(128) k_backtrack_faces(Mac mac, VelRing ring, float* px, float* py, float* pz,
+template <bool P2>
+__global__ void __launch_bounds__(128) k_backtrack_faces(Mac mac_, VelRing ring, float* px, float* py, float* pz,
                                                          float* Tx, float* Ty, float* Tz) {
+    const Mac mac = with_pow2<P2>(mac_);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
     FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
@@ -754,7 +779,9 @@ __global__ void __launch_bounds__(128) k_backtrack_faces(Mac mac, VelRing ring, 
 }
 
 // advect_u_semi_lagrangian (hermite.py:1578-1621)
-__global__ void __launch_bounds__(128) k_advect_sl(Mac mac, float dt, float* ox, float* oy, float* oz) {
+template <bool P2>
+__global__ void __launch_bounds__(128) k_advect_sl(Mac mac_, float dt, float* ox, float* oy, float* oz) {
+    const Mac mac = with_pow2<P2>(mac_);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
     FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
@@ -781,8 +808,10 @@ struct Face3 {
 };
 
 // map_u / map_u_psi pullback with fused BFECC arithmetic (edge_pullback_u)
-__global__ void __launch_bounds__(256) k_pullback_u(Mac mac, Face3 pos, Face3 col, Face3 init, float scale, Face3 sub,
+template <bool P2>
+__global__ void __launch_bounds__(256) k_pullback_u(Mac mac_, Face3 pos, Face3 col, Face3 init, float scale, Face3 sub,
                                                     float* ox, float* oy, float* oz) {
+    const Mac mac = with_pow2<P2>(mac_);
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_faces(mac.nx, mac.ny, mac.nz)) return;
     FaceIdx f = face_decompose(t, mac.nx, mac.ny, mac.nz);
@@ -826,10 +855,12 @@ EDGE_D void centre_from_faces(const Face3& pos, int nx, int ny, int nz, int i, i
                 (__ldg(a0 + c) + __ldg(a1 + c) + __ldg(b0 + c) + __ldg(b1 + c) + __ldg(c0 + c) + __ldg(c1 + c));
 }
 
-__global__ void __launch_bounds__(256) k_pullback_dye(Dye dye, const float* __restrict__ smoke0, Face3 pos,
+template <bool P2>
+__global__ void __launch_bounds__(256) k_pullback_dye(Dye dye_, const float* __restrict__ smoke0, Face3 pos,
                                                       const float* __restrict__ init, float scale,
                                                       const float* sub, const float* __restrict__ clampsrc,
                                                       int inplace_clamp, float* out) {
+    const Dye dye = with_pow2<P2>(dye_);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     int n = dye.nx * dye.ny * dye.nz;
     if (e >= n) return;
@@ -1264,7 +1295,9 @@ int edge_march_ge_packed(int nx, int ny, int nz, float dx, float dt, const float
     MapP m = make_mapp(in_packed, nx, ny, nz, dx);
     int n = nx * ny * nz;
     float4* o = (float4*)out_packed;
-    k_march_ge_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), m, dt, o);
+    const Mac mac = make_mac(ux, uy, uz, nx, ny, nz, dx);
+    if (mac.pow2) k_march_ge_p<false, true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, o);
+    else k_march_ge_p<false, false><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, o);
     k_fd3_dT_p<<<grid_for(n), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, o);
     k_fd3_d2T_p<<<grid_for(n), kBlock, 0, S(stream)>>>(nx, ny, nz, dx, o);
     return launch_status();
@@ -1330,13 +1363,21 @@ int edge_march_packed(int variant, int nx, int ny, int nz, float dx, float dt, f
     float4* o = (float4*)out_packed;
     if (variant == HV_GARM) {
         const int g = grid_for(n, 128);
-        if (identity) k_march_edge_p<true><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
-        else if (f64) k_march_edge_p<false, true><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
-        else k_march_edge_p<false><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        if (mac.pow2) {
+            if (identity) k_march_edge_p<true, false, true><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else if (f64) k_march_edge_p<false, true, true><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else k_march_edge_p<false, false, true><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        } else {
+            if (identity) k_march_edge_p<true, false, false><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else if (f64) k_march_edge_p<false, true, false><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+            else k_march_edge_p<false, false, false><<<g, 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        }
     } else if (variant == HV_FD) {
-        k_march_ed4_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        if (mac.pow2) k_march_ed4_p<true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        else k_march_ed4_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
     } else {
-        k_march_ed8_p<<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        if (mac.pow2) k_march_ed8_p<true><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
+        else k_march_ed8_p<false><<<grid_for(n, 128), 128, 0, S(stream)>>>(mac, m, dt, epsilon, o);
     }
     derive_planes(variant, nx, ny, nz, out_packed, S(stream));
     return launch_status();
@@ -1353,17 +1394,35 @@ int edge_face_map_packed(int variant, int nx, int ny, int nz, float dx, const fl
               gz = grid_for((long long)nx * ny * (nz + 1), 128);
     cudaStream_t st = S(stream);
     if (variant == HV_FD) {
-        k_face_map_p<HV_FD_P, 0><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
-        k_face_map_p<HV_FD_P, 1><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
-        k_face_map_p<HV_FD_P, 2><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        if (m.pow2) {
+            k_face_map_p<HV_FD_P, 0, true><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+            k_face_map_p<HV_FD_P, 1, true><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+            k_face_map_p<HV_FD_P, 2, true><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        } else {
+            k_face_map_p<HV_FD_P, 0, false><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+            k_face_map_p<HV_FD_P, 1, false><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+            k_face_map_p<HV_FD_P, 2, false><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        }
     } else if (variant == HV_GARM) {
-        k_face_map_p<HV_GARM_P, 0><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
-        k_face_map_p<HV_GARM_P, 1><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
-        k_face_map_p<HV_GARM_P, 2><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        if (m.pow2) {
+            k_face_map_p<HV_GARM_P, 0, true><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+            k_face_map_p<HV_GARM_P, 1, true><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+            k_face_map_p<HV_GARM_P, 2, true><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        } else {
+            k_face_map_p<HV_GARM_P, 0, false><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+            k_face_map_p<HV_GARM_P, 1, false><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+            k_face_map_p<HV_GARM_P, 2, false><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        }
     } else {
-        k_face_map_p<HV_FULL, 0><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
-        k_face_map_p<HV_FULL, 1><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
-        k_face_map_p<HV_FULL, 2><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        if (m.pow2) {
+            k_face_map_p<HV_FULL, 0, true><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+            k_face_map_p<HV_FULL, 1, true><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+            k_face_map_p<HV_FULL, 2, true><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        } else {
+            k_face_map_p<HV_FULL, 0, false><<<gx, 128, 0, st>>>(m, fpsix, fcolx);
+            k_face_map_p<HV_FULL, 1, false><<<gy, 128, 0, st>>>(m, fpsiy, fcoly);
+            k_face_map_p<HV_FULL, 2, false><<<gz, 128, 0, st>>>(m, fpsiz, fcolz);
+        }
     }
     return launch_status();
 }
@@ -1392,8 +1451,10 @@ int edge_face_map(int variant, int nx, int ny, int nz, float dx, const float* ps
 int edge_advance_map(int nx, int ny, int nz, float dx, float dt, const float* ux, const float* uy, const float* uz,
                      float* phix, float* phiy, float* phiz, float* Fx, float* Fy, float* Fz, void* stream) {
     if (!dims_ok(nx, ny, nz) || !ux || !uy || !uz || !phix || !phiy || !phiz || !Fx || !Fy || !Fz) return EDGE_EINVAL;
-    k_advance_map<<<grid_for(n_faces(nx, ny, nz), 128), 128, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), dt,
-                                                                             phix, phiy, phiz, Fx, Fy, Fz);
+    const Mac mac = make_mac(ux, uy, uz, nx, ny, nz, dx);
+    const int g = grid_for(n_faces(nx, ny, nz), 128);
+    if (mac.pow2) k_advance_map<true><<<g, 128, 0, S(stream)>>>(mac, dt, phix, phiy, phiz, Fx, Fy, Fz);
+    else k_advance_map<false><<<g, 128, 0, S(stream)>>>(mac, dt, phix, phiy, phiz, Fx, Fy, Fz);
     return launch_status();
 }
 
@@ -1417,9 +1478,10 @@ int edge_efm_backtrack(int nx, int ny, int nz, float dx, int curr_step, const fl
         ring.u[s][0] = ring.u[s][1] = ring.u[s][2] = nullptr;
         ring.dt[s] = 0.0f;
     }
-    k_backtrack_faces<<<grid_for(n_faces(nx, ny, nz), 128), 128, 0, S(stream)>>>(
-        make_mac(ux_cache[curr_step], uy_cache[curr_step], uz_cache[curr_step], nx, ny, nz, dx), ring, psix, psiy,
-        psiz, Tx, Ty, Tz);
+    const Mac mac = make_mac(ux_cache[curr_step], uy_cache[curr_step], uz_cache[curr_step], nx, ny, nz, dx);
+    const int g = grid_for(n_faces(nx, ny, nz), 128);
+    if (mac.pow2) k_backtrack_faces<true><<<g, 128, 0, S(stream)>>>(mac, ring, psix, psiy, psiz, Tx, Ty, Tz);
+    else k_backtrack_faces<false><<<g, 128, 0, S(stream)>>>(mac, ring, psix, psiy, psiz, Tx, Ty, Tz);
     return launch_status();
 }
 
@@ -1427,8 +1489,10 @@ int edge_advect_u_sl(int nx, int ny, int nz, float dx, float dt, const float* ux
                      float* ux1, float* uy1, float* uz1, void* stream) {
     if (!dims_ok(nx, ny, nz) || !ux0 || !uy0 || !uz0 || !ux1 || !uy1 || !uz1) return EDGE_EINVAL;
     if (ux1 == ux0 || uy1 == uy0 || uz1 == uz0) return EDGE_EINVAL;
-    k_advect_sl<<<grid_for(n_faces(nx, ny, nz), 128), 128, 0, S(stream)>>>(make_mac(ux0, uy0, uz0, nx, ny, nz, dx), dt,
-                                                                           ux1, uy1, uz1);
+    const Mac mac = make_mac(ux0, uy0, uz0, nx, ny, nz, dx);
+    const int g = grid_for(n_faces(nx, ny, nz), 128);
+    if (mac.pow2) k_advect_sl<true><<<g, 128, 0, S(stream)>>>(mac, dt, ux1, uy1, uz1);
+    else k_advect_sl<false><<<g, 128, 0, S(stream)>>>(mac, dt, ux1, uy1, uz1);
     return launch_status();
 }
 
@@ -1443,8 +1507,10 @@ int edge_pullback_u(int nx, int ny, int nz, float dx, const float* ux0, const fl
     if (ux1 == ux0 || uy1 == uy0 || uz1 == uz0) return EDGE_EINVAL;
     Face3 pos = {{posx, posy, posz}}, col = {{colx, coly, colz}}, init = {{initx, inity, initz}},
           sub = {{subx, suby, subz}};
-    k_pullback_u<<<grid_for(n_faces(nx, ny, nz)), kBlock, 0, S(stream)>>>(make_mac(ux0, uy0, uz0, nx, ny, nz, dx), pos,
-                                                                          col, init, scale, sub, ux1, uy1, uz1);
+    const Mac mac = make_mac(ux0, uy0, uz0, nx, ny, nz, dx);
+    const int g = grid_for(n_faces(nx, ny, nz));
+    if (mac.pow2) k_pullback_u<true><<<g, kBlock, 0, S(stream)>>>(mac, pos, col, init, scale, sub, ux1, uy1, uz1);
+    else k_pullback_u<false><<<g, kBlock, 0, S(stream)>>>(mac, pos, col, init, scale, sub, ux1, uy1, uz1);
     return launch_status();
 }
 
@@ -1477,8 +1543,13 @@ int edge_pullback_dye(int nx, int ny, int nz, float dx, const float* smoke0, con
     if (!inplace_clamp && out == smoke0) return EDGE_EINVAL;
     Face3 pos = {{posx, posy, posz}};
     int n = nx * ny * nz;
-    k_pullback_dye<<<grid_for(n), kBlock, 0, S(stream)>>>(make_dye(nx, ny, nz, dx), smoke0, pos, init, scale, sub,
-                                                          clampsrc, inplace_clamp, out);
+    const Dye dye = make_dye(nx, ny, nz, dx);
+    if (dye.pow2)
+        k_pullback_dye<true><<<grid_for(n), kBlock, 0, S(stream)>>>(dye, smoke0, pos, init, scale, sub, clampsrc,
+                                                                    inplace_clamp, out);
+    else
+        k_pullback_dye<false><<<grid_for(n), kBlock, 0, S(stream)>>>(dye, smoke0, pos, init, scale, sub, clampsrc,
+                                                                     inplace_clamp, out);
     return launch_status();
 }
 
