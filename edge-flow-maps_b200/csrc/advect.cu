@@ -213,16 +213,6 @@ EDGE_D void compose_jac(const float (&G)[3][3], const float (&C)[3][3], float (&
         }
 }
 
-// The sampler struct with its power-of-two flag fixed at compile time: the
-// hot kernels are built for both cases (P2 = pow2f(dx), chosen at launch), so
-// over_dx is the exact multiply by 1/dx or the division with no run-time
-// select between them (which made every sample evaluate the division too).
-template <bool P2, class T>
-EDGE_D T with_pow2(T s) {
-    s.pow2 = P2 ? 1 : 0;
-    return s;
-}
-
 template <bool IDENT, bool F64, bool P2>
 __global__ void __launch_bounds__(128, 5) k_march_edge_p(Mac mac_, MapP m_, float dt, float eps, float4* __restrict__ out) {
     const Mac mac = with_pow2<P2>(mac_);

@@ -33,6 +33,15 @@ static inline bool pow2f(float x) {
     return x > 0.0f && frexpf(x, &e) == 0.5f;
 }
 EDGE_D float over_dx(float x, float dx, float inv_dx, bool pow2) { return pow2 ? x * inv_dx : x / dx; }
+// A sampler struct with its power-of-two flag fixed at compile time: the hot
+// kernels are built for both cases (P2 = pow2f(dx), chosen at launch), so
+// over_dx is the exact multiply by 1/dx or the division with no run-time
+// select between them (which made every sample evaluate the division too).
+template <bool P2, class T>
+EDGE_D T with_pow2(T s) {
+    s.pow2 = P2 ? 1 : 0;
+    return s;
+}
 // v[a] with constant indices only (a run-time index into a register array
 // or a kernel-parameter array puts it in local memory)
 EDGE_D float sel3(const float v[3], int a) { return a == 0 ? v[0] : (a == 1 ? v[1] : v[2]); }

@@ -19,8 +19,10 @@ inline int st(void) {
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // lp.py:6-29 update_particles_acc
-__global__ void k_lp_acc(Mac mac, const float* __restrict__ vel, const float* __restrict__ pos, float* acc, int num,
+template <bool P2>
+__global__ void k_lp_acc(Mac mac_, const float* __restrict__ vel, const float* __restrict__ pos, float* acc, int num,
                          int nmax, float dt, float St, float gravity) {
+    const Mac mac = with_pow2<P2>(mac_);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nmax) return;
     float a[3] = {0.f, 0.f, 0.f};
@@ -53,8 +55,10 @@ __global__ void k_lp_velocity(const float* __restrict__ acc, float* vel, const f
 }
 
 // lp.py:73-97 calculate_velocity_diff
-__global__ void k_lp_vel_diff(Mac mac, const float* __restrict__ vel, float* vdiff, const float* __restrict__ pos,
+template <bool P2>
+__global__ void k_lp_vel_diff(Mac mac_, const float* __restrict__ vel, float* vdiff, const float* __restrict__ pos,
                               int num, float kk) {
+    const Mac mac = with_pow2<P2>(mac_);
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= num) return;
     float p[3] = {pos[3 * e], pos[3 * e + 1], pos[3 * e + 2]};
@@ -66,7 +70,8 @@ __global__ void k_lp_vel_diff(Mac mac, const float* __restrict__ vel, float* vdi
 // lp.py:100-156 laden_particles_back_with_computing_particle: quadratic
 // B-spline scatter of the drag onto the three face grids (atomic adds, like
 // the reference's `+=` in a parallel loop)
-__global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float* dx_, float* dy_, float* dz_,
+template <bool P2>
+__global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float inv_dx, float* dx_, float* dy_, float* dz_,
                          const float* __restrict__ vdiff, const float* __restrict__ pos,
                          const float* __restrict__ rad, int num, float lrad, float Lx, float Ly, float Lz) {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -75,7 +80,7 @@ __global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float* dx_, float* dy
     if (p[0] < 3 * dx || p[1] < 3 * dx || p[2] < 3 * dx || p[0] > Lx - 3 * dx || p[1] > Ly - 3 * dx ||
         p[2] > Lz - 3 * dx)
         return;
-    float g[3] = {p[0] / dx, p[1] / dx, p[2] / dx};
+    float g[3] = {over_dx(p[0], dx, inv_dx, P2), over_dx(p[1], dx, inv_dx, P2), over_dx(p[2], dx, inv_dx, P2)};
     float r = rad[e];
     float scale = r * r * r / (lrad * lrad * lrad);
     float* D[3] = {dx_, dy_, dz_};
@@ -171,8 +176,9 @@ int edge_lp_acc(int nx, int ny, int nz, float dx, const float* ux, const float* 
     if (nx < 4 || ny < 4 || nz < 4 || !ux || !uy || !uz || num < 0 || nmax < num || (nmax && (!vel || !pos || !acc)))
         return EDGE_EINVAL;
     if (nmax == 0) return EDGE_OK;
-    k_lp_acc<<<grid_for(nmax), 256, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), vel, pos, acc, num, nmax, dt,
-                                                    St, gravity);
+    const Mac mac = make_mac(ux, uy, uz, nx, ny, nz, dx);
+    if (mac.pow2) k_lp_acc<true><<<grid_for(nmax), 256, 0, S(stream)>>>(mac, vel, pos, acc, num, nmax, dt, St, gravity);
+    else k_lp_acc<false><<<grid_for(nmax), 256, 0, S(stream)>>>(mac, vel, pos, acc, num, nmax, dt, St, gravity);
     return st();
 }
 
@@ -192,7 +198,9 @@ int edge_lp_vel_diff(int nx, int ny, int nz, float dx, const float* ux, const fl
     if (num == 0) return EDGE_OK;
     float eratio = 1.0f / (epiral_radius_ratio * epiral_radius_ratio * epiral_radius_ratio);
     float kk = 1.0f / St * density_ratio * eratio;
-    k_lp_vel_diff<<<grid_for(num), 256, 0, S(stream)>>>(make_mac(ux, uy, uz, nx, ny, nz, dx), vel, vdiff, pos, num, kk);
+    const Mac mac = make_mac(ux, uy, uz, nx, ny, nz, dx);
+    if (mac.pow2) k_lp_vel_diff<true><<<grid_for(num), 256, 0, S(stream)>>>(mac, vel, vdiff, pos, num, kk);
+    else k_lp_vel_diff<false><<<grid_for(num), 256, 0, S(stream)>>>(mac, vel, vdiff, pos, num, kk);
     return st();
 }
 
@@ -207,8 +215,13 @@ int edge_lp_p2g(int nx, int ny, int nz, float dx, float* dragx, float* dragy, fl
     if ((e = cudaMemsetAsync(dragy, 0, (size_t)nx * (ny + 1) * nz * 4, s)) != cudaSuccess) return (int)e;
     if ((e = cudaMemsetAsync(dragz, 0, (size_t)nx * ny * (nz + 1) * 4, s)) != cudaSuccess) return (int)e;
     if (num == 0) return EDGE_OK;
-    k_lp_p2g<<<grid_for(num), 256, 0, s>>>(nx, ny, nz, dx, dragx, dragy, dragz, vdiff, pos, rad, num, laden_radius, Lx,
-                                           Ly, Lz);
+    // p / dx as the reference writes it: the exact multiply by 1/dx when dx is a power of two
+    if (pow2f(dx))
+        k_lp_p2g<true><<<grid_for(num), 256, 0, s>>>(nx, ny, nz, dx, 1.0f / dx, dragx, dragy, dragz, vdiff, pos, rad,
+                                                     num, laden_radius, Lx, Ly, Lz);
+    else
+        k_lp_p2g<false><<<grid_for(num), 256, 0, s>>>(nx, ny, nz, dx, 1.0f / dx, dragx, dragy, dragz, vdiff, pos, rad,
+                                                      num, laden_radius, Lx, Ly, Lz);
     return st();
 }
 
