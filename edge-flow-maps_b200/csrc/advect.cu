@@ -571,10 +571,11 @@ __global__ void __launch_bounds__(128, V == HV_FULL ? 5 : 4) k_face_map_p(MapP m
     const long long nf = (long long)(m.nx + (A == 0)) * n1 * n2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nf) return;
-    const int e = (int)t;
-    const int k = (int)(t % n2);
-    const long long r = t / n2;
-    const int j = (int)(r % n1), i = (int)(r / n1);
+    const unsigned u = (unsigned)t;  // one face grid: fits 32 bits
+    const int e = (int)u;
+    const int k = (int)(u % (unsigned)n2);
+    const unsigned r = u / (unsigned)n2;
+    const int j = (int)(r % (unsigned)n1), i = (int)(r / (unsigned)n1);
     float X[3], val[3], G[3][3];
     face_pos(A, i, j, k, m.dx, X);
     hermite3p<V, true, A>(m, X, val, G);

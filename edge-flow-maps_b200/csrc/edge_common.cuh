@@ -727,11 +727,14 @@ EDGE_D FaceIdx face_decompose(long long t, int nx, int ny, int nz) {
     if (t < nfx) { f.axis = 0; n1 = ny; n2 = nz; }
     else if (t < nfx + nfy) { f.axis = 1; t -= nfx; n1 = ny + 1; n2 = nz; }
     else { f.axis = 2; t -= nfx + nfy; n1 = ny; n2 = nz + 1; }
-    f.e = (int)t;
-    f.k = (int)(t % n2);
-    long long r = t / n2;
-    f.j = (int)(r % n1);
-    f.i = (int)(r / n1);
+    // within one face grid the index fits 32 bits (f.e is an int): unsigned
+    // 32-bit division instead of the 64-bit one
+    const unsigned u = (unsigned)t;
+    f.e = (int)u;
+    f.k = (int)(u % (unsigned)n2);
+    const unsigned r = u / (unsigned)n2;
+    f.j = (int)(r % (unsigned)n1);
+    f.i = (int)(r / (unsigned)n1);
     return f;
 }
 
