@@ -571,6 +571,36 @@ EDGE_D void hcoef_p(const MapP& m, int ii, int jj, int kk, int im, int ip, int j
     }
 }
 
+// The coefficients of hcoef_p divided by dx^(number of g factors), for a
+// power-of-two dx (every such scaling is then exact): the g basis functions
+// carry the factor dx instead (hermite3p), which gives every product of the
+// contraction the same value with 3 multiplications per corner instead of 33.
+template <int VARIANT>
+EDGE_D void hcoef_p_unscaled(const MapP& m, int ii, int jj, int kk, float t[3][8]) {
+    const int e = idx3(ii, jj, kk, m.ny, m.nz);
+    const float inv = m.inv_dx;
+    float4 P = ldp(m, 0, e), G0 = ldp(m, 1, e), G1 = ldp(m, 2, e), G2 = ldp(m, 3, e);
+    float4 A = ldp(m, 4, e), B = ldp(m, 5, e), C = ldp(m, 6, e), D = ldp(m, 7, e);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        t[c][0] = c4(P, c);
+        t[c][4] = c4(G0, c);
+        t[c][2] = c4(G1, c);
+        t[c][1] = c4(G2, c);
+        if (VARIANT == HV_FD_P) {  // planes 4-7 hold the terms over dx (hcoef_p multiplies by dx once)
+            t[c][3] = c4(A, c) * inv;
+            t[c][5] = c4(B, c) * inv;
+            t[c][6] = c4(C, c) * inv;
+            t[c][7] = c4(D, c) * inv * inv;
+        } else {
+            t[c][3] = c4(A, c);
+            t[c][5] = c4(B, c);
+            t[c][6] = c4(C, c);
+            t[c][7] = VARIANT == HV_GARM_P ? c4(D, c) * inv : c4(D, c);  // GARM_P plane 7 holds psi_xyz over dx
+        }
+    }
+}
+
 // hermite3 on the packed layout: the 8 corners are visited once and feed all
 // three components.  GSEL >= 0 computes only column GSEL of the gradient
 // (grad[c][GSEL]; the other columns are left unset) with the same arithmetic:
@@ -583,6 +613,17 @@ EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[
     float q[3] = {over_dx(p[0], m.dx, m.inv_dx, m.pow2) - 0.5f, over_dx(p[1], m.dx, m.inv_dx, m.pow2) - 0.5f,
                   over_dx(p[2], m.dx, m.inv_dx, m.pow2) - 0.5f};
     HAxis X = haxis(q[0], m.hi[0], m.nx), Y = haxis(q[1], m.hi[1], m.ny), Z = haxis(q[2], m.hi[2], m.nz);
+    // power-of-two dx: the g basis functions carry dx and the coefficients
+    // come unscaled (hcoef_p_unscaled); the same products, fewer multiplies
+    const bool fold = (VARIANT == HV_FD_P || VARIANT == HV_GARM_P || VARIANT == HV_FULL) && m.pow2;
+    if (fold) {
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            X.g[c] *= m.dx; X.dg[c] *= m.dx;
+            Y.g[c] *= m.dx; Y.dg[c] *= m.dx;
+            Z.g[c] *= m.dx; Z.dg[c] *= m.dx;
+        }
+    }
     float v[3] = {0.f, 0.f, 0.f}, gx[3] = {0.f, 0.f, 0.f}, gy[3] = {0.f, 0.f, 0.f}, gz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int i = 0; i < 2; i++) {
@@ -597,7 +638,8 @@ EDGE_D void hermite3p(const MapP& m, const float p[3], float val[3], float grad[
             for (int k = 0; k < 2; k++) {
                 int kk = k ? Z.cp : Z.c0, km = k ? Z.c0 : Z.cm, kp = k ? Z.cpp : Z.cp;
                 float t[3][8];
-                hcoef_p<VARIANT>(m, ii, jj, kk, im, ip, jm, jp, km, kp, t);
+                if (fold) hcoef_p_unscaled<VARIANT>(m, ii, jj, kk, t);
+                else hcoef_p<VARIANT>(m, ii, jj, kk, im, ip, jm, jp, km, kp, t);
 #pragma unroll
                 for (int c = 0; c < 3; c++)
 #pragma unroll
