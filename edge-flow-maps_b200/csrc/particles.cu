@@ -93,20 +93,30 @@ __global__ void k_lp_p2g(int nx, int ny, int nz, float dx, float inv_dx, float* 
         }
         int n0 = nx + (a == 0), n1 = ny + (a == 1), n2 = nz + (a == 2);
         float val = vdiff[3 * e + a];
+        // the four taps' weights of each axis, once (the loops below used to
+        // re-evaluate N2 for every tap of the inner loops)
+        float W[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int o = 0; o < 4; o++) W[c][o] = N2(g[c] - (float)(base[c] + o - 1) - off[c]);
+#pragma unroll
         for (int oi = -1; oi < 3; oi++) {
             int f0 = base[0] + oi;
             if (f0 < 0 || f0 >= n0) continue;
-            float wx = N2(g[0] - (float)f0 - off[0]);
+            float wx = W[0][oi + 1];
             if (wx == 0.0f) continue;
+#pragma unroll
             for (int oj = -1; oj < 3; oj++) {
                 int f1 = base[1] + oj;
                 if (f1 < 0 || f1 >= n1) continue;
-                float wy = N2(g[1] - (float)f1 - off[1]);
+                float wy = W[1][oj + 1];
                 if (wy == 0.0f) continue;
+#pragma unroll
                 for (int ok = -1; ok < 3; ok++) {
                     int f2 = base[2] + ok;
                     if (f2 < 0 || f2 >= n2) continue;
-                    float w = wx * wy * N2(g[2] - (float)f2 - off[2]);
+                    float w = wx * wy * W[2][ok + 1];
                     if (w == 0.0f) continue;
                     atomicAdd(D[a] + idx3(f0, f1, f2, n1, n2), val * w * scale);
                 }
